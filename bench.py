@@ -1,0 +1,365 @@
+"""Throughput of the B200 PM step (particle-steps/s) on the headline workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl djb|reference] [--size c3|c2|small]
+
+Workload (default `c3`): 512³ particles, 1024³ mesh, L = 1000 Mpc/h, flat ΛCDM
+(Ωm 0.31, Ωb 0.049, h 0.677, n_s 0.965, σ8 0.81, EH transfer), 3LPT initial
+conditions at a = 0.02 from seeded white noise, PCS assignment, interlacing
+(antialias = 1), order-6 gradient, BullFrog stepper over W+K steps from a = 0.02
+to 1 (W + K = 20 by default). A step is one drift-kick-drift step of the whole
+particle set. W warm-up steps run untimed, then exactly K steps are timed with CUDA
+events on the solver's stream between a barrier + synchronize on both sides; the
+meshes (4.3 GB each) exceed L2, so no flush is needed between steps.
+
+Multi-GPU (torchrun): replicas only — every rank evolves its own box (seed + rank),
+no collective on the data path; value = all ranks' particle-steps / max time.
+
+`--impl reference` times the CPU restatement of the reference's algorithm (the
+oracle's OpenMP/pocketfft port, float32, all host threads) on a bounded sample of
+the same workload (128³ particles / 256³ mesh, same options), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "discodj.jl_b200"))
+
+METRIC = "particle-steps/s at 512³/1024³ mesh"
+UNIT = "particle-steps/s"
+COSMO = dict(Omega_c=0.31 - 0.049, Omega_b=0.049, h=0.677, n_s=0.965, sigma8=0.81)
+SIZES = {
+    # name: n, res, L, lpt order
+    "c3": (512, 1024, 1000.0, 3),
+    "c2": (256, 512, 500.0, 3),
+    "small": (64, 128, 125.0, 2),
+}
+OPTIONS = dict(worder=4, antialias=1, grad_order=6, lap_order=0, deconvolve=False)
+A_INI, A_END = 0.02, 1.0
+
+
+def algorithmic_bytes(n, res, nshift=2):
+    """Per-step and per-kernel algorithmic HBM bytes (float32).
+
+    step: n_shift·(24·N_m + 24·N_p) + 48·N_p (one compulsory pass per array).
+    kernels, per launch (one launch covers the 2 interlacing meshes):
+      scatter: read Ψ, Mom (24 B/particle), write Ψ (12), write each mesh (4 B/cell)
+      gather:  read Ψ, Mom (24), write Ψ, Mom (24), read each potential mesh (4 B/cell)
+      kspace:  read + write the half spectrum of one mesh (16 B/complex mode)"""
+    Np, Nm = n ** 3, res ** 3
+    modes = res * res * (res // 2 + 1)
+    return dict(
+        step=nshift * (24 * Nm + 24 * Np) + 48 * Np,
+        scatter=36 * Np + 4 * Nm * nshift,
+        gather=48 * Np + 4 * Nm * nshift,
+        kspace=16 * modes,
+    )
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+        time.sleep(0.25)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the top kernel from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_ics(cosmo, n, L, lpt, seed, device):
+    import torch
+
+    from djb200 import ics
+    dt = torch.float32 if n >= 256 else torch.float64
+    psi, pi = ics.lpt_ics(cosmo, n, L, A_INI, n_order=lpt, seed=seed, device=device, dtype=dt)
+    return psi.float(), pi.float()
+
+
+def cpu_sample(steps: int, warmup: int, seed: int = 42):
+    """CPU port (float32, all threads) on 128³/256³ with the headline options."""
+    import numpy as np
+
+    import djb200
+    from oracle import cpm
+    from oracle import pm as opm
+    n, res, L = 128, 256, 250.0
+    cosmo = djb200.Cosmology(**COSMO)
+    psi, pi = make_ics(cosmo, n, L, 3, seed, "cpu")
+    psi = psi.numpy()
+    mom = pi.numpy()
+    co = djb200.stepper_coefficients(cosmo, "bullfrog", A_INI, A_END, steps + warmup)
+    cfg = opm.PMConfig(res_pm=res, n_part=n, boxsize=L, **OPTIONS)
+    P = cpm.CPUPM(cfg, dtype=np.float32)
+    for k in range(warmup):
+        psi, mom = P.step(psi, mom, co["ddrift1"][k], co["alpha"][k], co["beta"][k], co["ddrift2"][k])
+    t0 = time.perf_counter()
+    for k in range(warmup, warmup + steps):
+        psi, mom = P.step(psi, mom, co["ddrift1"][k], co["alpha"][k], co["beta"][k], co["ddrift2"][k])
+    dt = time.perf_counter() - t0
+    return dict(value=n ** 3 * steps / dt, unit=UNIT, cores=cpm.threads(), kind="port",
+                sample=f"{n}^3 particles / {res}^3 mesh (L={L:g}), PCS, antialias=1, grad 6, BullFrog; "
+                       f"{steps} timed steps after {warmup} warm-up; float32 OpenMP scatter/gather + "
+                       f"pocketfft", ms_per_step=1e3 * dt / steps)
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    n, res, L, lpt = SIZES[args.size]
+    cb = cpu_sample(args.steps, args.warmup)
+    line = dict(metric=METRIC, value=cb["value"], unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=cb["ms_per_step"], higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f32", data="synthetic",
+                config=config_block(args.size, n, res, L, lpt, world), impl="reference",
+                cpu_baseline={k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                e2e=dict(value=cb["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def config_block(size, n, res, L, lpt, world):
+    return dict(workload=f"PM step {n}^3 particles / {res}^3 mesh, L={L:g} Mpc/h, {lpt}LPT ICs at a={A_INI}, "
+                         f"PCS + interlacing (antialias=1), order-6 gradient, BullFrog to a=1",
+                size=size, n_part=n, res_pm=res, boxsize=L, worder=4, antialias=1, grad_order=6,
+                stepper="bullfrog", parallelism=f"replicas{world}" if world > 1 else "single",
+                l2="inputs larger than L2 (each mesh exceeds 126 MB); no flush")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=17)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="djb", choices=["djb", "reference"])
+    ap.add_argument("--size", default="c3", choices=sorted(SIZES))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("warm-up must be >= 3 steps")
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    import numpy as np
+    import torch
+
+    import djb200
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    n, res, L, lpt = SIZES[args.size]
+    cosmo = djb200.Cosmology(**COSMO)
+    psi, pi = make_ics(cosmo, n, L, lpt, 42 + rank, dev)
+    psi_d = djb200.native_view(psi)
+    pi_d = djb200.native_view(pi)
+    # pinned host copies for the end-to-end leg
+    psi_h = torch.empty((3, n, n, n), dtype=torch.float32, pin_memory=True)
+    pi_h = torch.empty_like(psi_h, pin_memory=True)
+    psi_h.copy_(psi_d)
+    pi_h.copy_(pi_d)
+    del psi, pi
+    torch.cuda.empty_cache()
+    nsteps = args.warmup + args.steps
+    co = djb200.stepper_coefficients(cosmo, "bullfrog", A_INI, A_END, nsteps)
+    cfg = djb200.PMConfig(res_pm=res, n_part=n, boxsize=L, **OPTIONS)
+    S = djb200.PMSolver(cfg, device=local)
+    stream = torch.cuda.current_stream()
+    S.set_stream(stream.cuda_stream)
+    S.set_state(psi_d, pi_d)
+    del psi_d, pi_d
+    for k in range(args.warmup):
+        S.step(co["ddrift1"][k], co["alpha"][k], co["beta"][k], co["ddrift2"][k])
+    S.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    S.profile(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.warmup, nsteps):
+        S.step(co["ddrift1"][k], co["alpha"][k], co["beta"][k], co["ddrift2"][k])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_local = e0.elapsed_time(e1)
+    prof = S.profile_read()
+    clk = clocks.stop()
+    S.synchronize()
+    ms = allmax(world, ms_local)
+    Np = n ** 3
+    value = world * Np * args.steps / (ms / 1e3)
+
+    # end to end through the C ABI with host buffers: H2D of (Ψ, Π) from pinned memory,
+    # K fused steps, D2H of (X, P) into pinned memory, all inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        xo = torch.empty((3, n, n, n), dtype=torch.float32, pin_memory=True)
+        po = torch.empty_like(xo, pin_memory=True)
+        from djb200 import _lib
+        import ctypes as C
+        co2 = djb200.stepper_coefficients(cosmo, "bullfrog", A_INI, A_END, args.steps)
+        arrs = [np.ascontiguousarray(co2[k]) for k in ("ddrift1", "alpha", "beta", "ddrift2")]
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.check(_lib.lib.djb_set_state(S.handle, C.c_void_p(psi_h.data_ptr()), C.c_void_p(pi_h.data_ptr()),
+                                          1.0, _lib.MEM_HOST))
+        _lib.check(_lib.lib.djb_run(S.handle, args.steps, *[_lib.dptr(a) for a in arrs]))
+        _lib.check(_lib.lib.djb_get_output(S.handle, C.c_void_p(xo.data_ptr()), C.c_void_p(po.data_ptr()), 1,
+                                           1.0, cosmo.Fplus(A_END), _lib.MEM_HOST))
+        t_e2e = time.perf_counter() - t0
+        barrier(world)
+        t_e2e = allmax(world, t_e2e)
+        e2e = dict(value=world * Np * args.steps / t_e2e, unit=UNIT,
+                   h2d_bytes_per_step=int(2 * 12 * Np / args.steps),
+                   d2h_bytes_per_step=int(2 * 12 * Np / args.steps),
+                   note=f"one run of {args.steps} steps through djb_set_state/djb_run/djb_get_output with "
+                        f"pinned host buffers; bytes per step = state in + (X, P) out over the run")
+
+    # roofline of the dominant kernel of this library (CUDA-event time per launch)
+    ab = algorithmic_bytes(n, res)
+    peak, peak_kind = measured_peaks()
+    mine = {k: prof[k] for k in ("scatter", "kspace", "gather")}
+    top = max(mine, key=lambda k: mine[k][0])
+    t_ms, launches, calls = mine[top]
+    per_launch_ms = t_ms / max(calls, 1)
+    per_launch_bytes = ab[top] if top != "kspace" else ab["kspace"]
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+    tr = profile_traffic()
+    traffic = None
+    if tr and tr.get("kernel") == top and tr.get("size") == args.size:
+        traffic = tr.get("dram_bytes_per_launch")
+    step_bytes = ab["step"]
+    step_ms = ms / args.steps
+    roof = dict(bound="hbm", kernel=top, achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                traffic=traffic, peak_source=f"{peak_kind} hbm_gbs",
+                algorithmic_bytes_per_launch=per_launch_bytes, ms_per_launch=per_launch_ms)
+    phases = {k: dict(ms_per_step=v[0] / args.steps, launches=v[1]) for k, v in prof.items() if v[2]}
+    step_roof = dict(algorithmic_bytes=step_bytes, achieved=step_bytes / (step_ms / 1e3) / 1e9, peak=peak,
+                     frac=step_bytes / (step_ms / 1e3) / 1e9 / peak, unit="GB/s")
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_sample(2, 1)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=step_ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                    data="synthetic (seeded white noise -> EH P(k) -> 3LPT)",
+                    config=config_block(args.size, n, res, L, lpt, world), roofline=roof,
+                    step_roofline=step_roof, phases=phases, cpu_baseline=cpu, e2e=e2e, clocks=clk,
+                    gpu_launches=int(sum(v[1] for v in prof.values())),
+                    device_bytes=S.device_bytes)
+        print(json.dumps(line), flush=True)
+    S.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,260 @@
+// Isotropic power spectrum with float64 shell sums
+// (native/DiscoDJNative/src/analysis/power_spectrum.jl:25-79).
+//
+// The field is transformed in float32 by cuFFT (R2C, x axis halved). Each mode's
+// |δ(k)|²·V/res⁶, its weight (0.5 on the two self-conjugate planes of the halved
+// axis, power_spectrum.jl:59-60) and |k| are formed in float64 and summed per
+// shell: per-block shared-memory partials, then float64 atomics.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <vector>
+
+#include "common.h"
+
+using djb::fail;
+
+struct djb_solver;
+namespace djb {
+int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cudaStream_t* st);
+int64_t solver_np(const djb_solver* s);
+cufftHandle solver_r2c(const djb_solver* s);
+double solver_boxsize(const djb_solver* s);
+}  // namespace djb
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxBins = 1024;
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(DJB_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));      \
+    } while (0)
+
+#define CUFFT_TRY(expr)                                                                     \
+    do {                                                                                    \
+        cufftResult r_ = (expr);                                                            \
+        if (r_ != CUFFT_SUCCESS) return fail(DJB_ERR_CUFFT, "%s failed: cufft status %d", #expr, int(r_)); \
+    } while (0)
+
+// Shell sums: sums[4*b + 0] = Σ w·P, [1] = Σ w, [2] = Σ |k|, counts[b] = modes.
+__global__ void __launch_bounds__(kThreads) k_shells(const float2* __restrict__ f, int res, double dk,
+                                                      double norm, const double* __restrict__ edges,
+                                                      int bins, double* __restrict__ sums,
+                                                      unsigned long long* __restrict__ counts) {
+    extern __shared__ double sm[];
+    double* s_wp = sm;
+    double* s_w = sm + bins;
+    double* s_k = sm + 2 * bins;
+    unsigned long long* s_n = reinterpret_cast<unsigned long long*>(sm + 3 * bins);
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+        s_wp[b] = 0.0;
+        s_w[b] = 0.0;
+        s_k[b] = 0.0;
+        s_n[b] = 0ull;
+    }
+    __syncthreads();
+    const int nh = res / 2 + 1;
+    const int64_t total = int64_t(res) * res * nh;
+    const double kmin = edges[0], kmax = edges[bins];
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int kx = int(t % nh);
+        const int iy = int((t / nh) % res);
+        const int iz = int(t / (int64_t(nh) * res));
+        // full axes: index <= res/2 positive (power_spectrum.jl:40)
+        const double ky = double(iy <= res / 2 ? iy : iy - res) * dk;
+        const double kz = double(iz <= res / 2 ? iz : iz - res) * dk;
+        const double kh = double(kx) * dk;
+        // same association as the reference's kx²+ky²+kz² with its halved axis last
+        const double k = sqrt((kz * kz + ky * ky) + kh * kh);
+        if (!(k >= kmin && k < kmax)) continue;
+        int lo = 0, hi = bins;  // edges[lo] <= k < edges[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (edges[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        const float2 v = f[t];
+        const double p = (double(v.x) * v.x + double(v.y) * v.y) * norm;
+        const double w = (kx == 0 || kx == nh - 1) ? 0.5 : 1.0;
+        atomicAdd(&s_wp[lo], w * p);
+        atomicAdd(&s_w[lo], w);
+        atomicAdd(&s_k[lo], k);
+        atomicAdd(&s_n[lo], 1ull);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+        if (s_n[b] == 0ull) continue;
+        atomicAdd(&sums[4 * b + 0], s_wp[b]);
+        atomicAdd(&sums[4 * b + 1], s_w[b]);
+        atomicAdd(&sums[4 * b + 2], s_k[b]);
+        atomicAdd(&counts[b], s_n[b]);
+    }
+}
+
+// Julia LinRange element j of n (power_spectrum.jl:50-52).
+double linrange(double a, double b, int j, int n) {
+    if (j == 0) return a;
+    if (j == n - 1) return b;
+    const double t = double(j) / double(n - 1);
+    return (1.0 - t) * a + t * b;
+}
+
+std::vector<double> bin_edges(int res, double boxsize, int bins, bool logarithmic) {
+    const double dk = 2 * M_PI / boxsize;
+    const double kny = M_PI * res / boxsize;
+    const double kmin = dk, kmax = kny * std::sqrt(3.0);
+    std::vector<double> e(bins + 1);
+    for (int j = 0; j <= bins; ++j)
+        e[j] = logarithmic ? std::pow(10.0, linrange(std::log10(kmin), std::log10(kmax), j, bins + 1))
+                           : linrange(kmin, kmax, j, bins + 1);
+    return e;
+}
+
+// Bins the spectrum `spec` (already transformed) and writes k, P, N on the host.
+int shells(const float2* spec, int res, double boxsize, double scale2, int bins, bool logarithmic,
+           double* k_out, double* pk_out, int64_t* n_out, cudaStream_t st) {
+    std::vector<double> e = bin_edges(res, boxsize, bins, logarithmic);
+    double* d_edges = nullptr;
+    double* d_sums = nullptr;
+    unsigned long long* d_counts = nullptr;
+    int rc = DJB_OK;
+    auto cleanup = [&]() {
+        if (d_edges) cudaFreeAsync(d_edges, st);
+        if (d_sums) cudaFreeAsync(d_sums, st);
+        if (d_counts) cudaFreeAsync(d_counts, st);
+    };
+    if (cudaMallocAsync((void**)&d_edges, sizeof(double) * (bins + 1), st) != cudaSuccess ||
+        cudaMallocAsync((void**)&d_sums, sizeof(double) * 4 * bins, st) != cudaSuccess ||
+        cudaMallocAsync((void**)&d_counts, sizeof(unsigned long long) * bins, st) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return fail(DJB_ERR_ALLOC, "power spectrum work area allocation failed");
+    }
+    std::vector<double> sums(4 * size_t(bins));
+    std::vector<unsigned long long> counts(bins);
+    do {
+        if (cudaMemcpyAsync(d_edges, e.data(), sizeof(double) * (bins + 1), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemsetAsync(d_sums, 0, sizeof(double) * 4 * bins, st) != cudaSuccess ||
+            cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * bins, st) != cudaSuccess) {
+            rc = fail(DJB_ERR_CUDA, "power spectrum set-up copy failed");
+            break;
+        }
+        const double V = boxsize * boxsize * boxsize;
+        const double r3 = double(res) * res * res;
+        const double norm = V / (r3 * r3) * scale2;
+        const int64_t total = int64_t(res) * res * (res / 2 + 1);
+        int grid = int(std::min<int64_t>((total + kThreads - 1) / kThreads, 148 * 8));
+        const size_t smem = size_t(bins) * 4 * sizeof(double);
+        k_shells<<<grid, kThreads, smem, st>>>(spec, res, 2 * M_PI / boxsize, norm, d_edges, bins, d_sums, d_counts);
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) {
+            rc = fail(DJB_ERR_CUDA, "shell kernel launch failed: %s", cudaGetErrorString(le));
+            break;
+        }
+        if (cudaMemcpyAsync(sums.data(), d_sums, sizeof(double) * 4 * bins, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(counts.data(), d_counts, sizeof(unsigned long long) * bins, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = fail(DJB_ERR_CUDA, "power spectrum read-back failed");
+            break;
+        }
+    } while (false);
+    cleanup();
+    if (rc != DJB_OK) return rc;
+    for (int b = 0; b < bins; ++b) {
+        const unsigned long long n = counts[b];
+        if (n == 0) {
+            k_out[b] = std::sqrt(e[b] * e[b + 1]);
+            pk_out[b] = 0.0;
+            n_out[b] = 0;
+        } else {
+            k_out[b] = sums[4 * b + 2] / double(n);
+            pk_out[b] = sums[4 * b + 0] / sums[4 * b + 1];
+            n_out[b] = int64_t(n);
+        }
+    }
+    return DJB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int djb_power_spectrum(const float* field, int32_t res, double boxsize, int32_t bins, int32_t logarithmic,
+                       double* k, double* pk, int64_t* nmodes, int32_t mem, int32_t device) {
+    djb::clear_error();
+    if (!field || !k || !pk || !nmodes) return fail(DJB_ERR_INVALID, "null argument");
+    if (res < 2 || (res & 1)) return fail(DJB_ERR_INVALID, "field must be cubic with an even side");
+    if (bins < 1 || bins > kMaxBins) return fail(DJB_ERR_INVALID, "bins must be in 1..%d", kMaxBins);
+    if (!(boxsize > 0)) return fail(DJB_ERR_INVALID, "boxsize must be positive");
+    CUDA_TRY(cudaSetDevice(device));
+    cudaStream_t st;
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const int pitch = res + 2;
+    float* mesh = nullptr;
+    cufftHandle plan = 0;
+    bool have_plan = false;
+    int rc = DJB_OK;
+    do {
+        if (cudaMallocAsync((void**)&mesh, sizeof(float) * size_t(res) * res * pitch, st) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(DJB_ERR_ALLOC, "power spectrum mesh allocation failed");
+            break;
+        }
+        // column-major (res,res,res) [ix,iy,iz] rows of res floats into rows of res+2
+        if (cudaMemcpy2DAsync(mesh, sizeof(float) * pitch, field, sizeof(float) * res, sizeof(float) * res,
+                              size_t(res) * res,
+                              mem == DJB_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                              st) != cudaSuccess) {
+            rc = fail(DJB_ERR_CUDA, "field copy failed");
+            break;
+        }
+        long long dims[3] = {res, res, res};
+        long long rembed[3] = {res, res, pitch};
+        long long cembed[3] = {res, res, res / 2 + 1};
+        size_t work = 0;
+        if (cufftCreate(&plan) != CUFFT_SUCCESS) {
+            rc = fail(DJB_ERR_CUFFT, "cufftCreate failed");
+            break;
+        }
+        have_plan = true;
+        if (cufftMakePlanMany64(plan, 3, dims, rembed, 1, rembed[0] * rembed[1] * rembed[2], cembed, 1,
+                                cembed[0] * cembed[1] * cembed[2], CUFFT_R2C, 1, &work) != CUFFT_SUCCESS ||
+            cufftSetStream(plan, st) != CUFFT_SUCCESS ||
+            cufftExecR2C(plan, mesh, reinterpret_cast<cufftComplex*>(mesh)) != CUFFT_SUCCESS) {
+            rc = fail(DJB_ERR_CUFFT, "power spectrum transform failed");
+            break;
+        }
+        rc = shells(reinterpret_cast<const float2*>(mesh), res, boxsize, 1.0, bins, logarithmic != 0, k, pk,
+                    nmodes, st);
+    } while (false);
+    if (have_plan) cufftDestroy(plan);
+    if (mesh) cudaFreeAsync(mesh, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logarithmic, double* k, double* pk,
+                             int64_t* nmodes) {
+    djb::clear_error();
+    if (!s || !k || !pk || !nmodes) return fail(DJB_ERR_INVALID, "null argument");
+    if (bins < 1 || bins > kMaxBins) return fail(DJB_ERR_INVALID, "bins must be in 1..%d", kMaxBins);
+    float* mesh = nullptr;
+    int res = 0, pitch = 0;
+    cudaStream_t st = nullptr;
+    int rc = djb::solver_deposit_cic(s, &mesh, &res, &pitch, &st);
+    if (rc != DJB_OK) return rc;
+    CUFFT_TRY(cufftExecR2C(djb::solver_r2c(s), mesh, reinterpret_cast<cufftComplex*>(mesh)));
+    // δ = mesh·res³/n³ − 1: for k ≠ 0 the spectrum scales by (res³/n³)²
+    const double f = double(res) * res * res / double(djb::solver_np(s));
+    return shells(reinterpret_cast<const float2*>(mesh), res, djb::solver_boxsize(s), f * f, bins,
+                  logarithmic != 0, k, pk, nmodes, st);
+}
+
+}  // extern "C"

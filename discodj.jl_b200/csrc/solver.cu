@@ -1,0 +1,1354 @@
+// libdjb200 PM solver: device state, cuFFT plans, and the orchestration of one
+// force evaluation / one drift-kick-drift step (the hot path of DiscoDJNative's
+// `run_nbody`, native/DiscoDJNative/src/nbody/pm.jl:466-521 and run_nbody.jl:155-163).
+//
+// One step, for each group of interlacing shifts (up to kMaxGroup meshes live):
+//   k_scatter      drift Psi += dd1*Mom (first group only), X = q + Psi + shift,
+//                  W-order mass assignment into the group's meshes
+//   [resampling]   extra particle sets from the Lagrangian sheet (pm.jl:443-464)
+//   cuFFT R2C      in place, per mesh
+//   k_kspace_*     x Kφ (Green's function, deconvolution, 1/(ρ̄ n_sets N)), and for
+//                  grad_order 0 the ik gradient into three spectra
+//   cuFFT C2R      in place (unnormalised; 1/N folded into Kφ)
+//   k_gather_*     force interpolation; finite-difference gradients are applied to
+//                  the potential inside the gather; the last group finishes the
+//                  mean over shifts, the kick Mom = a*Mom + b*acc and the drift
+//                  Psi += dd2*Mom
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "pm_kernels.cuh"
+
+using djb::fail;
+
+namespace {
+
+constexpr int kMaxGroup = 2;  // interlacing meshes processed per particle pass
+constexpr int kThreads = 256;
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(DJB_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));      \
+    } while (0)
+
+#define CUFFT_TRY(expr)                                                                     \
+    do {                                                                                    \
+        cufftResult r_ = (expr);                                                            \
+        if (r_ != CUFFT_SUCCESS) return fail(DJB_ERR_CUFFT, "%s failed: cufft status %d", #expr, int(r_)); \
+    } while (0)
+
+// Shift list of the `dealias` decorator (pm.jl:237-246), in the same order.
+std::vector<double> aa_shifts(int aa, double dh) {
+    std::vector<double> s;
+    auto push = [&](double a, double b, double c) {
+        s.push_back(a);
+        s.push_back(b);
+        s.push_back(c);
+    };
+    if (aa == 0) {
+        push(0, 0, 0);
+    } else if (aa == -1) {
+        push(dh, dh, dh);
+    } else if (aa == 1) {
+        push(0, 0, 0);
+        push(dh, dh, dh);
+    } else {
+        const double v[2] = {0.0, dh};
+        for (double a : v)
+            for (double b : v)
+                for (double c : v) push(a, b, c);
+        if (aa == 3) {
+            const double q = dh / 2, u[2] = {-q, q};
+            for (double a : u)
+                for (double b : u)
+                    for (double c : u) push(a, b, c);
+        }
+    }
+    return s;
+}
+
+// pm.jl:233-234: offsets (0..nr-1)/nr per axis, last axis fastest, zero offset dropped.
+std::vector<double> resample_shifts(int nr) {
+    std::vector<double> s;
+    for (int a = 0; a < nr; ++a)
+        for (int b = 0; b < nr; ++b)
+            for (int c = 0; c < nr; ++c) {
+                if (a == 0 && b == 0 && c == 0) continue;
+                s.push_back(double(a) / nr);
+                s.push_back(double(b) / nr);
+                s.push_back(double(c) / nr);
+            }
+    return s;
+}
+
+struct Shift3 {
+    float x, y, z;
+};
+
+struct GroupShifts {
+    Shift3 s[kMaxGroup];
+};
+
+}  // namespace
+
+// ─────────────────────────────────────────────────────────────────────────────
+// kernels
+// ─────────────────────────────────────────────────────────────────────────────
+namespace djb {
+
+// Mass assignment of NS shifted copies of the particles (pm.jl:57-74; interlacing
+// copies as in pm.jl:515-517). When `mom` is non-null the first drift of the
+// step is applied first and written back: Psi <- Psi + dd1*Mom (run_nbody.jl:156).
+template <int W, int NS>
+__global__ void __launch_bounds__(kThreads) k_scatter(
+    float* __restrict__ psi, const float* __restrict__ mom, float dd1, const float* __restrict__ q1,
+    int n, int64_t np, float L, int res, int pitch, GroupShifts sh, float* __restrict__ mesh0,
+    float* __restrict__ mesh1, int* err) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const int i = int(p % n);
+    const int j = int((p / n) % n);
+    const int k = int(p / (int64_t(n) * n));
+    float ps[3] = {psi[p], psi[p + np], psi[p + 2 * np]};
+    if (mom) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ps[c] = ps[c] + dd1 * mom[p + c * np];
+            psi[p + c * np] = ps[c];
+        }
+    }
+    const float X[3] = {ps[0] + q1[i], ps[1] + q1[j], ps[2] + q1[k]};
+    const float resf = float(res);
+#pragma unroll
+    for (int g = 0; g < NS; ++g) {
+        float* mesh = (g == 0) ? mesh0 : mesh1;
+        const float gx = grid_coord(X[0] + sh.s[g].x, L, resf, err);
+        const float gy = grid_coord(X[1] + sh.s[g].y, L, resf, err);
+        const float gz = grid_coord(X[2] + sh.s[g].z, L, resf, err);
+        float wx[W], wy[W], wz[W];
+        int ix[W], iy[W], iz[W];
+        axis_weights<W>(gx, res, wx, ix);
+        axis_weights<W>(gy, res, wy, iy);
+        axis_weights<W>(gz, res, wz, iz);
+#pragma unroll
+        for (int c = 0; c < W; ++c) {
+#pragma unroll
+            for (int b = 0; b < W; ++b) {
+                float* row = mesh + (int64_t(iz[c]) * res + iy[b]) * pitch;
+#pragma unroll
+                for (int a = 0; a < W; ++a) atomicAdd(row + ix[a], wx[a] * wy[b] * wz[c]);
+            }
+        }
+    }
+}
+
+// Deposit of externally placed positions (resampled sheet particles): X given per
+// component in `xr` (3 blocks of `count` floats). pm.jl:477,481.
+template <int W>
+__global__ void __launch_bounds__(kThreads) k_scatter_positions(
+    const float* __restrict__ xr, int64_t count, int64_t cstride, float L, int res, int pitch,
+    float* __restrict__ mesh, int* err) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    const float resf = float(res);
+    const float gx = grid_coord(xr[p], L, resf, err);
+    const float gy = grid_coord(xr[p + cstride], L, resf, err);
+    const float gz = grid_coord(xr[p + 2 * cstride], L, resf, err);
+    float wx[W], wy[W], wz[W];
+    int ix[W], iy[W], iz[W];
+    axis_weights<W>(gx, res, wx, ix);
+    axis_weights<W>(gy, res, wy, iy);
+    axis_weights<W>(gz, res, wz, iz);
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+#pragma unroll
+        for (int b = 0; b < W; ++b) {
+            float* row = mesh + (int64_t(iz[c]) * res + iy[b]) * pitch;
+#pragma unroll
+            for (int a = 0; a < W; ++a) atomicAdd(row + ix[a], wx[a] * wy[b] * wz[c]);
+        }
+}
+
+// Combined Fourier multiplier Kφ (pm.jl:389-391) evaluated per mode from 1-D
+// float64 tables: Kφ = s0 * mak / (T[kx] + T[ky] + T[kz]), DC = 0. T = -k² for
+// lap_order 0 (so 1/T = -1/k², pm.jl:166-170) or the finite-difference terms
+// (pm.jl:140-147,171-176); mak = Π sinc^(-2W) (pm.jl:150-151) or 1.
+__device__ __forceinline__ float kphi(const double* __restrict__ T, const double* __restrict__ M,
+                                      double s0, int kx, int ky, int kz) {
+    if ((kx | ky | kz) == 0) return 0.0f;
+    double v = s0 / (T[kx] + T[ky] + T[kz]);
+    if (M) v *= M[kx] * M[ky] * M[kz];
+    return float(v);
+}
+
+// fd <- Kφ·fd in place on a half spectrum [kz][ky][kx], kx in [0, res/2] (pm.jl:317-320,632).
+__global__ void __launch_bounds__(kThreads) k_kspace_mul(float2* __restrict__ f, int res,
+                                                          const double* __restrict__ T,
+                                                          const double* __restrict__ M, double s0) {
+    const int nh = res / 2 + 1;
+    const int64_t total = int64_t(res) * res * nh;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int kx = int(t % nh);
+        const int ky = int((t / nh) % res);
+        const int kz = int(t / (int64_t(nh) * res));
+        const float K = kphi(T, M, s0, kx, ky, kz);
+        float2 v = f[t];
+        v.x *= K;
+        v.y *= K;
+        f[t] = v;
+    }
+}
+
+// ik gradient (grad_order 0): out_ax = -(i g_ax Kφ fd) for the three axes
+// (pm.jl:322-328,487-492). gh: halved-axis k with Nyquist zeroed; gf: full-axis k
+// with Nyquist zeroed (pm.jl:125-130).
+__global__ void __launch_bounds__(kThreads) k_kspace_ik(const float2* __restrict__ f, int res,
+                                                         const double* __restrict__ T,
+                                                         const double* __restrict__ M, double s0,
+                                                         const float* __restrict__ gh,
+                                                         const float* __restrict__ gf,
+                                                         float2* __restrict__ ox,
+                                                         float2* __restrict__ oy,
+                                                         float2* __restrict__ oz) {
+    const int nh = res / 2 + 1;
+    const int64_t total = int64_t(res) * res * nh;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int kx = int(t % nh);
+        const int ky = int((t / nh) % res);
+        const int kz = int(t / (int64_t(nh) * res));
+        const float K = kphi(T, M, s0, kx, ky, kz);
+        const float2 v = f[t];
+        const float g[3] = {gh[kx], gf[ky], gf[kz]};
+        float2* o[3] = {ox, oy, oz};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float tk = g[c] * K;  // (i g)·K·(a + i b) = (-g K b) + i (g K a); negated
+            o[c][t] = make_float2(tk * v.y, -(tk * v.x));
+        }
+    }
+}
+
+// Σ over the W³ nodes of w · F_c, with F_c = -D_c φ the order-2R central
+// difference (pm.jl:330-342,419-424) applied to the potential on the fly.
+// Written as one pass over the cross-shaped union of the three stencils: for each
+// axis the weights are convolved with the antisymmetric difference stencil, so
+// each potential value is loaded once per particle.
+template <int W, int R>
+__device__ __forceinline__ void gather_fd(const float* __restrict__ phi, int res, int pitch, float gx,
+                                          float gy, float gz, float c1, float c2, float c3,
+                                          float& Sx, float& Sy, float& Sz) {
+    constexpr int E = W + 2 * R;
+    float wx[W], wy[W], wz[W];
+    int cx[W], cy[W], cz[W];
+    axis_weights<W>(gx, res, wx, cx);
+    axis_weights<W>(gy, res, wy, cy);
+    axis_weights<W>(gz, res, wz, cz);
+    const int bx = wbase<W>(gx) + WLo<W>::v, by = wbase<W>(gy) + WLo<W>::v,
+              bz = wbase<W>(gz) + WLo<W>::v;
+    const float cc[4] = {0.0f, c1, c2, c3};
+    // kappa(t) = coefficient of φ(node + t) in F(node): -c_t for t > 0, +c_|t| for t < 0.
+    float ux[E], uy[E], uz[E];
+    int ex[E];
+    int64_t ey[E], ez[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+#pragma unroll
+        for (int a = 0; a < W; ++a) {
+            const int t = e - R - a;
+            const float kap = (t > 0 && t <= R) ? -cc[t > 0 ? t : 0] : ((t < 0 && -t <= R) ? cc[t < 0 ? -t : 0] : 0.0f);
+            sx += wx[a] * kap;
+            sy += wy[a] * kap;
+            sz += wz[a] * kap;
+        }
+        ux[e] = sx;
+        uy[e] = sy;
+        uz[e] = sz;
+        ex[e] = wrapi(bx - R + e, res);
+        ey[e] = int64_t(wrapi(by - R + e, res)) * pitch;
+        ez[e] = int64_t(wrapi(bz - R + e, res)) * res * pitch;
+    }
+    (void)cx;
+    (void)cy;
+    (void)cz;
+    float sX = 0.0f, sY = 0.0f, sZ = 0.0f;
+    // core rows: y and z inside the W-node stencil, x over the extended range
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+#pragma unroll
+        for (int b = 0; b < W; ++b) {
+            const float* row = phi + ez[c + R] + ey[b + R];
+            float rx = 0.0f, rc = 0.0f;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const float v = __ldg(row + ex[e]);
+                rx += ux[e] * v;
+                if (e >= R && e < R + W) rc += wx[e - R] * v;
+            }
+            sX += (wy[b] * wz[c]) * rx;
+            sY += (uy[b + R] * wz[c]) * rc;
+            sZ += (uz[c + R] * wy[b]) * rc;
+        }
+    }
+    // y halo rows (for the y derivative) and z halo rows (for the z derivative)
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+#pragma unroll
+        for (int h = 0; h < 2 * R; ++h) {
+            const int e = (h < R) ? h : h + W;
+            const float* row = phi + ez[c + R] + ey[e];
+            float rc = 0.0f;
+#pragma unroll
+            for (int a = 0; a < W; ++a) rc += wx[a] * __ldg(row + ex[a + R]);
+            sY += (uy[e] * wz[c]) * rc;
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2 * R; ++h) {
+        const int e = (h < R) ? h : h + W;
+#pragma unroll
+        for (int b = 0; b < W; ++b) {
+            const float* row = phi + ez[e] + ey[b + R];
+            float rc = 0.0f;
+#pragma unroll
+            for (int a = 0; a < W; ++a) rc += wx[a] * __ldg(row + ex[a + R]);
+            sZ += (uz[e] * wy[b]) * rc;
+        }
+    }
+    Sx = sX;
+    Sy = sY;
+    Sz = sZ;
+}
+
+// Σ over the W³ nodes of w·F_c for three precomputed force meshes (ik gradient;
+// pm.jl:344-364).
+template <int W>
+__device__ __forceinline__ void gather_f3(const float* __restrict__ fx, const float* __restrict__ fy,
+                                          const float* __restrict__ fz, int res, int pitch, float gx,
+                                          float gy, float gz, float& Sx, float& Sy, float& Sz) {
+    float wx[W], wy[W], wz[W];
+    int ix[W], iy[W], iz[W];
+    axis_weights<W>(gx, res, wx, ix);
+    axis_weights<W>(gy, res, wy, iy);
+    axis_weights<W>(gz, res, wz, iz);
+    float s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+#pragma unroll
+        for (int b = 0; b < W; ++b) {
+            const int64_t r = (int64_t(iz[c]) * res + iy[b]) * pitch;
+#pragma unroll
+            for (int a = 0; a < W; ++a) {
+                const float w = wx[a] * wy[b] * wz[c];
+                s1 += __ldg(fx + r + ix[a]) * w;
+                s2 += __ldg(fy + r + ix[a]) * w;
+                s3 += __ldg(fz + r + ix[a]) * w;
+            }
+        }
+    Sx = s1;
+    Sy = s2;
+    Sz = s3;
+}
+
+struct GatherArgs {
+    float* psi;         // displacements (read; written by the fused final drift)
+    float* mom;         // momenta (read/written by the fused kick) or null
+    float* acc;         // running acceleration sums (partial groups) / output
+    const float* q1;    // lattice coordinates q_i = i*L/n
+    const float* mesh[kMaxGroup];      // potentials (FD) or x-force meshes (ik)
+    const float* meshy[kMaxGroup];     // ik: y-force meshes
+    const float* meshz[kMaxGroup];     // ik: z-force meshes
+    GroupShifts sh;
+    int n;
+    int64_t np;
+    float L;
+    int res, pitch;
+    float c1, c2, c3;
+    int first;          // 1: start the sums at zero; 0: continue from acc
+    int last;           // 1: finish (mean over shifts, then write acc or kick-drift)
+    float nshift_f;     // number of interlacing shifts (divisor when > 1)
+    int divide;
+    int step;           // 1: kick + drift after the last group; 0: write acc
+    float alpha, beta, dd2;
+    int* err;
+};
+
+template <int W, int R, int NS>
+__global__ void __launch_bounds__(kThreads) k_gather(GatherArgs A) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= A.np) return;
+    const int64_t np = A.np;
+    const int n = A.n;
+    const int i = int(p % n);
+    const int j = int((p / n) % n);
+    const int k = int(p / (int64_t(n) * n));
+    const float ps[3] = {A.psi[p], A.psi[p + np], A.psi[p + 2 * np]};
+    const float X[3] = {ps[0] + A.q1[i], ps[1] + A.q1[j], ps[2] + A.q1[k]};
+    float acc[3];
+    if (A.first) {
+        acc[0] = acc[1] = acc[2] = 0.0f;
+    } else {
+        acc[0] = A.acc[p];
+        acc[1] = A.acc[p + np];
+        acc[2] = A.acc[p + 2 * np];
+    }
+    const float resf = float(A.res);
+#pragma unroll
+    for (int g = 0; g < NS; ++g) {
+        const float gx = grid_coord(X[0] + A.sh.s[g].x, A.L, resf, A.err);
+        const float gy = grid_coord(X[1] + A.sh.s[g].y, A.L, resf, A.err);
+        const float gz = grid_coord(X[2] + A.sh.s[g].z, A.L, resf, A.err);
+        float s1, s2, s3;
+        if (R == 0)
+            gather_f3<W>(A.mesh[g], A.meshy[g], A.meshz[g], A.res, A.pitch, gx, gy, gz, s1, s2, s3);
+        else
+            gather_fd<W, (R == 0 ? 1 : R)>(A.mesh[g], A.res, A.pitch, gx, gy, gz, A.c1, A.c2, A.c3,
+                                           s1, s2, s3);
+        acc[0] += s1;
+        acc[1] += s2;
+        acc[2] += s3;
+    }
+    if (A.last && A.divide) {  // acc ./= length(shifts) (pm.jl:519)
+        acc[0] = acc[0] / A.nshift_f;
+        acc[1] = acc[1] / A.nshift_f;
+        acc[2] = acc[2] / A.nshift_f;
+    }
+    if (A.last && A.step) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float m = A.alpha * A.mom[p + c * np] + A.beta * acc[c];
+            A.mom[p + c * np] = m;
+            A.psi[p + c * np] = ps[c] + A.dd2 * m;
+        }
+    } else {
+        A.acc[p] = acc[0];
+        A.acc[p + np] = acc[1];
+        A.acc[p + 2 * np] = acc[2];
+    }
+}
+
+// ── elementwise kernels ───────────────────────────────────────────────────────
+__global__ void k_drift(float* __restrict__ psi, const float* __restrict__ mom, float dd, int64_t m) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m;
+         t += int64_t(gridDim.x) * blockDim.x)
+        psi[t] = psi[t] + dd * mom[t];
+}
+
+__global__ void k_kick_drift(float* __restrict__ psi, float* __restrict__ mom,
+                             const float* __restrict__ acc, float alpha, float beta, float dd2,
+                             int64_t m) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const float v = alpha * mom[t] + beta * acc[t];
+        mom[t] = v;
+        psi[t] = psi[t] + dd2 * v;
+    }
+}
+
+__global__ void k_set_mom(float* __restrict__ dst, const float* __restrict__ src, double scale,
+                          int64_t m) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m;
+         t += int64_t(gridDim.x) * blockDim.x)
+        dst[t] = float(double(src[t]) * scale);
+}
+
+// run_nbody.jl:148-149,164: X = mod(q + Psi + L, L) (or Psi), P = float((Mom/div)*mul).
+__global__ void k_output(const float* __restrict__ psi, const float* __restrict__ mom,
+                         const float* __restrict__ q1, int n, int64_t np, float L, int wrap,
+                         double pdiv, double pmul, float* __restrict__ xo, float* __restrict__ po) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < 3 * np;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int c = int(t / np);
+        const int64_t p = t - c * np;
+        if (xo) {
+            float x = psi[t];
+            if (wrap) {
+                const int ii = (c == 0) ? int(p % n) : (c == 1) ? int((p / n) % n) : int(p / (int64_t(n) * n));
+                x = x + q1[ii];
+                if (wrap == 1) x = jmodf(x + L, L);
+            }
+            xo[t] = x;
+        }
+        if (po) po[t] = float((double(mom[t]) / pdiv) * pmul);
+    }
+}
+
+// ── sheet resampling (pm.jl:186-234,426-464) ──────────────────────────────────
+// ψ_c = mod(X_c + s_c - q_c + L/2, L) - L/2 with X = q + Psi, written transposed to
+// [i][j][k] (k fastest, row padded to n+2) so that the in-place R2C halves the z
+// axis as the reference's rfft does (pm.jl:430-433).
+__global__ void k_wrap_psi(const float* __restrict__ psi, const float* __restrict__ q1, int n,
+                           int64_t np, float L, Shift3 s, int c, float* __restrict__ out,
+                           int padded) {
+    const int pitch = padded ? n + 2 : n;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < np;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        // t enumerates the output in [i][j][k] order (k fastest)
+        const int kk = int(t % n);
+        const int jj = int((t / n) % n);
+        const int ii = int(t / (int64_t(n) * n));
+        const int64_t p = ii + int64_t(n) * (jj + int64_t(n) * kk);  // input index, x fastest
+        const float sc = (c == 0) ? s.x : (c == 1) ? s.y : s.z;
+        const int qi = (c == 0) ? ii : (c == 1) ? jj : kk;
+        const float X = (psi[p + c * np] + q1[qi]) + sc;
+        const float v = jmodf((X - q1[qi]) + L / 2.0f, L) - L / 2.0f;
+        out[(int64_t(ii) * n + jj) * pitch + kk] = v;
+    }
+}
+
+// Phase shift of ψ̂ for a Lagrangian offset d (pm.jl:434-437,451-458): out =
+// ψ̂·px[i]·py[j]·pz[k]/n³ on the (n, n, n/2+1) spectrum [i][j][kz]. The kz = 0 and
+// kz = n/2 planes are made Hermitian ((H(k) + conj H(-k))/2), which is the value
+// a C2R that ignores the imaginary part of those planes after the full-axis
+// transforms produces from the raw product; it makes the result independent of
+// the C2R implementation.
+__global__ void k_phase(const float2* __restrict__ in, float2* __restrict__ out, int n,
+                        const float2* __restrict__ px, const float2* __restrict__ py,
+                        const float2* __restrict__ pz, float scale) {
+    const int nh = n / 2 + 1;
+    const int64_t total = int64_t(n) * n * nh;
+    auto cmul = [](float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int kz = int(t % nh);
+        const int j = int((t / nh) % n);
+        const int i = int(t / (int64_t(nh) * n));
+        float2 f = cmul(px[i], py[j]);
+        f = cmul(f, pz[kz]);
+        f.x *= scale;
+        f.y *= scale;
+        float2 h = cmul(in[t], f);
+        if (kz == 0 || kz == nh - 1) {
+            const int im = (n - i) % n, jm = (n - j) % n;
+            const int64_t tm = (int64_t(im) * n + jm) * nh + kz;
+            float2 fm = cmul(px[im], py[jm]);
+            fm = cmul(fm, pz[kz]);
+            fm.x *= scale;
+            fm.y *= scale;
+            const float2 hm = cmul(in[tm], fm);
+            h = make_float2(0.5f * (h.x + hm.x), 0.5f * (h.y - hm.y));
+        }
+        out[t] = h;
+    }
+}
+
+// Resampled positions X' = mod(q + ψ' + d·L/n + L, L) for the Fourier method
+// (pm.jl:438-441), ψ' in [i][j][k] padded layout, written to xr (3 blocks of n³,
+// same [i][j][k] order).
+__global__ void k_place(const float* __restrict__ rb, const float* __restrict__ q1, int n,
+                        int64_t np, float L, float shiftc, int c, float* __restrict__ xr) {
+    const int pitch = n + 2;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < np;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int kk = int(t % n);
+        const int jj = int((t / n) % n);
+        const int ii = int(t / (int64_t(n) * n));
+        const int qi = (c == 0) ? ii : (c == 1) ? jj : kk;
+        const float v = rb[(int64_t(ii) * n + jj) * pitch + kk];
+        xr[t + c * np] = jmodf(((q1[qi] + v) + shiftc) + L, L);
+    }
+}
+
+// Periodic trilinear resampling (pm.jl:207-212,220-231): ψ (x-fastest, 3 blocks)
+// interpolated at (i+dx, j+dy, k+dz), placed at q + ψ' + d·L/n, wrapped.
+__global__ void k_place_linear(const float* __restrict__ w, const float* __restrict__ q1, int n,
+                               int64_t np, float L, float dx, float dy, float dz, float sx,
+                               float sy, float sz, float* __restrict__ xr) {
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < np;
+         p += int64_t(gridDim.x) * blockDim.x) {
+        const int i = int(p % n);
+        const int j = int((p / n) % n);
+        const int k = int(p / (int64_t(n) * n));
+        const int i1 = (i + 1) % n, j1 = (j + 1) % n, k1 = (k + 1) % n;
+        auto at = [&](int a, int b, int cc) { return int64_t(a) + int64_t(n) * (b + int64_t(n) * cc); };
+        const float shifts[3] = {sx, sy, sz};
+        const int qi[3] = {i, j, k};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float* f = w + c * np;
+            const float v = f[at(i, j, k)] * (1 - dx) * (1 - dy) * (1 - dz) +
+                            f[at(i1, j, k)] * dx * (1 - dy) * (1 - dz) +
+                            f[at(i, j1, k)] * (1 - dx) * dy * (1 - dz) +
+                            f[at(i, j, k1)] * (1 - dx) * (1 - dy) * dz +
+                            f[at(i1, j1, k)] * dx * dy * (1 - dz) +
+                            f[at(i1, j, k1)] * dx * (1 - dy) * dz +
+                            f[at(i, j1, k1)] * (1 - dx) * dy * dz +
+                            f[at(i1, j1, k1)] * dx * dy * dz;
+            xr[p + c * np] = jmodf(((q1[qi[c]] + v) + shifts[c]) + L, L);
+        }
+    }
+}
+
+// ψ = mod(X + s - q + L/2, L) - L/2 in the particle layout (x fastest), 3 blocks.
+__global__ void k_wrap_psi_lin(const float* __restrict__ psi, const float* __restrict__ q1, int n,
+                               int64_t np, float L, Shift3 s, float* __restrict__ out) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < 3 * np;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int c = int(t / np);
+        const int64_t p = t - c * np;
+        const int qi = (c == 0) ? int(p % n) : (c == 1) ? int((p / n) % n) : int(p / (int64_t(n) * n));
+        const float sc = (c == 0) ? s.x : (c == 1) ? s.y : s.z;
+        const float X = (psi[t] + q1[qi]) + sc;
+        out[t] = jmodf((X - q1[qi]) + L / 2.0f, L) - L / 2.0f;
+    }
+}
+
+}  // namespace djb
+
+// ─────────────────────────────────────────────────────────────────────────────
+// solver object
+// ─────────────────────────────────────────────────────────────────────────────
+namespace {
+
+// Phases of a force evaluation, timed with CUDA events on the solver's stream.
+enum Phase { PH_CLEAR = 0, PH_SCATTER, PH_RESAMPLE, PH_R2C, PH_KSPACE, PH_C2R, PH_GATHER, PH_COUNT };
+
+// Launch counts of this library's kernels (always on) and, when enabled, per-phase
+// device time from event pairs recorded around each phase.
+struct Profiler {
+    bool on = false;
+    struct Rec {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Rec> recs;
+    size_t next = 0;
+    cudaEvent_t cur = nullptr;
+    int64_t launches[PH_COUNT] = {};
+    int64_t calls[PH_COUNT] = {};
+
+    cudaEvent_t take() {
+        if (next == pool.size()) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            pool.push_back(e);
+        }
+        return pool[next++];
+    }
+    void begin(cudaStream_t st, int ph) {
+        (void)ph;
+        if (!on) return;
+        cur = take();
+        if (cur) cudaEventRecord(cur, st);
+    }
+    void end(cudaStream_t st, int ph, int nlaunch) {
+        launches[ph] += nlaunch;
+        calls[ph] += 1;
+        if (!on || !cur) return;
+        cudaEvent_t b = take();
+        if (!b) return;
+        cudaEventRecord(b, st);
+        recs.push_back({ph, cur, b});
+        cur = nullptr;
+    }
+    void reset() {
+        recs.clear();
+        next = 0;
+        for (int i = 0; i < PH_COUNT; ++i) launches[i] = calls[i] = 0;
+    }
+    void destroy() {
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+        pool.clear();
+        recs.clear();
+        next = 0;
+    }
+};
+
+}  // namespace
+
+struct djb_solver {
+    Profiler prof;
+    djb_pm_config cfg{};
+    int n = 0, res = 0, pitch = 0, W = 2, R = 0;
+    int64_t np = 0;          // particles
+    int64_t mesh_floats = 0; // res*res*(res+2)
+    double L = 0;
+    float Lf = 0;
+    int nshift = 1, group = 1;
+    std::vector<double> shifts;     // 3 per shift
+    std::vector<double> rshifts;    // resampling offsets, 3 per offset
+    float c1 = 0, c2 = 0, c3 = 0;   // FD coefficients (pm.jl:419-424)
+    double s0 = 0;                  // Kφ scale
+
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cufftHandle r2c = 0, c2r = 0, r2c_n = 0, c2r_n = 0;
+    bool have_r2c = false, have_c2r = false, have_r2c_n = false, have_c2r_n = false;
+
+    float* psi = nullptr;
+    float* mom = nullptr;
+    float* acc = nullptr;
+    float* q1 = nullptr;
+    float* mesh[kMaxGroup] = {nullptr, nullptr};
+    float* fmesh[kMaxGroup][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    double* lapT = nullptr;
+    double* makT = nullptr;
+    float* gh = nullptr;
+    float* gf = nullptr;
+    // resampling work areas
+    float2* psihat = nullptr;   // 3 spectra (n, n, n/2+1)
+    float2* cb = nullptr;       // one spectrum
+    float* rb = nullptr;        // real n*n*(n+2) (in-place C2R)
+    float* xr = nullptr;        // 3*np resampled positions
+    float2* phase = nullptr;    // px, py, pz tables (n + n + n/2+1)
+    int* err = nullptr;
+    bool have_state = false;
+    int64_t bytes = 0;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+int dmalloc(djb_solver* s, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DJB_ERR_ALLOC, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    s->allocs.push_back(*p);
+    s->bytes += int64_t(bytes);
+    return DJB_OK;
+}
+
+#define TRY(expr)                 \
+    do {                          \
+        int rc_ = (expr);         \
+        if (rc_ != DJB_OK) return rc_; \
+    } while (0)
+
+int validate(const djb_pm_config& c) {
+    if (c.worder < 2 || c.worder > 4) return fail(DJB_ERR_INVALID, "worder must be 2, 3 or 4");
+    if (!(c.grad_order == 0 || c.grad_order == 2 || c.grad_order == 4 || c.grad_order == 6))
+        return fail(DJB_ERR_INVALID, "grad_order must be 0, 2, 4 or 6");
+    if (!(c.lap_order == 0 || c.lap_order == 2 || c.lap_order == 4 || c.lap_order == 6))
+        return fail(DJB_ERR_INVALID, "lap_order must be 0, 2, 4 or 6");
+    if (c.antialias < -1 || c.antialias > 3)
+        return fail(DJB_ERR_INVALID, "antialias must be -1, 0, 1, 2 or 3");
+    if (c.resampling != DJB_RESAMPLE_FOURIER && c.resampling != DJB_RESAMPLE_LINEAR)
+        return fail(DJB_ERR_INVALID, "resampling must be :fourier or :linear");
+    if (c.res_pm < 8 || (c.res_pm & 1))
+        return fail(DJB_ERR_INVALID, "res_pm must be even and >= 8 (got %d)", c.res_pm);
+    if (c.n_part < 2) return fail(DJB_ERR_INVALID, "n_part must be >= 2 (got %d)", c.n_part);
+    if (c.n_resample < 1) return fail(DJB_ERR_INVALID, "n_resample must be >= 1");
+    if (c.n_resample > 1 && c.resampling == DJB_RESAMPLE_FOURIER && (c.n_part & 1))
+        return fail(DJB_ERR_INVALID, "Fourier resampling needs an even n_part");
+    if (!(c.boxsize > 0.0)) return fail(DJB_ERR_INVALID, "boxsize must be positive");
+    if (c.lean && !(c.antialias == 0 && c.n_resample == 1 && c.grad_order != 0))
+        return fail(DJB_ERR_INVALID,
+                    "PMSolverLean supports antialias = 0, n_resample = 1 and finite-difference gradients (2/4/6)");
+    return DJB_OK;
+}
+
+int make_plan(cufftHandle* h, bool* have, int n, cufftType type, cudaStream_t st, size_t* work) {
+    CUFFT_TRY(cufftCreate(h));
+    *have = true;
+    long long dims[3] = {n, n, n};
+    long long rembed[3] = {n, n, 2 * (n / 2 + 1)};
+    long long cembed[3] = {n, n, n / 2 + 1};
+    const bool fwd = (type == CUFFT_R2C);
+    long long* inembed = fwd ? rembed : cembed;
+    long long* onembed = fwd ? cembed : rembed;
+    long long idist = inembed[0] * inembed[1] * inembed[2];
+    long long odist = onembed[0] * onembed[1] * onembed[2];
+    CUFFT_TRY(cufftMakePlanMany64(*h, 3, dims, inembed, 1, idist, onembed, 1, odist, type, 1, work));
+    CUFFT_TRY(cufftSetStream(*h, st));
+    return DJB_OK;
+}
+
+int grid_for(int64_t count) {
+    int64_t b = (count + kThreads - 1) / kThreads;
+    return int(std::min<int64_t>(b, 148LL * 64));
+}
+
+inline int blocks(int64_t count) { return int((count + kThreads - 1) / kThreads); }
+
+GroupShifts group_shifts(const djb_solver* s, int first, int ns) {
+    GroupShifts g{};
+    for (int i = 0; i < ns; ++i) {
+        g.s[i].x = float(s->shifts[3 * (first + i) + 0]);
+        g.s[i].y = float(s->shifts[3 * (first + i) + 1]);
+        g.s[i].z = float(s->shifts[3 * (first + i) + 2]);
+    }
+    return g;
+}
+
+template <int W, int NS>
+void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, float* m0,
+                      float* m1) {
+    djb::k_scatter<W, NS><<<blocks(s->np), kThreads, 0, s->stream>>>(
+        s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err);
+}
+
+void launch_scatter(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, int ns) {
+    float* m0 = s->mesh[0];
+    float* m1 = s->mesh[1];
+#define DJB_SC(W_)                                                        \
+    if (s->W == W_) {                                                      \
+        if (ns == 1) launch_scatter_t<W_, 1>(s, mom, dd1, g, m0, m1);       \
+        else launch_scatter_t<W_, 2>(s, mom, dd1, g, m0, m1);               \
+    }
+    DJB_SC(2) DJB_SC(3) DJB_SC(4)
+#undef DJB_SC
+}
+
+void launch_scatter_positions(djb_solver* s, const float* xr, int64_t count, float* mesh) {
+    const int b = blocks(count);
+    if (s->W == 2) djb::k_scatter_positions<2><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, s->pitch, mesh, s->err);
+    if (s->W == 3) djb::k_scatter_positions<3><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, s->pitch, mesh, s->err);
+    if (s->W == 4) djb::k_scatter_positions<4><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, s->pitch, mesh, s->err);
+}
+
+template <int W, int R>
+void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
+    if (ns == 1) djb::k_gather<W, R, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(a);
+    else djb::k_gather<W, R, 2><<<blocks(s->np), kThreads, 0, s->stream>>>(a);
+}
+
+template <int W>
+void launch_gather_w(djb_solver* s, const djb::GatherArgs& a, int ns) {
+    switch (s->R) {
+        case 0: launch_gather_wr<W, 0>(s, a, ns); break;
+        case 1: launch_gather_wr<W, 1>(s, a, ns); break;
+        case 2: launch_gather_wr<W, 2>(s, a, ns); break;
+        default: launch_gather_wr<W, 3>(s, a, ns); break;
+    }
+}
+
+void launch_gather(djb_solver* s, const djb::GatherArgs& a, int ns) {
+    if (s->W == 2) launch_gather_w<2>(s, a, ns);
+    else if (s->W == 3) launch_gather_w<3>(s, a, ns);
+    else launch_gather_w<4>(s, a, ns);
+}
+
+// Extra particle sets of the Lagrangian sheet for shift `si`, deposited into `mesh`
+// (pm.jl:471-484).
+int resample_deposit(djb_solver* s, int si, float* mesh) {
+    const int n = s->n;
+    const int64_t np = s->np;
+    const Shift3 sh{float(s->shifts[3 * si]), float(s->shifts[3 * si + 1]), float(s->shifts[3 * si + 2])};
+    const int nh = n / 2 + 1;
+    const int64_t nspec = int64_t(n) * n * nh;
+    const int64_t nreal = int64_t(n) * n * (n + 2);
+    const int nof = int(s->rshifts.size() / 3);
+    if (s->cfg.resampling == DJB_RESAMPLE_FOURIER) {
+        for (int c = 0; c < 3; ++c) {
+            djb::k_wrap_psi<<<grid_for(np), kThreads, 0, s->stream>>>(s->psi, s->q1, n, np, s->Lf, sh, c, s->rb, 1);
+            CUFFT_TRY(cufftExecR2C(s->r2c_n, s->rb, reinterpret_cast<cufftComplex*>(s->psihat + c * nspec)));
+        }
+        for (int o = 0; o < nof; ++o) {
+            const double d[3] = {s->rshifts[3 * o], s->rshifts[3 * o + 1], s->rshifts[3 * o + 2]};
+            const float2* px = s->phase + int64_t(o) * (2 * n + nh);
+            for (int c = 0; c < 3; ++c) {
+                djb::k_phase<<<grid_for(nspec), kThreads, 0, s->stream>>>(
+                    s->psihat + c * nspec, s->cb, n, px, px + n, px + 2 * n, float(1.0 / (double(n) * n * n)));
+                CUFFT_TRY(cufftExecC2R(s->c2r_n, reinterpret_cast<cufftComplex*>(s->cb), s->rb));
+                djb::k_place<<<grid_for(np), kThreads, 0, s->stream>>>(
+                    s->rb, s->q1, n, np, s->Lf, float(d[c] * s->cfg.boxsize / n), c, s->xr);
+            }
+            launch_scatter_positions(s, s->xr, np, mesh);
+        }
+        (void)nreal;
+    } else {
+        djb::k_wrap_psi_lin<<<grid_for(3 * np), kThreads, 0, s->stream>>>(s->psi, s->q1, n, np, s->Lf, sh, s->rb);
+        for (int o = 0; o < nof; ++o) {
+            const double* d = &s->rshifts[3 * o];
+            djb::k_place_linear<<<grid_for(np), kThreads, 0, s->stream>>>(
+                s->rb, s->q1, n, np, s->Lf, float(d[0]), float(d[1]), float(d[2]),
+                float(d[0] * s->cfg.boxsize / n), float(d[1] * s->cfg.boxsize / n),
+                float(d[2] * s->cfg.boxsize / n), s->xr);
+            launch_scatter_positions(s, s->xr, np, mesh);
+        }
+    }
+    return DJB_OK;
+}
+
+// Force evaluation for all shifts; if `step`, fused with the drift/kick/drift.
+// Reads s->psi (and s->mom). Output: s->acc (step == 0) or updated psi/mom.
+int force(djb_solver* s, bool step, double dd1, double alpha, double beta, double dd2) {
+    const int nh = s->res / 2 + 1;
+    const int64_t nspec = int64_t(s->res) * s->res * nh;
+    const bool ik = (s->cfg.grad_order == 0);
+    const bool resample = (s->cfg.n_resample > 1);
+    for (int first = 0; first < s->nshift; first += s->group) {
+        const int ns = std::min(s->group, s->nshift - first);
+        const GroupShifts g = group_shifts(s, first, ns);
+        s->prof.begin(s->stream, PH_CLEAR);
+        for (int m = 0; m < ns; ++m)
+            CUDA_TRY(cudaMemsetAsync(s->mesh[m], 0, size_t(s->mesh_floats) * sizeof(float), s->stream));
+        s->prof.end(s->stream, PH_CLEAR, 0);
+        const bool drift_here = step && first == 0;
+        s->prof.begin(s->stream, PH_SCATTER);
+        launch_scatter(s, drift_here ? s->mom : nullptr, float(dd1), g, ns);
+        s->prof.end(s->stream, PH_SCATTER, 1);
+        if (resample) {
+            s->prof.begin(s->stream, PH_RESAMPLE);
+            TRY(resample_deposit(s, first, s->mesh[0]));
+            s->prof.end(s->stream, PH_RESAMPLE, 0);
+        }
+        for (int m = 0; m < ns; ++m) {
+            float* mesh = s->mesh[m];
+            cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
+            s->prof.begin(s->stream, PH_R2C);
+            CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
+            s->prof.end(s->stream, PH_R2C, 0);
+            if (!ik) {
+                s->prof.begin(s->stream, PH_KSPACE);
+                djb::k_kspace_mul<<<grid_for(nspec), kThreads, 0, s->stream>>>(
+                    reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
+                s->prof.end(s->stream, PH_KSPACE, 1);
+                s->prof.begin(s->stream, PH_C2R);
+                CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
+                s->prof.end(s->stream, PH_C2R, 0);
+            } else {
+                s->prof.begin(s->stream, PH_KSPACE);
+                djb::k_kspace_ik<<<grid_for(nspec), kThreads, 0, s->stream>>>(
+                    reinterpret_cast<const float2*>(mesh), s->res, s->lapT, s->makT, s->s0, s->gh, s->gf,
+                    reinterpret_cast<float2*>(s->fmesh[m][0]), reinterpret_cast<float2*>(s->fmesh[m][1]),
+                    reinterpret_cast<float2*>(s->fmesh[m][2]));
+                s->prof.end(s->stream, PH_KSPACE, 1);
+                s->prof.begin(s->stream, PH_C2R);
+                for (int c = 0; c < 3; ++c)
+                    CUFFT_TRY(cufftExecC2R(s->c2r, reinterpret_cast<cufftComplex*>(s->fmesh[m][c]),
+                                           s->fmesh[m][c]));
+                s->prof.end(s->stream, PH_C2R, 0);
+            }
+        }
+        djb::GatherArgs a{};
+        a.psi = s->psi;
+        a.mom = s->mom;
+        a.acc = s->acc;
+        a.q1 = s->q1;
+        for (int m = 0; m < ns; ++m) {
+            a.mesh[m] = ik ? s->fmesh[m][0] : s->mesh[m];
+            a.meshy[m] = ik ? s->fmesh[m][1] : nullptr;
+            a.meshz[m] = ik ? s->fmesh[m][2] : nullptr;
+        }
+        a.sh = g;
+        a.n = s->n;
+        a.np = s->np;
+        a.L = s->Lf;
+        a.res = s->res;
+        a.pitch = s->pitch;
+        a.c1 = s->c1;
+        a.c2 = s->c2;
+        a.c3 = s->c3;
+        a.first = (first == 0);
+        a.last = (first + ns >= s->nshift);
+        a.divide = (s->nshift > 1);
+        a.nshift_f = float(s->nshift);
+        a.step = step ? 1 : 0;
+        a.alpha = float(alpha);
+        a.beta = float(beta);
+        a.dd2 = float(dd2);
+        a.err = s->err;
+        s->prof.begin(s->stream, PH_GATHER);
+        launch_gather(s, a, ns);
+        s->prof.end(s->stream, PH_GATHER, 1);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+int check_err(djb_solver* s) {
+    int h = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (h) {
+        CUDA_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->stream));
+        return fail(DJB_ERR_DEVICE, "non-finite particle position encountered (device error word %d)", h);
+    }
+    return DJB_OK;
+}
+
+int copy_in(djb_solver* s, float* dst, const float* src, size_t count, int mem) {
+    CUDA_TRY(cudaMemcpyAsync(dst, src, count * sizeof(float),
+                             mem == DJB_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                             s->stream));
+    return DJB_OK;
+}
+
+int copy_out(djb_solver* s, float* dst, const float* src, size_t count, int mem) {
+    CUDA_TRY(cudaMemcpyAsync(dst, src, count * sizeof(float),
+                             mem == DJB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                             s->stream));
+    return DJB_OK;
+}
+
+void release(djb_solver* s) {
+    if (!s) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->cfg.device);
+    s->prof.destroy();
+    if (s->have_r2c) cufftDestroy(s->r2c);
+    if (s->have_c2r) cufftDestroy(s->c2r);
+    if (s->have_r2c_n) cufftDestroy(s->r2c_n);
+    if (s->have_c2r_n) cufftDestroy(s->c2r_n);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    if (prev >= 0) cudaSetDevice(prev);
+    delete s;
+}
+
+int create(const djb_pm_config* cfg, djb_solver** out) {
+    TRY(validate(*cfg));
+    djb_solver* s = new (std::nothrow) djb_solver();
+    if (!s) return fail(DJB_ERR_ALLOC, "host allocation failed");
+    *out = s;
+    s->cfg = *cfg;
+    CUDA_TRY(cudaSetDevice(cfg->device));
+    s->n = cfg->n_part;
+    s->res = cfg->res_pm;
+    s->pitch = s->res + 2;
+    s->np = int64_t(s->n) * s->n * s->n;
+    s->mesh_floats = int64_t(s->res) * s->res * s->pitch;
+    s->L = cfg->boxsize;
+    s->Lf = float(cfg->boxsize);
+    s->W = cfg->worder;
+    s->R = cfg->grad_order / 2;
+    s->shifts = aa_shifts(cfg->antialias, 0.5 * s->L / s->res);
+    s->nshift = int(s->shifts.size() / 3);
+    const bool resample = cfg->n_resample > 1;
+    const bool ik = cfg->grad_order == 0;
+    s->group = resample ? 1 : std::min(kMaxGroup, s->nshift);
+    if (resample) s->rshifts = resample_shifts(cfg->n_resample);
+    if (!ik) {
+        // pm.jl:419-424 in float64, rounded to float like T.(...)
+        const double h = s->L / s->res;
+        double d1 = 0, d2 = 0, d3 = 0;
+        if (cfg->grad_order == 2) d1 = 1 / (2 * h);
+        if (cfg->grad_order == 4) { d1 = 8 / (12 * h); d2 = -1 / (12 * h); }
+        if (cfg->grad_order == 6) { d1 = 45 / (60 * h); d2 = -9 / (60 * h); d3 = 1 / (60 * h); }
+        s->c1 = float(d1);
+        s->c2 = float(d2);
+        s->c3 = float(d3);
+    }
+    CUDA_TRY(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+    s->stream = s->own_stream;
+
+    // 1-D tables (float64): lap terms, deconvolution, ik gradient
+    const int res = s->res;
+    std::vector<double> T(res), M(res);
+    const double dk = 2 * M_PI / s->L;
+    const double mm = (res / 2) * dk / M_PI;  // maximum(abs.(k))/π = res/L
+    for (int i = 0; i < res; ++i) {
+        const double k = (i < res / 2 ? i : i - res) * 2 * M_PI / s->L;
+        if (cfg->lap_order == 0) {
+            T[i] = -(k * k);
+        } else {
+            const double c1 = std::cos(k / mm), c2 = std::cos(2 * k / mm), c3 = std::cos(3 * k / mm);
+            if (cfg->lap_order == 2) T[i] = -2 * (1 - c1) * mm * mm;
+            if (cfg->lap_order == 4) T[i] = -(c2 - 16 * c1 + 15) / 6 * (mm * mm);
+            if (cfg->lap_order == 6) T[i] = -(-2 * c3 + 27 * c2 - 270 * c1 + 245) / 90 * (mm * mm);
+        }
+        const double x = k / (2 * M_PI) / mm;
+        const double sinc = (x == 0) ? 1.0 : std::sin(M_PI * x) / (M_PI * x);
+        M[i] = std::pow(sinc, -2.0 * cfg->worder);
+    }
+    // The 1-D tables serve the halved axis too: every term is even in k.
+    const double rhomean = double(s->np) / (double(res) * res * res);
+    const double nsets = double(cfg->n_resample) * cfg->n_resample * cfg->n_resample;
+    s->s0 = 1.0 / rhomean / nsets / (double(res) * res * res);
+    TRY(dmalloc(s, (void**)&s->lapT, sizeof(double) * res));
+    CUDA_TRY(cudaMemcpy(s->lapT, T.data(), sizeof(double) * res, cudaMemcpyHostToDevice));
+    if (cfg->deconvolve) {
+        TRY(dmalloc(s, (void**)&s->makT, sizeof(double) * res));
+        CUDA_TRY(cudaMemcpy(s->makT, M.data(), sizeof(double) * res, cudaMemcpyHostToDevice));
+    }
+    if (ik) {
+        std::vector<float> gh(res / 2 + 1), gf(res);
+        for (int m = 0; m <= res / 2; ++m) gh[m] = (m == res / 2) ? 0.0f : float(m * 2 * M_PI / s->L);
+        for (int m = 0; m < res; ++m) gf[m] = (m == res / 2) ? 0.0f : float((m < res / 2 ? m : m - res) * 2 * M_PI / s->L);
+        TRY(dmalloc(s, (void**)&s->gh, sizeof(float) * gh.size()));
+        TRY(dmalloc(s, (void**)&s->gf, sizeof(float) * gf.size()));
+        CUDA_TRY(cudaMemcpy(s->gh, gh.data(), sizeof(float) * gh.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(s->gf, gf.data(), sizeof(float) * gf.size(), cudaMemcpyHostToDevice));
+    }
+    // lattice coordinates (pm.jl:186): float(i * (L/n))
+    std::vector<float> q(s->n);
+    for (int i = 0; i < s->n; ++i) q[i] = float(i * (s->L / s->n));
+    TRY(dmalloc(s, (void**)&s->q1, sizeof(float) * s->n));
+    CUDA_TRY(cudaMemcpy(s->q1, q.data(), sizeof(float) * s->n, cudaMemcpyHostToDevice));
+
+    const size_t pbytes = size_t(3 * s->np) * sizeof(float);
+    TRY(dmalloc(s, (void**)&s->psi, pbytes));
+    TRY(dmalloc(s, (void**)&s->mom, pbytes));
+    TRY(dmalloc(s, (void**)&s->acc, pbytes));
+    for (int m = 0; m < s->group; ++m) {
+        TRY(dmalloc(s, (void**)&s->mesh[m], size_t(s->mesh_floats) * sizeof(float)));
+        if (ik)
+            for (int c = 0; c < 3; ++c)
+                TRY(dmalloc(s, (void**)&s->fmesh[m][c], size_t(s->mesh_floats) * sizeof(float)));
+    }
+    TRY(dmalloc(s, (void**)&s->err, sizeof(int)));
+    CUDA_TRY(cudaMemset(s->err, 0, sizeof(int)));
+    size_t work = 0;
+    TRY(make_plan(&s->r2c, &s->have_r2c, res, CUFFT_R2C, s->stream, &work));
+    s->bytes += int64_t(work);
+    TRY(make_plan(&s->c2r, &s->have_c2r, res, CUFFT_C2R, s->stream, &work));
+    s->bytes += int64_t(work);
+    if (resample) {
+        const int n = s->n, nh = n / 2 + 1;
+        const int64_t nspec = int64_t(n) * n * nh;
+        TRY(dmalloc(s, (void**)&s->rb, sizeof(float) * std::max<int64_t>(int64_t(n) * n * (n + 2), 3 * s->np)));
+        TRY(dmalloc(s, (void**)&s->xr, pbytes));
+        if (cfg->resampling == DJB_RESAMPLE_FOURIER) {
+            TRY(dmalloc(s, (void**)&s->psihat, sizeof(float2) * 3 * nspec));
+            TRY(dmalloc(s, (void**)&s->cb, sizeof(float2) * nspec));
+            // phase tables exp(2πi m d/n) per offset (pm.jl:453-456); full axes hold
+            // -n/2 at index n/2, the halved axis m/n for m = 0..n/2
+            const int nof = int(s->rshifts.size() / 3);
+            std::vector<float2> h(size_t(nof) * (2 * n + nh));
+            for (int o = 0; o < nof; ++o) {
+                const double* d = &s->rshifts[3 * o];
+                float2* t = &h[size_t(o) * (2 * n + nh)];
+                for (int m = 0; m < n; ++m) {
+                    const double mf = double(m < n / 2 ? m : m - n) / n;
+                    t[m] = make_float2(float(std::cos(2 * M_PI * mf * d[0])), float(std::sin(2 * M_PI * mf * d[0])));
+                    t[n + m] = make_float2(float(std::cos(2 * M_PI * mf * d[1])), float(std::sin(2 * M_PI * mf * d[1])));
+                }
+                for (int m = 0; m < nh; ++m) {
+                    const double mh = double(m) / n;
+                    t[2 * n + m] = make_float2(float(std::cos(2 * M_PI * mh * d[2])), float(std::sin(2 * M_PI * mh * d[2])));
+                }
+            }
+            TRY(dmalloc(s, (void**)&s->phase, sizeof(float2) * h.size()));
+            CUDA_TRY(cudaMemcpy(s->phase, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
+            TRY(make_plan(&s->r2c_n, &s->have_r2c_n, n, CUFFT_R2C, s->stream, &work));
+            s->bytes += int64_t(work);
+            TRY(make_plan(&s->c2r_n, &s->have_c2r_n, n, CUFFT_C2R, s->stream, &work));
+            s->bytes += int64_t(work);
+        }
+    }
+    return DJB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* djb_version(void) { return "djb200 0.1 (sm_100a)"; }
+
+int djb_solver_create(const djb_pm_config* cfg, djb_solver** out) {
+    djb::clear_error();
+    if (!cfg || !out) return fail(DJB_ERR_INVALID, "djb_solver_create: null argument");
+    *out = nullptr;
+    djb_solver* s = nullptr;
+    int rc = create(cfg, &s);
+    if (rc != DJB_OK) {
+        std::string msg = djb_last_error();
+        release(s);
+        return fail(rc, "%s", msg.c_str());
+    }
+    *out = s;
+    return DJB_OK;
+}
+
+int djb_solver_destroy(djb_solver* s) {
+    release(s);
+    return DJB_OK;
+}
+
+int djb_solver_set_stream(djb_solver* s, void* stream) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    s->stream = stream ? static_cast<cudaStream_t>(stream) : s->own_stream;
+    if (s->have_r2c) CUFFT_TRY(cufftSetStream(s->r2c, s->stream));
+    if (s->have_c2r) CUFFT_TRY(cufftSetStream(s->c2r, s->stream));
+    if (s->have_r2c_n) CUFFT_TRY(cufftSetStream(s->r2c_n, s->stream));
+    if (s->have_c2r_n) CUFFT_TRY(cufftSetStream(s->c2r_n, s->stream));
+    return DJB_OK;
+}
+
+int djb_solver_device_bytes(const djb_solver* s, int64_t* bytes) {
+    if (!s || !bytes) return fail(DJB_ERR_INVALID, "null argument");
+    *bytes = s->bytes;
+    return DJB_OK;
+}
+
+int djb_pm_acceleration(djb_solver* s, const float* psi, float* acc, int32_t mem) {
+    djb::clear_error();
+    if (!s || !psi || !acc) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    // The displacements are staged in a stream-ordered buffer so that the resident
+    // particle state of run_nbody survives a force call (pm.jl:507-521 uses S.X).
+    float* saved = s->psi;
+    float* stage = nullptr;
+    const size_t count = size_t(3 * s->np);
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&stage), count * sizeof(float), s->stream);
+    if (e != cudaSuccess) return fail(DJB_ERR_ALLOC, "staging allocation failed: %s", cudaGetErrorString(e));
+    int rc = copy_in(s, stage, psi, count, mem);
+    if (rc == DJB_OK) {
+        s->psi = stage;
+        rc = force(s, false, 0, 0, 0, 0);
+        s->psi = saved;
+    }
+    if (rc == DJB_OK) rc = copy_out(s, acc, s->acc, count, mem);
+    cudaFreeAsync(stage, s->stream);
+    if (rc != DJB_OK) return rc;
+    return check_err(s);
+}
+
+int djb_set_state(djb_solver* s, const float* psi, const float* mom, double mom_scale, int32_t mem) {
+    djb::clear_error();
+    if (!s || !psi || !mom) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    TRY(copy_in(s, s->psi, psi, count, mem));
+    if (mom_scale == 1.0) {
+        TRY(copy_in(s, s->mom, mom, count, mem));
+    } else {
+        TRY(copy_in(s, s->acc, mom, count, mem));
+        djb::k_set_mom<<<grid_for(count), kThreads, 0, s->stream>>>(s->mom, s->acc, mom_scale, int64_t(count));
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->have_state = true;
+    return DJB_OK;
+}
+
+int djb_get_state(djb_solver* s, float* psi, float* mom, int32_t mem) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    if (!s->have_state) return fail(DJB_ERR_STATE, "no particle state set");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    if (psi) TRY(copy_out(s, psi, s->psi, count, mem));
+    if (mom) TRY(copy_out(s, mom, s->mom, count, mem));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return check_err(s);
+}
+
+int djb_step(djb_solver* s, double dd1, double alpha, double beta, double dd2) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    if (!s->have_state) return fail(DJB_ERR_STATE, "no particle state set");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    if (s->cfg.n_resample > 1) {
+        // Resampling reads the drifted positions per shift; drift first, then the
+        // unfused force and kick-drift.
+        djb::k_drift<<<grid_for(3 * s->np), kThreads, 0, s->stream>>>(s->psi, s->mom, float(dd1), 3 * s->np);
+        TRY(force(s, false, 0, 0, 0, 0));
+        djb::k_kick_drift<<<grid_for(3 * s->np), kThreads, 0, s->stream>>>(
+            s->psi, s->mom, s->acc, float(alpha), float(beta), float(dd2), 3 * s->np);
+        CUDA_TRY(cudaGetLastError());
+        return DJB_OK;
+    }
+    return force(s, true, dd1, alpha, beta, dd2);
+}
+
+int djb_run(djb_solver* s, int32_t n_steps, const double* dd1, const double* alpha, const double* beta,
+            const double* dd2) {
+    djb::clear_error();
+    if (!s || !dd1 || !alpha || !beta || !dd2) return fail(DJB_ERR_INVALID, "null argument");
+    for (int k = 0; k < n_steps; ++k) TRY(djb_step(s, dd1[k], alpha[k], beta[k], dd2[k]));
+    return djb_synchronize(s);
+}
+
+int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wrap, double p_div, double p_mul,
+                   int32_t mem) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    if (!s->have_state) return fail(DJB_ERR_STATE, "no particle state set");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    float* xo = nullptr;
+    float* po = nullptr;
+    float* stage = nullptr;
+    if (mem == DJB_MEM_HOST) {
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&stage), 2 * count * sizeof(float), s->stream);
+        if (e != cudaSuccess) return fail(DJB_ERR_ALLOC, "staging allocation failed: %s", cudaGetErrorString(e));
+        xo = x_out ? stage : nullptr;
+        po = p_out ? stage + count : nullptr;
+    } else {
+        xo = x_out;
+        po = p_out;
+    }
+    djb::k_output<<<grid_for(count), kThreads, 0, s->stream>>>(s->psi, s->mom, s->q1, s->n, s->np, s->Lf, wrap,
+                                                               p_div, p_mul, xo, po);
+    int rc = DJB_OK;
+    if (cudaGetLastError() != cudaSuccess) rc = fail(DJB_ERR_CUDA, "output kernel launch failed");
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) {
+        if (x_out) rc = copy_out(s, x_out, xo, count, DJB_MEM_HOST);
+        if (rc == DJB_OK && p_out) rc = copy_out(s, p_out, po, count, DJB_MEM_HOST);
+    }
+    if (stage) cudaFreeAsync(stage, s->stream);
+    if (rc != DJB_OK) return rc;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return check_err(s);
+}
+
+int djb_solver_profile(djb_solver* s, int32_t enable) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->prof.reset();
+    s->prof.on = enable != 0;
+    return DJB_OK;
+}
+
+int djb_solver_profile_read(djb_solver* s, double* ms, int64_t* launches, int64_t* calls, int32_t nphase) {
+    djb::clear_error();
+    if (!s || !ms || !launches || !calls) return fail(DJB_ERR_INVALID, "null argument");
+    if (nphase < PH_COUNT) return fail(DJB_ERR_INVALID, "need room for %d phases", int(PH_COUNT));
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    for (int i = 0; i < nphase; ++i) {
+        ms[i] = 0.0;
+        launches[i] = i < PH_COUNT ? s->prof.launches[i] : 0;
+        calls[i] = i < PH_COUNT ? s->prof.calls[i] : 0;
+    }
+    for (const auto& r : s->prof.recs) {
+        float t = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&t, r.a, r.b));
+        ms[r.phase] += double(t);
+    }
+    s->prof.reset();
+    return DJB_OK;
+}
+
+int djb_synchronize(djb_solver* s) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    CUDA_TRY(cudaGetLastError());
+    return check_err(s);
+}
+
+}  // extern "C"
+
+// Exposed to power.cu: the solver's CIC deposit of its state for P(k).
+namespace djb {
+cufftHandle solver_r2c(const djb_solver* s) { return s->r2c; }
+double solver_boxsize(const djb_solver* s) { return s->L; }
+int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cudaStream_t* st) {
+    if (!s->have_state) return fail(DJB_ERR_STATE, "no particle state set");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    CUDA_TRY(cudaMemsetAsync(s->mesh[0], 0, size_t(s->mesh_floats) * sizeof(float), s->stream));
+    GroupShifts g{};
+    launch_scatter_t<2, 1>(s, nullptr, 0.0f, g, s->mesh[0], nullptr);
+    CUDA_TRY(cudaGetLastError());
+    *mesh_out = s->mesh[0];
+    *res = s->res;
+    *pitch = s->pitch;
+    *st = s->stream;
+    return DJB_OK;
+}
+int64_t solver_np(const djb_solver* s) { return s->np; }
+}  // namespace djb

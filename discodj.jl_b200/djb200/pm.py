@@ -1,0 +1,215 @@
+"""PM force on the B200: `PMConfig`, `PMSolver`, `pm_acceleration`.
+
+Mirrors native/DiscoDJNative/src/nbody/pm.jl:28-46,366-414,503-529,545-585 on top
+of libdjb200's C ABI. Arrays follow the reference's logical layout: particle
+fields are (n,n,n,3) indexed [i,j,k,c]. Host arrays are numpy (any order; they
+are converted to the column-major float32 memory the C ABI takes). Device arrays
+are torch CUDA tensors in that memory layout, i.e. shape (3,n,n,n) contiguous
+indexed [c,k,j,i] (`native_view`/`logical_view` convert).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import MEM_DEVICE, MEM_HOST, check, lib
+
+
+@dataclass
+class PMConfig:
+    """pm.jl:35-46 (keyword names and defaults as there)."""
+    res_pm: int
+    n_part: int
+    boxsize: float
+    worder: int = 2
+    deconvolve: bool = False
+    antialias: int = 0
+    grad_order: int = 4
+    lap_order: int = 0
+    n_resample: int = 1
+    resampling: str = "fourier"
+
+    def to_c(self, lean: bool = False, device: int = 0) -> _lib.PMConfigC:
+        if self.resampling not in _lib.RESAMPLING:
+            raise _lib.DJBInvalidOption(_lib.DJB_ERR_INVALID, "resampling must be :fourier or :linear")
+        return _lib.PMConfigC(int(self.res_pm), int(self.n_part), float(self.boxsize), int(self.worder),
+                              int(bool(self.deconvolve)), int(self.antialias), int(self.grad_order),
+                              int(self.lap_order), int(self.n_resample), _lib.RESAMPLING[self.resampling],
+                              int(bool(lean)), int(device))
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def native_host(a, n: int) -> np.ndarray:
+    """(n,n,n,3) logical array -> float32 numpy in the C ABI's memory order."""
+    a = np.asarray(a)
+    if a.shape != (n, n, n, 3):
+        raise ValueError(f"expected a ({n},{n},{n},3) particle array, got {a.shape}")
+    return np.asfortranarray(a, dtype=np.float32)
+
+
+def native_view(t):
+    """(n,n,n,3) torch tensor -> contiguous (3,n,n,n) tensor with the C ABI's memory order."""
+    return t.permute(3, 2, 1, 0).contiguous()
+
+
+def logical_view(t):
+    """Inverse of `native_view`: (3,n,n,n) -> (n,n,n,3) view."""
+    return t.permute(3, 2, 1, 0)
+
+
+def _ptr_mem(x, n: int):
+    """(pointer, mem kind, keep-alive) for a particle array argument."""
+    if _is_torch(x):
+        if x.dtype.__repr__() != "torch.float32" or not x.is_contiguous() or tuple(x.shape) != (3, n, n, n):
+            raise ValueError("device particle arrays must be contiguous float32 (3,n,n,n) tensors "
+                             "(use djb200.native_view)")
+        if x.is_cuda:
+            return C.c_void_p(x.data_ptr()), MEM_DEVICE, x
+        x = x.numpy()
+        return C.c_void_p(x.ctypes.data), MEM_HOST, x
+    h = native_host(x, n)
+    return C.c_void_p(h.ctypes.data), MEM_HOST, h
+
+
+class PMSolver:
+    """B200 PM workspace (`PMSolver` / `PMSolverLean`, pm.jl:371-414,547-585).
+
+    Owns the device meshes, cuFFT plans and the resident particle state."""
+
+    def __init__(self, cfg: PMConfig, like=None, *, lean: bool = False, device: int = 0):
+        self.cfg = cfg
+        self.lean = lean
+        self.device = device
+        self.n = int(cfg.n_part)
+        c = cfg.to_c(lean=lean, device=device)
+        h = C.c_void_p()
+        check(lib.djb_solver_create(C.byref(c), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.djb_solver_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def device_bytes(self) -> int:
+        v = C.c_int64()
+        check(lib.djb_solver_device_bytes(self._h, C.byref(v)))
+        return v.value
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib.djb_solver_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    # pm_acceleration!(S, psi)
+    def acceleration(self, psi, out=None):
+        n = self.n
+        p, mem, keep = _ptr_mem(psi, n)
+        if out is None:
+            if mem == MEM_DEVICE:
+                import torch
+                out = torch.empty((3, n, n, n), dtype=torch.float32, device=psi.device)
+            else:
+                out = np.empty((n, n, n, 3), dtype=np.float32, order="F")
+        optr = C.c_void_p(out.data_ptr()) if _is_torch(out) else C.c_void_p(out.ctypes.data)
+        if _is_torch(out) != (mem == MEM_DEVICE) or (not _is_torch(out) and not out.flags.f_contiguous):
+            raise ValueError("out must match psi's memory kind and layout")
+        check(lib.djb_pm_acceleration(self._h, p, optr, mem))
+        del keep
+        return out
+
+    def set_state(self, psi, mom, mom_scale: float = 1.0):
+        n = self.n
+        p, mem, k1 = _ptr_mem(psi, n)
+        m, mem2, k2 = _ptr_mem(mom, n)
+        if mem != mem2:
+            raise ValueError("psi and mom must live in the same memory")
+        check(lib.djb_set_state(self._h, p, m, float(mom_scale), mem))
+        del k1, k2
+
+    def get_state(self, device: bool = False):
+        n = self.n
+        if device:
+            import torch
+            psi = torch.empty((3, n, n, n), dtype=torch.float32, device=f"cuda:{self.device}")
+            mom = torch.empty_like(psi)
+            check(lib.djb_get_state(self._h, C.c_void_p(psi.data_ptr()), C.c_void_p(mom.data_ptr()), MEM_DEVICE))
+            return psi, mom
+        psi = np.empty((n, n, n, 3), dtype=np.float32, order="F")
+        mom = np.empty((n, n, n, 3), dtype=np.float32, order="F")
+        check(lib.djb_get_state(self._h, C.c_void_p(psi.ctypes.data), C.c_void_p(mom.ctypes.data), MEM_HOST))
+        return psi, mom
+
+    def step(self, dd1: float, alpha: float, beta: float, dd2: float):
+        check(lib.djb_step(self._h, float(dd1), float(alpha), float(beta), float(dd2)))
+
+    def run(self, dd1, alpha, beta, dd2):
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (dd1, alpha, beta, dd2)]
+        check(lib.djb_run(self._h, len(arrs[0]), *[_lib.dptr(a) for a in arrs]))
+
+    def synchronize(self):
+        check(lib.djb_synchronize(self._h))
+
+    PHASES = ("clear", "scatter", "resample", "r2c", "kspace", "c2r", "gather")
+
+    def profile(self, enable: bool = True):
+        """Start (or stop) per-phase CUDA-event timing; resets the sums."""
+        check(lib.djb_solver_profile(self._h, int(bool(enable))))
+
+    def profile_read(self) -> dict:
+        """{phase: (ms, kernel launches, executions)} since the last read; resets."""
+        n = 8
+        ms = np.zeros(n)
+        la = np.zeros(n, dtype=np.int64)
+        ca = np.zeros(n, dtype=np.int64)
+        check(lib.djb_solver_profile_read(self._h, _lib.dptr(ms), _lib.i64ptr(la), _lib.i64ptr(ca), n))
+        return {name: (float(ms[i]), int(la[i]), int(ca[i])) for i, name in enumerate(self.PHASES)}
+
+    def output(self, wrap: bool, p_div: float = 1.0, p_mul: float = 1.0, x=True, p=True):
+        n = self.n
+        xo = np.empty((n, n, n, 3), dtype=np.float32, order="F") if x else None
+        po = np.empty((n, n, n, 3), dtype=np.float32, order="F") if p else None
+        check(lib.djb_get_output(self._h, C.c_void_p(xo.ctypes.data) if x else None,
+                                 C.c_void_p(po.ctypes.data) if p else None, int(wrap),
+                                 float(p_div), float(p_mul), MEM_HOST))
+        return xo, po
+
+    def state_power_spectrum(self, bins: int = 32, logarithmic: bool = True):
+        k = np.empty(bins)
+        pk = np.empty(bins)
+        nm = np.empty(bins, dtype=np.int64)
+        check(lib.djb_state_power_spectrum(self._h, int(bins), int(bool(logarithmic)), _lib.dptr(k),
+                                           _lib.dptr(pk), _lib.i64ptr(nm)))
+        return k, pk, nm
+
+
+def pm_acceleration(psi, cfg: PMConfig, solver: PMSolver | None = None):
+    """pm.jl:528-529: −∇φ at X = q + ψ (a fresh array)."""
+    if solver is None:
+        with PMSolver(cfg) as s:
+            return s.acceleration(psi)
+    return solver.acceleration(psi)
+
+
+def pm_acceleration_(solver: PMSolver, psi, out=None):
+    """pm.jl:507 `pm_acceleration!(S, psi)` (writes into `out` when given)."""
+    return solver.acceleration(psi, out=out)

@@ -1,0 +1,36 @@
+"""P(k) on the B200 with float64 shell sums (power_spectrum.jl:25-79)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import MEM_DEVICE, MEM_HOST, check, dptr, i64ptr, lib
+
+
+def evaluate_power_spectrum(field, boxsize: float, bins: int = 20, logarithmic: bool = True,
+                            deconvolve: bool = False, device: int = 0):
+    """(k, Pk, N_modes) of a (res,res,res) field indexed [ix,iy,iz] (a numpy array, or a
+    torch CUDA tensor of shape (res,res,res) in column-major memory, i.e. a contiguous
+    tensor indexed [iz,iy,ix]). `deconvolve` is accepted and unused, as in the reference."""
+    del deconvolve
+    if type(field).__module__.startswith("torch") and field.is_cuda:
+        res = int(field.shape[0])
+        if not field.is_contiguous() or tuple(field.shape) != (res, res, res):
+            raise ValueError("device field must be a contiguous cubic float32 tensor")
+        ptr, mem, keep = C.c_void_p(field.data_ptr()), MEM_DEVICE, field
+        device = field.device.index or 0
+    else:
+        a = np.asarray(field)
+        res = a.shape[0]
+        if a.shape != (res, res, res):
+            raise ValueError("field must be cubic")
+        keep = np.asfortranarray(a, dtype=np.float32)
+        ptr, mem = C.c_void_p(keep.ctypes.data), MEM_HOST
+    k = np.empty(bins)
+    pk = np.empty(bins)
+    nm = np.empty(bins, dtype=np.int64)
+    check(lib.djb_power_spectrum(ptr, int(res), float(boxsize), int(bins), int(bool(logarithmic)), dptr(k),
+                                 dptr(pk), i64ptr(nm), mem, int(device)))
+    del keep
+    return k, pk, nm

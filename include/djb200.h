@@ -1,0 +1,191 @@
+/*
+ * djb200.h — C ABI of libdjb200.so, a B200 (sm_100a) particle-mesh step for
+ * DiscoDJNative's `run_nbody` (yipihey/DiscoDJ.jl).
+ *
+ * Every function returns an int status (DJB_OK = 0). On failure the message is
+ * available from djb_last_error() (per calling thread). Invalid options raise
+ * DJB_ERR_INVALID with the same wording the reference uses in its Julia
+ * `error(...)` calls.
+ *
+ * Array conventions (the reference's, native/DiscoDJNative/src/nbody/pm.jl:15-17):
+ *   particle fields are Julia (n,n,n,3) Float32 arrays in column-major order,
+ *   i.e. three component blocks of n^3 floats, x index fastest. A pointer is host
+ *   memory when `mem` = DJB_MEM_HOST and device memory (a CuArray's pointer on
+ *   the solver's device) when `mem` = DJB_MEM_DEVICE.
+ *   A field mesh for djb_power_spectrum is (res,res,res) Float32 column-major
+ *   [ix,iy,iz] (x fastest).
+ *
+ * Threading: one solver per stream; calls on one solver are not re-entrant.
+ * Calls are synchronous with respect to the host unless stated otherwise.
+ */
+#ifndef DJB200_H
+#define DJB200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DJB_API __attribute__((visibility("default")))
+#else
+#define DJB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DJB_OK 0
+#define DJB_ERR_INVALID 1   /* invalid option or argument */
+#define DJB_ERR_CUDA 2      /* CUDA runtime error */
+#define DJB_ERR_CUFFT 3     /* cuFFT error */
+#define DJB_ERR_ALLOC 4     /* device or host allocation failed */
+#define DJB_ERR_STATE 5     /* call made in the wrong state (e.g. no particle state set) */
+#define DJB_ERR_DEVICE 6    /* a device-side check failed (error word set by a kernel) */
+
+#define DJB_MEM_HOST 0
+#define DJB_MEM_DEVICE 1
+
+/* steppers (run_nbody.jl:48-101) */
+#define DJB_STEPPER_BULLFROG 0
+#define DJB_STEPPER_FASTPM 1
+#define DJB_STEPPER_SYMPLECTIC 2
+
+/* time variables (run_nbody.jl:27-40); DJB_TIME_ARRAY = explicit vector of a */
+#define DJB_TIME_A 0
+#define DJB_TIME_LOG_A 1
+#define DJB_TIME_D 2
+#define DJB_TIME_SUPERCONFT 3
+#define DJB_TIME_ARRAY 4
+
+/* sheet resampling methods (pm.jl:45) */
+#define DJB_RESAMPLE_FOURIER 0
+#define DJB_RESAMPLE_LINEAR 1
+
+/* Options of the PM force. Mirrors `PMConfig` (pm.jl:35-46) field by field;
+ * `lean` selects the `PMSolverLean` restrictions (pm.jl:569-571). */
+typedef struct djb_pm_config {
+    int32_t res_pm;      /* mesh cells per side (even, >= 8) */
+    int32_t n_part;      /* particles per side (n_part^3 particles) */
+    double boxsize;      /* box side L */
+    int32_t worder;      /* 2 CIC, 3 TSC, 4 PCS */
+    int32_t deconvolve;  /* 0/1: divide by the assignment window twice */
+    int32_t antialias;   /* -1, 0, 1, 2, 3 interlacing shift sets */
+    int32_t grad_order;  /* 0 (ik), 2, 4, 6 finite-difference gradient */
+    int32_t lap_order;   /* 0 (-1/k^2), 2, 4, 6 finite-difference inverse Laplacian */
+    int32_t n_resample;  /* sheet resampling factor per axis (1 = off) */
+    int32_t resampling;  /* DJB_RESAMPLE_FOURIER or DJB_RESAMPLE_LINEAR */
+    int32_t lean;        /* 0/1: apply the PMSolverLean option restrictions */
+    int32_t device;      /* CUDA device ordinal */
+} djb_pm_config;
+
+typedef struct djb_cosmology djb_cosmology;
+typedef struct djb_solver djb_solver;
+
+/* ── library ─────────────────────────────────────────────────────────────── */
+DJB_API const char* djb_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+DJB_API const char* djb_last_error(void);
+
+/* ── cosmology and time tables (host, float64) ───────────────────────────── */
+/* Replaces `Cosmology(; Omega_c, Omega_b, h, sigma8, n_s, Omega_k, w0, wa)` +
+ * `compute_timetables(c; n_pts, a_ini)`
+ * (native/DiscoDJNative/src/cosmology/Cosmology.jl:22-45,86-115).
+ * params = {Omega_c, Omega_b, h, sigma8, n_s, Omega_k, w0, wa}. */
+DJB_API int djb_cosmology_create(const double params[8], int32_t n_pts, double a_ini,
+                         djb_cosmology** out);
+/* Replaces `Cosmology(name::String)` (Cosmology.jl:158-165). */
+DJB_API int djb_cosmology_create_named(const char* name, djb_cosmology** out);
+DJB_API int djb_cosmology_destroy(djb_cosmology* c);
+/* Number of table points (2500 by default). */
+DJB_API int djb_cosmology_table_size(const djb_cosmology* c, int32_t* n);
+/* Copies one table: 0 a, 1 Dplus (D1), 2 dDplus/da, 3 D2plus, 4 dD2plus/da,
+ * 5 superconformal time, 6 f1, 7 f2, 8 D3a, 9 D3b, 10 D3c
+ * (timetables.jl:23-24; Cosmology.jl:32-44). */
+DJB_API int djb_cosmology_table(const djb_cosmology* c, int32_t which, double* out, int32_t n);
+/* The eight parameters {Omega_c, Omega_b, h, sigma8, n_s, Omega_k, w0, wa}
+ * (Cosmology.jl:22-30). */
+DJB_API int djb_cosmology_params(const djb_cosmology* c, double out[8]);
+/* Unnormalised D1(a=1) (`_D1_unnormed_at_1`). */
+DJB_API int djb_cosmology_d1_unnormed(const djb_cosmology* c, double* out);
+/* Evaluates one timetable lookup at x: 0 Dplus(a) (`_Dplus`, timetables.jl:44),
+ * 1 dDplus/da (`growth_Dplusda` :30), 2 D2plus(a) (`_D2plus` :45),
+ * 3 dD2plus/da (:32), 4 superconft(a) (:34), 5 a_of_superconft(s) (:36),
+ * 6 a_of_Dplus(D) (:38), 7 Fplus(a) (:40), 8 hubble_E(a) (Cosmology.jl:55),
+ * 9 Omega_m (Cosmology.jl:47; x ignored). */
+DJB_API int djb_cosmology_eval(const djb_cosmology* c, int32_t what, double x, double* out);
+/* Replaces `stepper_coefficients(cosmo, stepper, a_ini, a_end, n_steps; time_var)`
+ * (native/DiscoDJNative/src/nbody/run_nbody.jl:48-101). Outputs have n_steps
+ * entries, all_a has n_steps+1. `time_var_array` (n_steps+1 scale factors) is
+ * read only when time_var == DJB_TIME_ARRAY. */
+DJB_API int djb_stepper_coefficients(const djb_cosmology* c, int32_t stepper, int32_t time_var,
+                             const double* time_var_array, double a_ini, double a_end,
+                             int32_t n_steps, double* alpha, double* beta, double* ddrift1,
+                             double* ddrift2, double* all_a);
+
+/* ── PM solver ───────────────────────────────────────────────────────────── */
+/* Replaces `PMSolver(cfg, like)` / `PMSolverLean(cfg, like)` (pm.jl:385-414,569-585):
+ * validates the options (pm.jl:136,146,214,245,423,570-571), allocates the
+ * device meshes, FFT plans and particle state on cfg->device. */
+DJB_API int djb_solver_create(const djb_pm_config* cfg, djb_solver** out);
+DJB_API int djb_solver_destroy(djb_solver* s);
+/* Runs subsequent work of this solver on `stream` (a cudaStream_t; NULL = the
+ * solver's own stream). */
+DJB_API int djb_solver_set_stream(djb_solver* s, void* stream);
+/* Device bytes held by the solver (meshes, particle state, cuFFT work areas). */
+DJB_API int djb_solver_device_bytes(const djb_solver* s, int64_t* bytes);
+
+/* Replaces `pm_acceleration!(S, psi)` (pm.jl:507-521, lean :623-641): writes
+ * acc = -grad(phi) at X = q + psi, (n,n,n,3) Float32, for displacements psi. */
+DJB_API int djb_pm_acceleration(djb_solver* s, const float* psi, float* acc, int32_t mem);
+
+/* Particle state (Psi, Mom) resident in HBM (run_nbody.jl:143-144).
+ * Mom is set to float(double(mom_in[i]) * mom_scale): mom_scale = Fplus(a_ini) for
+ * the symplectic stepper (`_pi_to_v`, run_nbody.jl:104), 1 otherwise. */
+DJB_API int djb_set_state(djb_solver* s, const float* psi, const float* mom, double mom_scale,
+                  int32_t mem);
+DJB_API int djb_get_state(djb_solver* s, float* psi, float* mom, int32_t mem);
+/* One drift-kick-drift step (run_nbody.jl:156-158):
+ *   Psi += dd1*Mom;  Mom = alpha*Mom + beta*acc(Psi);  Psi += dd2*Mom.
+ * The first drift is fused into the mass assignment and the kick and second drift
+ * into the force interpolation. Asynchronous on the solver's stream. */
+DJB_API int djb_step(djb_solver* s, double ddrift1, double alpha, double beta, double ddrift2);
+/* n_steps consecutive steps with per-step coefficients (the loop of run_nbody.jl:155-163). */
+DJB_API int djb_run(djb_solver* s, int32_t n_steps, const double* ddrift1, const double* alpha,
+            const double* beta, const double* ddrift2);
+/* Output of run_nbody.jl:148-171: x_out = Psi (wrap = 0), mod(q + Psi + L, L)
+ * (wrap = 1, the wrapped positions) or q + Psi (wrap = 2, `addq`), and
+ * p_out = float((double(Mom) / p_div) * p_mul) (`canon`, run_nbody.jl:149).
+ * Either pointer may be NULL. */
+DJB_API int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wrap, double p_div,
+                   double p_mul, int32_t mem);
+/* Per-phase timing with CUDA events on the solver's stream (enable = 1) and launch
+ * counts of this library's kernels. Phases: 0 mesh clear, 1 mass assignment,
+ * 2 sheet resampling, 3 R2C, 4 k-space multiply, 5 C2R, 6 force interpolation
+ * (fused kick-drift). Enabling or disabling resets the sums. */
+DJB_API int djb_solver_profile(djb_solver* s, int32_t enable);
+/* Reads and resets the sums: ms[phase] device milliseconds (0 when timing is off),
+ * launches[phase] kernel launches of this library, calls[phase] phase executions.
+ * nphase >= 7. */
+DJB_API int djb_solver_profile_read(djb_solver* s, double* ms, int64_t* launches, int64_t* calls,
+                                    int32_t nphase);
+/* Waits for the solver's queued work and reports a device-side error word, if any. */
+DJB_API int djb_synchronize(djb_solver* s);
+
+/* ── power spectrum (shell sums in float64) ──────────────────────────────── */
+/* Replaces `evaluate_power_spectrum(field, boxsize; bins, logarithmic)`
+ * (native/DiscoDJNative/src/analysis/power_spectrum.jl:25-79). `field` is a
+ * (res,res,res) Float32 column-major mesh. k, pk: `bins` doubles; nmodes: `bins`
+ * int64. Allocates its own device work area per call. */
+DJB_API int djb_power_spectrum(const float* field, int32_t res, double boxsize, int32_t bins,
+                       int32_t logarithmic, double* k, double* pk, int64_t* nmodes,
+                       int32_t mem, int32_t device);
+/* P(k) of the solver's current particle state: CIC deposit of q + Psi on the
+ * solver's mesh, delta = mesh*res^3/n^3 - 1, then the shell sums above (the
+ * snapshot measurement of studies/eft_shell_crossing/src/measure.jl:430-447). */
+DJB_API int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logarithmic, double* k,
+                             double* pk, int64_t* nmodes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DJB200_H */

@@ -1,0 +1,180 @@
+"""GPU parity: the CUDA path through the C ABI against the float64 oracle and the
+reference's golden vectors, every PM option of the fixture (16³ particles, 32³ mesh).
+
+Tolerances (float32 kernels vs float64 references, metric max|x−y|/max|y|):
+  acceleration 2e-5, displacement after the run 2e-5, momentum 2e-5, P(k) 1e-4 per bin.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import PARITY_CONFIGS, config_attrs, rel, run_kwargs
+
+pytestmark = pytest.mark.gpu
+
+ACC_TOL = 2e-5
+RUN_TOL = 2e-5
+PK_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def djb(cuda_device):
+    import djb200
+    return djb200
+
+
+@pytest.fixture(scope="module")
+def cosmo(djb):
+    return djb.Cosmology("Planck18EEBAOSN")
+
+
+def _cfg(djb, golden, name):
+    kw = run_kwargs(golden, name)
+    return djb.PMConfig(res_pm=kw["res_pm"], n_part=16, boxsize=100.0, worder=kw["worder"],
+                        deconvolve=kw["deconvolve"], antialias=kw["antialias"], grad_order=kw["grad_kernel_order"],
+                        lap_order=kw["laplace_kernel_order"], n_resample=kw["n_resample"],
+                        resampling=kw["resampling_method"])
+
+
+@pytest.mark.parametrize("name", PARITY_CONFIGS)
+def test_pm_acceleration_vs_golden(djb, golden, name):
+    acc = djb.pm_acceleration(golden["ics/psi_ini"], _cfg(djb, golden, name))
+    assert acc.shape == (16, 16, 16, 3) and acc.dtype == np.float32
+    assert rel(acc, golden[f"{name}/acc_ini"]) < ACC_TOL
+
+
+@pytest.mark.parametrize("name", PARITY_CONFIGS)
+def test_run_nbody_vs_golden(djb, golden, cosmo, name):
+    kw = run_kwargs(golden, name)
+    a = config_attrs(golden, name)
+    if a["ic_method"] == "bullfrog":
+        p0, m0 = djb.bullfrog_ics(cosmo, golden["ics/psi1"], kw["a_ini"], boxsize=100.0, res_pm=kw["res_pm"])
+    else:
+        p0, m0 = golden["ics/psi_ini"], golden["ics/pi_ini"]
+    psi, p, a_end = djb.run_nbody(cosmo, p0, m0, return_displacement=True, **kw)
+    assert a_end == kw["a_end"]
+    assert rel(psi, golden[f"{name}/psi_out"]) < RUN_TOL
+    assert rel(p, golden[f"{name}/p_out"]) < RUN_TOL
+
+
+def test_wrapped_positions_and_all_a(djb, golden, cosmo):
+    kw = run_kwargs(golden, "bullfrog_D_cic")
+    X, P, all_a = djb.run_nbody(cosmo, golden["ics/psi_ini"], golden["ics/pi_ini"], return_all_a=True, **kw)
+    assert np.all(X >= 0) and np.all(X < 100.0)
+    from oracle import nbody as onb
+    Xr = np.mod(onb.add_q(golden["bullfrog_D_cic/psi_out"], 100.0) + 100.0, 100.0)
+    d = np.abs(X - Xr)
+    d = np.minimum(d, 100.0 - d)  # periodic distance
+    assert d.max() < 1e-3
+    assert rel(all_a, golden["bullfrog_D_cic/all_a"]) < 1e-12
+
+
+def test_callbacks_and_history(djb, golden, cosmo):
+    """step_callback/callback_when select steps (pm_lean_tests.jl:121-124); collect_all
+    returns every step; the per-step path equals the fused run."""
+    kw = run_kwargs(golden, "fastpm_D_tsc")
+    seen = []
+    djb.run_nbody(cosmo, golden["ics/psi_ini"], golden["ics/pi_ini"], return_displacement=True,
+                  step_callback=lambda k, a, X, P: seen.append(k), callback_when=lambda k, a: k in (0, 4, 6), **kw)
+    assert seen == [0, 4, 6]
+    hx, hp, all_a = djb.run_nbody(cosmo, golden["ics/psi_ini"], golden["ics/pi_ini"], return_displacement=True,
+                                  collect_all=True, **kw)
+    assert len(hx) == kw["n_steps"] + 1 and len(all_a) == kw["n_steps"] + 1
+    assert rel(hx[0], golden["ics/psi_ini"]) < 1e-6
+    assert rel(hx[-1], golden["fastpm_D_tsc/psi_out"]) < RUN_TOL
+    assert rel(hp[-1], golden["fastpm_D_tsc/p_out"]) < RUN_TOL
+
+
+def test_lean_equals_full(djb):
+    """PMSolverLean ≡ PMSolver (pm_lean_tests.jl:96-107): n=24, res=48, L=120."""
+    rng = np.random.default_rng(5)
+    psi = (3 * rng.standard_normal((24, 24, 24, 3))).astype(np.float32)
+    for W, g in ((2, 4), (3, 2), (4, 6)):
+        cfg = djb.PMConfig(res_pm=48, n_part=24, boxsize=120.0, worder=W, grad_order=g)
+        with djb.PMSolver(cfg) as a, djb.PMSolver(cfg, lean=True) as b:
+            x, y = a.acceleration(psi), b.acceleration(psi)
+        assert rel(x, y) < 2e-5
+
+
+@pytest.mark.parametrize("W,g,aa,lap,dec", [(2, 4, 0, 0, False), (3, 2, 0, 4, False), (4, 6, 1, 0, True),
+                                            (2, 6, 2, 6, False), (4, 0, 1, 0, True), (3, 4, -1, 2, True)])
+def test_random_particles_vs_oracle(djb, W, g, aa, lap, dec):
+    """Strongly clustered random displacements (n=24, res=48) against the float64 oracle."""
+    from oracle import pm as opm
+    rng = np.random.default_rng(7 + W)
+    psi = (3 * rng.standard_normal((24, 24, 24, 3)))
+    cfg_o = opm.PMConfig(res_pm=48, n_part=24, boxsize=120.0, worder=W, grad_order=g, antialias=aa,
+                         lap_order=lap, deconvolve=dec)
+    cfg_d = djb.PMConfig(res_pm=48, n_part=24, boxsize=120.0, worder=W, grad_order=g, antialias=aa,
+                         lap_order=lap, deconvolve=dec)
+    ref = opm.pm_acceleration(cfg_o, psi.astype(np.float32).astype(np.float64))
+    got = djb.pm_acceleration(psi.astype(np.float32), cfg_d)
+    assert rel(got, ref) < ACC_TOL
+
+
+def test_device_arrays_roundtrip(djb, golden):
+    """CuArray-style call: device pointers in, device pointers out."""
+    import torch
+    cfg = _cfg(djb, golden, "bullfrog_D_cic")
+    psi_d = djb.native_view(torch.from_numpy(golden["ics/psi_ini"].astype(np.float32)).cuda())
+    with djb.PMSolver(cfg) as S:
+        acc_d = S.acceleration(psi_d)
+        acc_h = S.acceleration(golden["ics/psi_ini"])
+    got = djb.logical_view(acc_d).cpu().numpy()
+    assert np.array_equal(got, acc_h)
+
+
+def test_power_spectrum_vs_oracle(djb):
+    from oracle import power as opw
+    rng = np.random.default_rng(3)
+    field = rng.standard_normal((32, 32, 32))
+    field[3:9, 4:7, 10:20] += 4.0
+    k, pk, nm = djb.evaluate_power_spectrum(field.astype(np.float32), 250.0, bins=32, logarithmic=True)
+    kr, pkr, nmr = opw.evaluate_power_spectrum(field.astype(np.float32).astype(np.float64), 250.0, bins=32)
+    assert np.array_equal(nm, nmr)
+    assert rel(k, kr) < 1e-13
+    nz = nmr > 0
+    assert np.max(np.abs(pk[nz] / pkr[nz] - 1)) < PK_TOL
+    assert np.all(pk[~nz] == 0)
+    kl, pl, nl = djb.evaluate_power_spectrum(field.astype(np.float32), 250.0, bins=12, logarithmic=False)
+    klr, plr, nlr = opw.evaluate_power_spectrum(field.astype(np.float32).astype(np.float64), 250.0, bins=12,
+                                                logarithmic=False)
+    assert np.array_equal(nl, nlr) and np.max(np.abs(pl / plr - 1)) < PK_TOL
+
+
+def test_state_power_spectrum_vs_oracle(djb, golden):
+    """CIC deposit of the resident state -> δ -> P(k) (measure.jl:430-447)."""
+    from oracle import nbody as onb
+    from oracle import pm as opm
+    from oracle import power as opw
+    cfg = _cfg(djb, golden, "bullfrog_D_cic")
+    with djb.PMSolver(cfg) as S:
+        S.set_state(golden["ics/psi_ini"], golden["ics/pi_ini"])
+        k, pk, nm = S.state_power_spectrum(bins=16)
+    X = onb.add_q(golden["ics/psi_ini"].astype(np.float32).astype(np.float64), 100.0).reshape(-1, 3)
+    mesh = opm.pm_scatter(np.zeros((32, 32, 32)), X, 32, 100.0, 2)
+    kr, pkr, nmr = opw.evaluate_power_spectrum(opw.density_contrast(mesh, 16), 100.0, bins=16)
+    assert np.array_equal(nm, nmr)
+    nz = nmr > 0
+    assert np.max(np.abs(pk[nz] / pkr[nz] - 1)) < PK_TOL
+
+
+def test_nonfinite_position_is_reported_not_faulted(djb, golden):
+    """A NaN displacement sets the kernels' device error word; the call fails with
+    DJB_ERR_DEVICE and the solver stays usable."""
+    cfg = _cfg(djb, golden, "bullfrog_D_cic")
+    psi = golden["ics/psi_ini"].astype(np.float32).copy()
+    psi[3, 4, 5, 1] = np.nan
+    with djb.PMSolver(cfg) as S:
+        with pytest.raises(djb.DJBError, match="non-finite"):
+            S.acceleration(psi)
+        acc = S.acceleration(golden["ics/psi_ini"])
+    assert rel(acc, golden["bullfrog_D_cic/acc_ini"]) < ACC_TOL
+
+
+def test_state_calls_need_state(djb, golden):
+    cfg = _cfg(djb, golden, "bullfrog_D_cic")
+    with djb.PMSolver(cfg) as S:
+        with pytest.raises(djb.DJBError, match="no particle state"):
+            S.step(0.1, 1.0, 0.0, 0.1)

@@ -1,0 +1,137 @@
+"""CPU-side checks of libdjb200: the shared library loads and exports every symbol
+include/djb200.h declares; its float64 host code (cosmology tables, stepper
+coefficients) matches the golden vectors; option validation raises like the
+reference; the IC generator reproduces the fixture's 2LPT initial conditions.
+None of these launch a kernel."""
+from __future__ import annotations
+
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import PARITY_CONFIGS, ROOT, rel, run_kwargs
+
+djb200 = pytest.importorskip("djb200")
+
+HEADER = os.path.join(ROOT, "include", "djb200.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"DJB_API\s+(?:const\s+char\s*\*|int)\s+(djb_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(djb200.lib, s), s
+    # the ctypes signature table covers the header exactly
+    from djb200 import _lib
+    assert sorted(_lib.SIGNATURES) == syms
+
+
+def test_version_and_error_text():
+    assert b"sm_100a" in djb200.lib.djb_version()
+    assert djb200.lib.djb_last_error() is not None
+
+
+@pytest.fixture(scope="module")
+def cosmo():
+    return djb200.Cosmology("Planck18EEBAOSN")
+
+
+def test_cosmology_tables(golden, cosmo):
+    assert rel(cosmo.table("Dplus"), golden["cosmo/Dplus"]) < 1e-13
+    assert rel(cosmo.table("Dplusda"), golden["cosmo/Dplusda"]) < 1e-13
+    assert rel(cosmo.table("D2plus"), golden["cosmo/D2plus"]) < 1e-13
+    assert rel(cosmo.table("D2plusda"), golden["cosmo/D2plusda"]) < 1e-13
+    assert rel(cosmo.table("superconft"), golden["cosmo/superconft"]) < 1e-13
+    ref = json.loads(str(golden["cosmo/attrs"]))["Dplus_unnormed_at_1"]
+    assert abs(cosmo.D1_unnormed_at_1 / ref - 1) < 1e-13
+    assert abs(cosmo.Omega_m - json.loads(str(golden["cosmo/attrs"]))["Omega_m"]) < 1e-15
+
+
+def test_cosmology_matches_oracle():
+    from oracle import cosmology as cz
+    p = dict(Omega_c=0.261, Omega_b=0.049, h=0.677, sigma8=0.81, n_s=0.965)
+    a = djb200.Cosmology(**p)
+    b = cz.compute_timetables(cz.Cosmology(**p))
+    assert rel(a.table("Dplus"), b.D1_table) < 1e-14
+    assert rel(a.table("D3a"), b.D3a_table) < 1e-13
+    for x in (1e-3, 0.02, 0.5, 1.0):
+        assert abs(a.Fplus(x) / cz.Fplus(b, x) - 1) < 1e-13
+        assert abs(a.Dplus(x) / cz.Dplus(b, x) - 1) < 1e-14
+
+
+@pytest.mark.parametrize("name", PARITY_CONFIGS)
+def test_stepper_coefficients(golden, cosmo, name):
+    kw = run_kwargs(golden, name)
+    co = djb200.stepper_coefficients(cosmo, kw["stepper"], kw["a_ini"], kw["a_end"], kw["n_steps"],
+                                     time_var=kw["time_var"])
+    for k in ("alpha", "beta", "ddrift1", "ddrift2", "all_a"):
+        assert rel(co[k], golden[f"{name}/{k}"]) < 1e-12, k
+
+
+def test_unknown_cosmology_and_stepper_raise(cosmo):
+    with pytest.raises(djb200.DJBInvalidOption, match="Unknown cosmology"):
+        djb200.Cosmology("NotACosmology")
+    with pytest.raises(djb200.DJBInvalidOption, match="stepper must be"):
+        djb200.stepper_coefficients(cosmo, "leapfrog", 0.05, 1.0, 4)
+    with pytest.raises(djb200.DJBInvalidOption, match="time_var"):
+        djb200.stepper_coefficients(cosmo, "fastpm", 0.05, 1.0, 4, time_var="t")
+    with pytest.raises(djb200.DJBInvalidOption, match="n_steps \\+ 1"):
+        djb200.stepper_coefficients(cosmo, "fastpm", 0.05, 1.0, 4, time_var=np.array([0.1, 0.5, 1.0]))
+
+
+@pytest.mark.parametrize("field,value,msg", [
+    ("worder", 5, "worder must be 2, 3 or 4"),
+    ("grad_order", 3, "grad_order must be 0, 2, 4 or 6"),
+    ("lap_order", 1, "lap_order must be 0, 2, 4 or 6"),
+    ("antialias", 4, "antialias must be -1, 0, 1, 2 or 3"),
+    ("resampling", "cubic", "resampling must be :fourier or :linear"),
+])
+def test_invalid_pm_options_raise_before_touching_the_device(field, value, msg):
+    cfg = djb200.PMConfig(res_pm=32, n_part=16, boxsize=100.0)
+    setattr(cfg, field, value)
+    with pytest.raises(djb200.DJBInvalidOption, match=msg):
+        djb200.PMSolver(cfg)
+
+
+def test_lean_restrictions_raise():
+    """PMSolverLean supports antialias = 0, n_resample = 1, FD gradients (pm.jl:570-571)."""
+    for kw in (dict(antialias=1), dict(n_resample=2), dict(grad_order=0)):
+        cfg = djb200.PMConfig(res_pm=32, n_part=16, boxsize=100.0, **kw)
+        with pytest.raises(djb200.DJBInvalidOption, match="PMSolverLean supports"):
+            djb200.PMSolver(cfg, lean=True)
+
+
+def test_lpt_ics_match_fixture(golden, cosmo):
+    """fphi -> compute_core(n_order=2) -> nbody_ics_lpt reproduces the fixture's
+    Ψ, Π at a = 0.05 (nbody_parity_tests.jl:28-34, tolerance 1e-12)."""
+    import torch
+
+    from djb200 import ics
+    fphi = torch.from_numpy(golden["ics/fphi_re"] + 1j * golden["ics/fphi_im"])
+    shapes = {k: v.numpy() for k, v in ics.compute_core(fphi, 100.0, n_order=2).items()}
+    psi, pi = djb200.nbody_ics_lpt(cosmo, shapes, 0.05, 2)
+    assert rel(psi, golden["ics/psi_ini"]) < 1e-12
+    assert rel(pi, golden["ics/pi_ini"]) < 1e-12
+    # 1LPT shape at a = 1 (the fixture's psi1 is dΨ/dD of 1LPT)
+    assert rel(shapes["psi_1"], golden["ics/psi1"]) < 1e-12
+
+
+def test_3lpt_shapes_are_transverse_free_at_second_order_and_scale_cubically(golden):
+    """3LPT ψ₃ scales as φ³ and ψ₂ as φ² (EdS shapes are homogeneous in φ)."""
+    import torch
+
+    from djb200 import ics
+    fphi = torch.from_numpy(golden["ics/fphi_re"] + 1j * golden["ics/fphi_im"])
+    a = ics.compute_core(fphi, 100.0, n_order=3)
+    b = ics.compute_core(2.0 * fphi, 100.0, n_order=3)
+    assert rel(b["psi_2"].numpy(), 4.0 * a["psi_2"].numpy()) < 1e-12
+    assert rel(b["psi_3"].numpy(), 8.0 * a["psi_3"].numpy()) < 1e-12
+    assert float(a["psi_3"].abs().max()) > 0
