@@ -266,7 +266,8 @@ def main():
     co = djb200.stepper_coefficients(cosmo, "bullfrog", A_INI, A_END, nsteps)
     cfg = djb200.PMConfig(res_pm=res, n_part=n, boxsize=L, **OPTIONS)
     S = djb200.PMSolver(cfg, device=local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()          # a real stream: events and the solver share it
+    torch.cuda.set_stream(stream)
     S.set_stream(stream.cuda_stream)
     S.set_state(psi_d, pi_d)
     del psi_d, pi_d

@@ -18,6 +18,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -607,10 +608,17 @@ __global__ void k_wrap_psi_lin(const float* __restrict__ psi, const float* __res
 
 }  // namespace djb
 
+#include "tiled.cuh"
+
 // ─────────────────────────────────────────────────────────────────────────────
 // solver object
 // ─────────────────────────────────────────────────────────────────────────────
 namespace {
+
+// Shared-memory budgets of the tiled kernels: 24 K 32-bit cells (96 KB) for the mass
+// assignment, 24 K floats (96 KB) for the interpolation: 2 CTAs/SM each.
+constexpr int kScatterBudget = 24 * 1024;
+constexpr int kGatherBudget = 24 * 1024;
 
 // Phases of a force evaluation, timed with CUDA events on the solver's stream.
 enum Phase { PH_CLEAR = 0, PH_SCATTER, PH_RESAMPLE, PH_R2C, PH_KSPACE, PH_C2R, PH_GATHER, PH_COUNT };
@@ -706,6 +714,7 @@ struct djb_solver {
     float2* phase = nullptr;    // px, py, pz tables (n + n + n/2+1)
     int* err = nullptr;
     bool have_state = false;
+    bool tiled = true;  // shared-memory tiled scatter/gather (DJB_KERNELS=simple selects the per-particle ones)
     int64_t bytes = 0;
     std::vector<void*> allocs;
 };
@@ -785,9 +794,19 @@ GroupShifts group_shifts(const djb_solver* s, int first, int ns) {
     return g;
 }
 
+dim3 tile_grid(int n) {
+    return dim3((n + djb::kTX - 1) / djb::kTX, (n + djb::kTY - 1) / djb::kTY, (n + djb::kTZ - 1) / djb::kTZ);
+}
+
 template <int W, int NS>
 void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, float* m0,
                       float* m1) {
+    if (s->tiled) {
+        djb::k_scatter_tiled<W, NS><<<tile_grid(s->n), djb::kTileThreads, kScatterBudget * sizeof(unsigned int),
+                                      s->stream>>>(s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res,
+                                                   s->pitch, g, m0, m1, s->err, kScatterBudget);
+        return;
+    }
     djb::k_scatter<W, NS><<<blocks(s->np), kThreads, 0, s->stream>>>(
         s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err);
 }
@@ -813,8 +832,48 @@ void launch_scatter_positions(djb_solver* s, const float* xr, int64_t count, flo
 
 template <int W, int R>
 void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
+    if (R > 0 && s->tiled) {
+        constexpr int RR = R > 0 ? R : 1;
+        const size_t smem = kGatherBudget * sizeof(float);
+        if (ns == 1)
+            djb::k_gather_tiled<W, RR, 1><<<tile_grid(s->n), djb::kTileThreads, smem, s->stream>>>(a, kGatherBudget);
+        else
+            djb::k_gather_tiled<W, RR, 2><<<tile_grid(s->n), djb::kTileThreads, smem, s->stream>>>(a, kGatherBudget);
+        return;
+    }
     if (ns == 1) djb::k_gather<W, R, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(a);
     else djb::k_gather<W, R, 2><<<blocks(s->np), kThreads, 0, s->stream>>>(a);
+}
+
+// Opt the tiled interpolation kernels in to their shared-memory budget (> 48 KB).
+template <int W, int R>
+int tiled_attrs_wr() {
+    const int smem = kGatherBudget * int(sizeof(float));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return DJB_OK;
+}
+
+template <int W>
+int scatter_attrs_w() {
+    const int smem = kScatterBudget * int(sizeof(unsigned int));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_tiled<W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_tiled<W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return DJB_OK;
+}
+
+int tiled_attrs(int W, int R) {
+    // the CIC deposit of djb_state_power_spectrum uses the W = 2 kernels
+    TRY(scatter_attrs_w<2>());
+    if (W == 3) TRY(scatter_attrs_w<3>());
+    if (W == 4) TRY(scatter_attrs_w<4>());
+    if (R == 0) return DJB_OK;
+#define DJB_TA(W_, R_) \
+    if (W == W_ && R == R_) return tiled_attrs_wr<W_, R_>();
+    DJB_TA(2, 1) DJB_TA(2, 2) DJB_TA(2, 3) DJB_TA(3, 1) DJB_TA(3, 2) DJB_TA(3, 3)
+    DJB_TA(4, 1) DJB_TA(4, 2) DJB_TA(4, 3)
+#undef DJB_TA
+    return DJB_OK;
 }
 
 template <int W>
@@ -1019,6 +1078,11 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
     s->Lf = float(cfg->boxsize);
     s->W = cfg->worder;
     s->R = cfg->grad_order / 2;
+    {
+        const char* kind = std::getenv("DJB_KERNELS");
+        s->tiled = !(kind && std::strcmp(kind, "simple") == 0);
+    }
+    if (s->tiled) TRY(tiled_attrs(s->W, s->R));
     s->shifts = aa_shifts(cfg->antialias, 0.5 * s->L / s->res);
     s->nshift = int(s->shifts.size() / 3);
     const bool resample = cfg->n_resample > 1;

@@ -11,7 +11,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG_ROOT = os.path.dirname(HERE)
-LIB_PATH = os.path.join(PKG_ROOT, "lib", "libdjb200.so")
+LIB_PATH = os.environ.get("DJB200_LIB") or os.path.join(PKG_ROOT, "lib", "libdjb200.so")
 
 DJB_OK = 0
 DJB_ERR_INVALID = 1

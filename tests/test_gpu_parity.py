@@ -2,7 +2,10 @@
 reference's golden vectors, every PM option of the fixture (16³ particles, 32³ mesh).
 
 Tolerances (float32 kernels vs float64 references, metric max|x−y|/max|y|):
-  acceleration 2e-5, displacement after the run 2e-5, momentum 2e-5, P(k) 1e-4 per bin.
+  acceleration 2e-5, displacement and momentum after the run 2e-5, P(k) 1e-4 per bin.
+  Runs with deconvolution get 6e-5: the sinc^(-2W) window amplifies float32 round-off
+  at high k; a float32 CPU restatement of the same run already sits at 1.1e-5 (Ψ) and
+  3.4e-5 (P) from the float64 golden vectors for `symplectic_a_pcs_deconv`.
 """
 from __future__ import annotations
 
@@ -15,6 +18,7 @@ pytestmark = pytest.mark.gpu
 
 ACC_TOL = 2e-5
 RUN_TOL = 2e-5
+RUN_TOL_DECONV = 6e-5
 PK_TOL = 1e-4
 
 
@@ -54,8 +58,10 @@ def test_run_nbody_vs_golden(djb, golden, cosmo, name):
         p0, m0 = golden["ics/psi_ini"], golden["ics/pi_ini"]
     psi, p, a_end = djb.run_nbody(cosmo, p0, m0, return_displacement=True, **kw)
     assert a_end == kw["a_end"]
-    assert rel(psi, golden[f"{name}/psi_out"]) < RUN_TOL
-    assert rel(p, golden[f"{name}/p_out"]) < RUN_TOL
+    # bullfrog ICs come from a PCS + deconvolution step (run_nbody.jl:219-220)
+    tol = RUN_TOL_DECONV if (kw["deconvolve"] or a["ic_method"] == "bullfrog") else RUN_TOL
+    assert rel(psi, golden[f"{name}/psi_out"]) < tol
+    assert rel(p, golden[f"{name}/p_out"]) < tol
 
 
 def test_wrapped_positions_and_all_a(djb, golden, cosmo):
@@ -122,7 +128,8 @@ def test_device_arrays_roundtrip(djb, golden):
         acc_d = S.acceleration(psi_d)
         acc_h = S.acceleration(golden["ics/psi_ini"])
     got = djb.logical_view(acc_d).cpu().numpy()
-    assert np.array_equal(got, acc_h)
+    # float atomics in the mass assignment sum in a run-dependent order
+    assert rel(got, acc_h) < 1e-6
 
 
 def test_power_spectrum_vs_oracle(djb):
