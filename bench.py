@@ -140,7 +140,8 @@ def profile_traffic():
     return None
 
 
-def dist_setup():
+def dist_setup(backend: str | None = None):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo on CPU-only hosts."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -149,9 +150,17 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
+
+
+def replica_seed(rank: int, base: int = 42) -> int:
+    """Replicas only: every rank evolves an independent box."""
+    return base + rank
 
 
 def barrier(world):
@@ -161,13 +170,20 @@ def barrier(world):
 
 
 def allmax(world, x: float) -> float:
+    """Max over ranks (the timing rule: the slowest rank defines the step time)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_value(world: int, n_part: int, steps: int, ms_max: float) -> float:
+    """Whole-job particle-steps/s: all ranks' particles over the slowest rank's time."""
+    return world * n_part ** 3 * steps / (ms_max / 1e3)
 
 
 def make_ics(cosmo, n, L, lpt, seed, device):
@@ -252,7 +268,7 @@ def main():
     torch.cuda.set_device(local)
     n, res, L, lpt = SIZES[args.size]
     cosmo = djb200.Cosmology(**COSMO)
-    psi, pi = make_ics(cosmo, n, L, lpt, 42 + rank, dev)
+    psi, pi = make_ics(cosmo, n, L, lpt, replica_seed(rank), dev)
     psi_d = djb200.native_view(psi)
     pi_d = djb200.native_view(pi)
     # pinned host copies for the end-to-end leg
@@ -293,7 +309,7 @@ def main():
     S.synchronize()
     ms = allmax(world, ms_local)
     Np = n ** 3
-    value = world * Np * args.steps / (ms / 1e3)
+    value = aggregate_value(world, n, args.steps, ms)
 
     # end to end through the C ABI with host buffers: H2D of (Ψ, Π) from pinned memory,
     # K fused steps, D2H of (X, P) into pinned memory, all inside the timed region

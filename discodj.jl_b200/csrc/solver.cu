@@ -617,8 +617,14 @@ namespace {
 
 // Shared-memory budgets of the tiled kernels: 24 K 32-bit cells (96 KB) for the mass
 // assignment, 24 K floats (96 KB) for the interpolation: 2 CTAs/SM each.
-constexpr int kScatterBudget = 24 * 1024;
-constexpr int kGatherBudget = 24 * 1024;
+#ifndef DJB_SCATTER_BUDGET
+#define DJB_SCATTER_BUDGET (24 * 1024)
+#endif
+#ifndef DJB_GATHER_BUDGET
+#define DJB_GATHER_BUDGET (24 * 1024)
+#endif
+constexpr int kScatterBudget = DJB_SCATTER_BUDGET;
+constexpr int kGatherBudget = DJB_GATHER_BUDGET;
 
 // Phases of a force evaluation, timed with CUDA events on the solver's stream.
 enum Phase { PH_CLEAR = 0, PH_SCATTER, PH_RESAMPLE, PH_R2C, PH_KSPACE, PH_C2R, PH_GATHER, PH_COUNT };
