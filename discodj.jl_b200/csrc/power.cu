@@ -8,7 +8,9 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "common.h"
@@ -181,9 +183,103 @@ int shells(const float2* spec, int res, double boxsize, double scale2, int bins,
     return DJB_OK;
 }
 
+// ── non-allocating shell sums ─────────────────────────────────────────────────
+// Work area of djb_power_spectrum_shells_noalloc: bin edges, the four per-bin sums
+// and the per-bin mode counts, for at most kNoAllocBins bins. It lives in a
+// file-scope device array that every GPU loading the library holds until exit;
+// every call shares it, and it keeps the previous call's contents.
+constexpr int kNoAllocBins = 512;
+constexpr size_t kEdgesBytes = ((kNoAllocBins + 1) * sizeof(double) + 255) / 256 * 256;
+constexpr size_t kSumsBytes = 4 * kNoAllocBins * sizeof(double);
+constexpr size_t kCountsBytes = kNoAllocBins * sizeof(unsigned long long);
+constexpr size_t kNoAllocBytes = kEdgesBytes + kSumsBytes + kCountsBytes;  // 24,832 bytes
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch per device. In host code the symbol's name is
+// only a host-side stand-in, so the address comes from cudaGetSymbolAddress, taken
+// once per device with that device current.
+void* g_noalloc_addr[kMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+int noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(DJB_ERR_INVALID, "device ordinal %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(DJB_ERR_CUDA, "cudaGetSymbolAddress of the shell-sum scratch failed: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_addr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+    return DJB_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int djb_power_spectrum_shells_noalloc(const void* spectrum, int32_t res, double boxsize, int32_t bins,
+                                      int32_t logarithmic, double scale2, double* k, double* pk,
+                                      int64_t* nmodes, void* stream, int32_t device) {
+    djb::clear_error();
+    if (!spectrum || !k || !pk || !nmodes) return fail(DJB_ERR_INVALID, "null argument");
+    if (res < 2 || (res & 1)) return fail(DJB_ERR_INVALID, "field must be cubic with an even side");
+    if (bins < 1 || bins > kNoAllocBins)
+        return fail(DJB_ERR_INVALID,
+                    "bins = %d exceeds the %d bins of the non-allocating shell sums (use djb_power_spectrum)",
+                    bins, kNoAllocBins);
+    if (!(boxsize > 0)) return fail(DJB_ERR_INVALID, "boxsize must be positive");
+    CUDA_TRY(cudaSetDevice(device));
+    unsigned char* base = nullptr;
+    int rc = noalloc_scratch(device, &base);
+    if (rc != DJB_OK) return rc;
+    double* d_edges = reinterpret_cast<double*>(base);
+    double* d_sums = reinterpret_cast<double*>(base + kEdgesBytes);
+    unsigned long long* d_counts = reinterpret_cast<unsigned long long*>(base + kEdgesBytes + kSumsBytes);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // host-side work lives on the stack: nothing is allocated
+    double e[kNoAllocBins + 1];
+    double sums[4 * kNoAllocBins];
+    unsigned long long counts[kNoAllocBins];
+    {
+        const double dk = 2 * M_PI / boxsize;
+        const double kny = M_PI * res / boxsize;
+        const double kmin = dk, kmax = kny * std::sqrt(3.0);
+        for (int j = 0; j <= bins; ++j)
+            e[j] = logarithmic ? std::pow(10.0, linrange(std::log10(kmin), std::log10(kmax), j, bins + 1))
+                               : linrange(kmin, kmax, j, bins + 1);
+    }
+    CUDA_TRY(cudaMemcpyAsync(d_edges, e, sizeof(double) * (bins + 1), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(d_sums, 0, kSumsBytes, st));     // the previous call's sums remain otherwise
+    CUDA_TRY(cudaMemsetAsync(d_counts, 0, kCountsBytes, st));
+    const double V = boxsize * boxsize * boxsize;
+    const double r3 = double(res) * res * res;
+    const double norm = V / (r3 * r3) * scale2;
+    const int64_t total = int64_t(res) * res * (res / 2 + 1);
+    const int grid = int(std::min<int64_t>((total + kThreads - 1) / kThreads, 148 * 8));
+    k_shells<<<grid, kThreads, size_t(bins) * 4 * sizeof(double), st>>>(
+        static_cast<const float2*>(spectrum), res, 2 * M_PI / boxsize, norm, d_edges, bins, d_sums, d_counts);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(sums, d_sums, sizeof(double) * 4 * bins, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(counts, d_counts, sizeof(unsigned long long) * bins, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int b = 0; b < bins; ++b) {
+        if (counts[b] == 0) {
+            k[b] = std::sqrt(e[b] * e[b + 1]);
+            pk[b] = 0.0;
+            nmodes[b] = 0;
+        } else {
+            k[b] = sums[4 * b + 2] / double(counts[b]);
+            pk[b] = sums[4 * b + 0] / sums[4 * b + 1];
+            nmodes[b] = int64_t(counts[b]);
+        }
+    }
+    return DJB_OK;
+}
 
 int djb_power_spectrum(const float* field, int32_t res, double boxsize, int32_t bins, int32_t logarithmic,
                        double* k, double* pk, int64_t* nmodes, int32_t mem, int32_t device) {

@@ -34,3 +34,22 @@ def evaluate_power_spectrum(field, boxsize: float, bins: int = 20, logarithmic: 
                                  dptr(pk), i64ptr(nm), mem, int(device)))
     del keep
     return k, pk, nm
+
+
+def power_spectrum_shells_noalloc(spectrum, boxsize: float, bins: int = 20, logarithmic: bool = True,
+                                  scale2: float = 1.0, stream: int | None = None):
+    """Shell sums of a device half spectrum without any device allocation
+    (`djb_power_spectrum_shells_noalloc`). `spectrum` is a contiguous complex64 CUDA
+    tensor of shape (res, res, res//2+1) indexed [kz, ky, kx], e.g.
+    `torch.fft.rfftn(field_zyx, dim=(0, 1, 2))` of a field stored [iz, iy, ix]."""
+    res = int(spectrum.shape[0])
+    if tuple(spectrum.shape) != (res, res, res // 2 + 1) or not spectrum.is_contiguous():
+        raise ValueError("spectrum must be a contiguous (res, res, res//2+1) complex64 tensor")
+    k = np.empty(bins)
+    pk = np.empty(bins)
+    nm = np.empty(bins, dtype=np.int64)
+    check(lib.djb_power_spectrum_shells_noalloc(C.c_void_p(spectrum.data_ptr()), res, float(boxsize), int(bins),
+                                                int(bool(logarithmic)), float(scale2), dptr(k), dptr(pk),
+                                                i64ptr(nm), C.c_void_p(stream or 0),
+                                                int(spectrum.device.index or 0)))
+    return k, pk, nm

@@ -184,6 +184,31 @@ DJB_API int djb_power_spectrum(const float* field, int32_t res, double boxsize, 
 DJB_API int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logarithmic, double* k,
                              double* pk, int64_t* nmodes);
 
+/* ── non-allocating shell sums ──────────────────────────────────────────────
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory at the point of the call: code running while a stream is being
+ * captured into a CUDA graph (where cudaMalloc is not allowed), applications
+ * whose device memory is owned by a pool or an external framework that forbids
+ * allocations outside it, and step loops that must not synchronise the device
+ * through an allocator. The caller passes the half spectrum of a (res,res,res)
+ * field (device memory, complex64 [kz][ky][kx], kx in [0, res/2], as an in-place
+ * R2C of the x-fastest field produces it) and host outputs k, pk (double) and
+ * nmodes (int64) of `bins` entries; scale2 multiplies |delta(k)|^2 (1 for a field
+ * given directly). The per-bin work area is a file-scope device array for at
+ * most 512 bins (about 24 KB, held by every GPU that loads the library until
+ * exit); more bins are rejected with DJB_ERR_INVALID. The call allocates no
+ * device memory and calls no allocating library routine. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and caches
+ * it, so make that first call before any stream capture begins. All calls share
+ * the one array, which keeps the last call's contents (each call clears the sums
+ * it uses): calls that overlap on the GPU, on different streams or threads, race.
+ * Runs on `stream` (a cudaStream_t, NULL = legacy default) of `device` and waits
+ * for it before returning. Same results as djb_power_spectrum for the same field. */
+DJB_API int djb_power_spectrum_shells_noalloc(const void* spectrum, int32_t res, double boxsize,
+                                              int32_t bins, int32_t logarithmic, double scale2,
+                                              double* k, double* pk, int64_t* nmodes, void* stream,
+                                              int32_t device);
+
 #ifdef __cplusplus
 }
 #endif
