@@ -1,0 +1,295 @@
+// Brick-owned mass assignment and force interpolation.
+//
+// The particles are binned by the B^3-cell brick holding their (drifted) shift-0
+// base node (sort.cuh, linear brick order). One CTA owns one brick and every
+// particle binned into it. The brick's Eulerian box is known in advance:
+//   mass assignment  : nodes [B*b + lo - 1, B*b + B + W + 1), i.e. B + W + 2 per axis:
+//                      one node of margin on each side for the interlacing shifts
+//                      (+h/2, and -h/4 with antialias = 3) and odd-order rounding;
+//   interpolation    : the same box widened by the finite-difference halo R.
+// An empty brick costs one read of its count; a dense brick loops over its particles
+// in rounds of 256 while its box stays in shared memory. The staged volume per step
+// is (number of non-empty bricks) x (box volume), independent of how far particles
+// have moved from their Lagrangian positions.
+#pragma once
+
+#include "tiled.cuh"
+#include "sort.cuh"
+
+namespace djb {
+
+constexpr int kBrickRounds = 4;  // particles kept in registers per thread (interpolation)
+
+struct BrickList {
+    const unsigned* count;   // particles per brick
+    const unsigned* offset;  // block-local exclusive scan of count
+    const unsigned* bsum;    // scan of the block totals
+    const int* perm;         // particles in brick order
+    int nb;                  // bricks per axis
+    int brick;               // cells per brick side
+};
+
+__device__ __forceinline__ void brick_range(const BrickList& bl, int b, unsigned& start, unsigned& cnt) {
+    cnt = bl.count[b];
+    start = bl.offset[b] + bl.bsum[b / kScanBlock];
+}
+
+// Box of brick b: origin B*b + lo - R - 1 per axis, S = B + W + 2 + 2R nodes per axis.
+__device__ __forceinline__ TileBox brick_box(const BrickList& bl, int b, int lo_minus_r, int S) {
+    TileBox box;
+    const int bx = b % bl.nb, by = (b / bl.nb) % bl.nb, bz = b / (bl.nb * bl.nb);
+    box.o[0] = bx * bl.brick + lo_minus_r - 1;
+    box.o[1] = by * bl.brick + lo_minus_r - 1;
+    box.o[2] = bz * bl.brick + lo_minus_r - 1;
+    box.S[0] = box.S[1] = box.S[2] = S;
+    box.P = S | 1;
+    box.plane = box.P * S;
+    return box;
+}
+
+// Offset of a node from the box origin, periodic differences taken in [-4, res - 4):
+// valid offsets lie in [-1, B + W + 2R + 1] and res > B + W + 2R + 6 (brick <= res/2).
+__device__ __forceinline__ int box_rel(int node, int origin, int res) {
+    int v = (node - origin) % res;
+    if (v < -4) v += res;
+    else if (v >= res - 4) v -= res;
+    return v;
+}
+
+// ── mass assignment ───────────────────────────────────────────────────────────
+template <int W, int NS>
+__global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
+    const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
+    GroupShifts sh, float* __restrict__ mesh0, float* __restrict__ mesh1, int* err, BrickList bl) {
+    extern __shared__ unsigned int sacc[];
+    __shared__ int s_row[kMaxRows];
+    __shared__ int s_col[kMaxCols];
+    const int b = blockIdx.x;
+    unsigned start, cnt;
+    brick_range(bl, b, start, cnt);
+    if (cnt == 0) return;
+    const int tid = threadIdx.x;
+    constexpr int S_EXT = W + 2;  // box = brick + W + 2 nodes
+    const TileBox box = brick_box(bl, b, WLo<W>::v, bl.brick + S_EXT);
+    const float resf = float(res);
+    box_columns(box, res, s_col);
+    chunk_rows(box, res, 0, box.S[2], s_row);
+    __syncthreads();  // the row and column tables are read by every thread below
+    FastDiv fp;
+    fp.init(box.P);
+    const int cells = box.plane * box.S[2];
+#pragma unroll 1
+    for (int g = 0; g < NS; ++g) {
+        float* mesh = (g == 0) ? mesh0 : mesh1;
+        const Shift3 sg = (g == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
+        for (int t = tid; t < cells; t += kTileThreads) sacc[t] = 0u;
+        __syncthreads();
+        for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
+            const unsigned slot = r0 + tid;
+            if (slot >= cnt) continue;
+            const int64_t p = bl.perm[start + slot];
+            const int i = int(p % n), j = int((p / n) % n), k = int(p / (int64_t(n) * n));
+            const float X[3] = {psi[p] + q1[i], psi[p + np] + q1[j], psi[p + 2 * np] + q1[k]};
+            float w[3][W];
+            int d[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float s = (a == 0) ? sg.x : (a == 1) ? sg.y : sg.z;
+                const float gc = grid_coord(X[a] + s, L, resf, err);
+                const int bb = wbase<W>(gc);
+#pragma unroll
+                for (int o = 0; o < W; ++o) w[a][o] = wk<W>(fabsf(gc - float(bb + WLo<W>::v + o)));
+                d[a] = box_rel(bb + WLo<W>::v, box.o[a], res);
+                if (d[a] < 0 || d[a] > box.S[a] - W) {  // not binned consistently: report, stay in bounds
+                    atomicOr(err, 2);
+                    d[a] = d[a] < 0 ? 0 : box.S[a] - W;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+#pragma unroll
+                for (int bb = 0; bb < W; ++bb) {
+                    unsigned int* row = sacc + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+                    const float wyz = w[1][bb];
+#pragma unroll
+                    for (int a = 0; a < W; ++a)
+                        atomicAdd(row + a, __float2uint_rn(w[0][a] * wyz * w[2][c] * FixScale<W>::up));
+                }
+        }
+        __syncthreads();
+        for (int t = tid; t < cells; t += kTileThreads) {
+            const unsigned int v = sacc[t];
+            if (v == 0u) continue;
+            const int r = fp.div(t);
+            const int x = t - r * box.P;
+            atomicAdd(mesh + int64_t(s_row[r]) * pitch + s_col[x], __uint2float_rn(v) * FixScale<W>::down);
+        }
+        __syncthreads();
+    }
+}
+
+// ── force interpolation (finite-difference gradient of order 2R) ─────────────
+template <int W, int R, int NS>
+__global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, BrickList bl) {
+    extern __shared__ float sbox[];
+    __shared__ int s_row[kMaxRows];
+    __shared__ int s_col[kMaxCols];
+    constexpr int E = W + 2 * R;
+    const int b = blockIdx.x;
+    unsigned start, cnt;
+    brick_range(bl, b, start, cnt);
+    if (cnt == 0) return;
+    const int tid = threadIdx.x;
+    const int n = A.n;
+    const int64_t np = A.np;
+    const int res = A.res;
+    const TileBox box = brick_box(bl, b, WLo<W>::v - R, bl.brick + W + 2 + 2 * R);
+    box_columns(box, res, s_col);
+    chunk_rows(box, res, 0, box.S[2], s_row);
+    __syncthreads();  // the row and column tables are read by every thread below
+    FastDiv fp;
+    fp.init(box.P);
+    const int cells = box.plane * box.S[2];
+    const float resf = float(res);
+    const float cc[4] = {0.0f, A.c1, A.c2, A.c3};
+    for (unsigned sr = 0; sr < cnt; sr += kTileThreads * kBrickRounds) {
+        // the particles of this super-round stay in registers across the shifts
+        int64_t pr[kBrickRounds];
+        float ps[kBrickRounds][3], acc[kBrickRounds][3];
+#pragma unroll
+        for (int r = 0; r < kBrickRounds; ++r) {
+            const unsigned slot = sr + r * kTileThreads + tid;
+            pr[r] = (slot < cnt) ? int64_t(bl.perm[start + slot]) : -1;
+            acc[r][0] = acc[r][1] = acc[r][2] = 0.0f;
+            ps[r][0] = ps[r][1] = ps[r][2] = 0.0f;
+            if (pr[r] >= 0) {
+                const int64_t p = pr[r];
+                ps[r][0] = A.psi[p];
+                ps[r][1] = A.psi[p + np];
+                ps[r][2] = A.psi[p + 2 * np];
+                if (!A.first) {
+                    acc[r][0] = A.acc[p];
+                    acc[r][1] = A.acc[p + np];
+                    acc[r][2] = A.acc[p + 2 * np];
+                }
+            }
+        }
+#pragma unroll 1
+        for (int g = 0; g < NS; ++g) {
+            const float* phi = (g == 0) ? A.mesh[0] : A.mesh[NS > 1 ? 1 : 0];
+            const Shift3 sgs = (g == 0) ? A.sh.s[0] : A.sh.s[NS > 1 ? 1 : 0];
+            for (int t = tid; t < cells; t += kTileThreads) {
+                const int r = fp.div(t);
+                const int x = t - r * box.P;
+                if (x >= box.S[0]) continue;
+                const float* src = phi + int64_t(s_row[r]) * A.pitch + s_col[x];
+                const unsigned sa = unsigned(__cvta_generic_to_shared(sbox + t));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src));
+            }
+            asm volatile("cp.async.wait_all;\n" ::);
+            __syncthreads();
+#pragma unroll 1
+            for (int r = 0; r < kBrickRounds; ++r) {
+                if (pr[r] < 0) continue;
+                const int64_t p = pr[r];
+                const int i = int(p % n), j = int((p / n) % n), k = int(p / (int64_t(n) * n));
+                const float X[3] = {ps[r][0] + A.q1[i], ps[r][1] + A.q1[j], ps[r][2] + A.q1[k]};
+                float w[3][W], u[3][E];
+                int d[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float s = (a == 0) ? sgs.x : (a == 1) ? sgs.y : sgs.z;
+                    const float gc = grid_coord(X[a] + s, A.L, resf, A.err);
+                    const int bb = wbase<W>(gc);
+#pragma unroll
+                    for (int o = 0; o < W; ++o) w[a][o] = wk<W>(fabsf(gc - float(bb + WLo<W>::v + o)));
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        float sacc = 0.0f;
+#pragma unroll
+                        for (int o = 0; o < W; ++o) {
+                            const int t = e - R - o;
+                            if (t > 0 && t <= R) sacc -= w[a][o] * cc[t > 0 ? t : 0];
+                            if (t < 0 && -t <= R) sacc += w[a][o] * cc[t < 0 ? -t : 0];
+                        }
+                        u[a][e] = sacc;
+                    }
+                    d[a] = box_rel(bb + WLo<W>::v - R, box.o[a], res);
+                    if (d[a] < 0 || d[a] > box.S[a] - E) {  // not binned consistently: report, stay in bounds
+                        atomicOr(A.err, 2);
+                        d[a] = d[a] < 0 ? 0 : box.S[a] - E;
+                    }
+                }
+                float sX = 0.0f, sY = 0.0f, sZ = 0.0f;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const float* pl = sbox + (d[2] + e) * box.plane + d[0];
+                    if (e >= R && e < R + W) {
+                        const int c = e - R;
+#pragma unroll
+                        for (int bb = 0; bb < W; ++bb) {
+                            const float* row = pl + (d[1] + R + bb) * box.P;
+                            float rx = 0.0f, rc = 0.0f;
+#pragma unroll
+                            for (int x = 0; x < E; ++x) {
+                                const float v = row[x];
+                                rx += u[0][x] * v;
+                                if (x >= R && x < R + W) rc += w[0][x - R] * v;
+                            }
+                            sX += (w[1][bb] * w[2][c]) * rx;
+                            sY += (u[1][bb + R] * w[2][c]) * rc;
+                            sZ += (u[2][e] * w[1][bb]) * rc;
+                        }
+#pragma unroll
+                        for (int h = 0; h < 2 * R; ++h) {
+                            const int ey = (h < R) ? h : h + W;
+                            const float* row = pl + (d[1] + ey) * box.P + R;
+                            float rc = 0.0f;
+#pragma unroll
+                            for (int a = 0; a < W; ++a) rc += w[0][a] * row[a];
+                            sY += (u[1][ey] * w[2][c]) * rc;
+                        }
+                    } else {
+#pragma unroll
+                        for (int bb = 0; bb < W; ++bb) {
+                            const float* row = pl + (d[1] + R + bb) * box.P + R;
+                            float rc = 0.0f;
+#pragma unroll
+                            for (int a = 0; a < W; ++a) rc += w[0][a] * row[a];
+                            sZ += (u[2][e] * w[1][bb]) * rc;
+                        }
+                    }
+                }
+                acc[r][0] += sX;
+                acc[r][1] += sY;
+                acc[r][2] += sZ;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int r = 0; r < kBrickRounds; ++r) {
+            if (pr[r] < 0) continue;
+            const int64_t p = pr[r];
+            float a3[3] = {acc[r][0], acc[r][1], acc[r][2]};
+            if (A.last && A.divide) {
+                a3[0] = a3[0] / A.nshift_f;
+                a3[1] = a3[1] / A.nshift_f;
+                a3[2] = a3[2] / A.nshift_f;
+            }
+            if (A.last && A.step) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const float m = A.alpha * A.mom[p + c * np] + A.beta * a3[c];
+                    A.mom[p + c * np] = m;
+                    A.psi[p + c * np] = ps[r][c] + A.dd2 * m;
+                }
+            } else {
+                A.acc[p] = a3[0];
+                A.acc[p + np] = a3[1];
+                A.acc[p + 2 * np] = a3[2];
+            }
+        }
+    }
+}
+
+}  // namespace djb

@@ -384,6 +384,7 @@ struct GatherArgs {
     int step;           // 1: kick + drift after the last group; 0: write acc
     float alpha, beta, dd2;
     int* err;
+    const int* perm;    // brick-sorted particle order for the tiled kernels (null: Lagrangian tiles)
 };
 
 template <int W, int R, int NS>
@@ -608,7 +609,7 @@ __global__ void k_wrap_psi_lin(const float* __restrict__ psi, const float* __res
 
 }  // namespace djb
 
-#include "tiled.cuh"
+#include "brick.cuh"
 
 // ─────────────────────────────────────────────────────────────────────────────
 // solver object
@@ -627,7 +628,7 @@ constexpr int kScatterBudget = DJB_SCATTER_BUDGET;
 constexpr int kGatherBudget = DJB_GATHER_BUDGET;
 
 // Phases of a force evaluation, timed with CUDA events on the solver's stream.
-enum Phase { PH_CLEAR = 0, PH_SCATTER, PH_RESAMPLE, PH_R2C, PH_KSPACE, PH_C2R, PH_GATHER, PH_COUNT };
+enum Phase { PH_CLEAR = 0, PH_SCATTER, PH_RESAMPLE, PH_R2C, PH_KSPACE, PH_C2R, PH_GATHER, PH_SORT, PH_COUNT };
 
 // Launch counts of this library's kernels (always on) and, when enabled, per-phase
 // device time from event pairs recorded around each phase.
@@ -718,6 +719,17 @@ struct djb_solver {
     float* rb = nullptr;        // real n*n*(n+2) (in-place C2R)
     float* xr = nullptr;        // 3*np resampled positions
     float2* phase = nullptr;    // px, py, pz tables (n + n + n/2+1)
+    // brick sort of the particles (sort.cuh)
+    bool sorted = true;
+    djb::SortGeom sg{};
+    int64_t nbins = 0;
+    int nscan = 0;
+    unsigned* count = nullptr;
+    unsigned* offset = nullptr;
+    unsigned* bsum = nullptr;
+    uint2* keyrank = nullptr;
+    int* perm = nullptr;
+    const int* cur_perm = nullptr;  // order used by the tiled kernels of the current force call
     int* err = nullptr;
     bool have_state = false;
     bool tiled = true;  // shared-memory tiled scatter/gather (DJB_KERNELS=simple selects the per-particle ones)
@@ -804,13 +816,30 @@ dim3 tile_grid(int n) {
     return dim3((n + djb::kTX - 1) / djb::kTX, (n + djb::kTY - 1) / djb::kTY, (n + djb::kTZ - 1) / djb::kTZ);
 }
 
+djb::BrickList brick_list(const djb_solver* s) {
+    return djb::BrickList{s->count, s->offset, s->bsum, s->perm, s->sg.nb, s->sg.brick};
+}
+
+// Shared memory of the brick kernels: the fixed box, B + W + 2 (+ 2R) nodes per axis.
+size_t brick_smem(const djb_solver* s, int halo) {
+    const int S = s->sg.brick + s->W + 2 + 2 * halo;
+    return size_t(S | 1) * S * S * 4;
+}
+
 template <int W, int NS>
 void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, float* m0,
                       float* m1) {
+    if (s->tiled && s->cur_perm) {  // brick-owned: the drift was applied by the binning pass
+        djb::k_scatter_brick<W, NS><<<unsigned(s->nbins), djb::kTileThreads, brick_smem(s, 0), s->stream>>>(
+            s->psi, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err, brick_list(s));
+        return;
+    }
     if (s->tiled) {
-        djb::k_scatter_tiled<W, NS><<<tile_grid(s->n), djb::kTileThreads, kScatterBudget * sizeof(unsigned int),
-                                      s->stream>>>(s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res,
-                                                   s->pitch, g, m0, m1, s->err, kScatterBudget);
+        const dim3 grid = s->cur_perm ? dim3(unsigned((s->np + djb::kTileThreads - 1) / djb::kTileThreads))
+                                      : tile_grid(s->n);
+        djb::k_scatter_tiled<W, NS><<<grid, djb::kTileThreads, kScatterBudget * sizeof(unsigned int), s->stream>>>(
+            s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err, kScatterBudget,
+            s->cur_perm);
         return;
     }
     djb::k_scatter<W, NS><<<blocks(s->np), kThreads, 0, s->stream>>>(
@@ -838,13 +867,24 @@ void launch_scatter_positions(djb_solver* s, const float* xr, int64_t count, flo
 
 template <int W, int R>
 void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
+    if (R > 0 && s->tiled && a.perm) {
+        constexpr int RR = R > 0 ? R : 1;
+        const size_t smem = brick_smem(s, RR);
+        if (ns == 1)
+            djb::k_gather_brick<W, RR, 1><<<unsigned(s->nbins), djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
+        else
+            djb::k_gather_brick<W, RR, 2><<<unsigned(s->nbins), djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
+        return;
+    }
     if (R > 0 && s->tiled) {
         constexpr int RR = R > 0 ? R : 1;
         const size_t smem = kGatherBudget * sizeof(float);
+        const dim3 grid = a.perm ? dim3(unsigned((s->np + djb::kTileThreads - 1) / djb::kTileThreads))
+                                 : tile_grid(s->n);
         if (ns == 1)
-            djb::k_gather_tiled<W, RR, 1><<<tile_grid(s->n), djb::kTileThreads, smem, s->stream>>>(a, kGatherBudget);
+            djb::k_gather_tiled<W, RR, 1><<<grid, djb::kTileThreads, smem, s->stream>>>(a, kGatherBudget);
         else
-            djb::k_gather_tiled<W, RR, 2><<<tile_grid(s->n), djb::kTileThreads, smem, s->stream>>>(a, kGatherBudget);
+            djb::k_gather_tiled<W, RR, 2><<<grid, djb::kTileThreads, smem, s->stream>>>(a, kGatherBudget);
         return;
     }
     if (ns == 1) djb::k_gather<W, R, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(a);
@@ -857,6 +897,8 @@ int tiled_attrs_wr() {
     const int smem = kGatherBudget * int(sizeof(float));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     return DJB_OK;
 }
 
@@ -865,6 +907,8 @@ int scatter_attrs_w() {
     const int smem = kScatterBudget * int(sizeof(unsigned int));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_tiled<W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_tiled<W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     return DJB_OK;
 }
 
@@ -942,11 +986,30 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
 
 // Force evaluation for all shifts; if `step`, fused with the drift/kick/drift.
 // Reads s->psi (and s->mom). Output: s->acc (step == 0) or updated psi/mom.
+// Brick sort of the particles at X = q + Ψ (+ dd1·Mom when `mom`): perm (sort.cuh).
+int sort_particles(djb_solver* s, const float* mom, float dd1) {
+    s->prof.begin(s->stream, PH_SORT);
+    CUDA_TRY(cudaMemsetAsync(s->count, 0, size_t(s->nbins) * sizeof(unsigned), s->stream));
+    djb::k_bin<<<blocks(s->np), 256, 0, s->stream>>>(s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->sg, s->count,
+                                                      s->keyrank, s->err);
+    djb::k_scan_block<<<s->nscan, djb::kScanThreads, 0, s->stream>>>(s->count, s->nbins, s->offset, s->bsum);
+    djb::k_scan_sums<<<1, djb::kScanThreads, 0, s->stream>>>(s->bsum, s->nscan);
+    djb::k_place<<<blocks(s->np), 256, 0, s->stream>>>(s->keyrank, s->np, s->offset, s->bsum, s->perm);
+    s->prof.end(s->stream, PH_SORT, 4);
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
 int force(djb_solver* s, bool step, double dd1, double alpha, double beta, double dd2) {
     const int nh = s->res / 2 + 1;
     const int64_t nspec = int64_t(s->res) * s->res * nh;
     const bool ik = (s->cfg.grad_order == 0);
     const bool resample = (s->cfg.n_resample > 1);
+    s->cur_perm = nullptr;
+    if (s->tiled && s->sorted) {
+        TRY(sort_particles(s, step ? s->mom : nullptr, float(dd1)));
+        s->cur_perm = s->perm;
+    }
     for (int first = 0; first < s->nshift; first += s->group) {
         const int ns = std::min(s->group, s->nshift - first);
         const GroupShifts g = group_shifts(s, first, ns);
@@ -954,7 +1017,8 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         for (int m = 0; m < ns; ++m)
             CUDA_TRY(cudaMemsetAsync(s->mesh[m], 0, size_t(s->mesh_floats) * sizeof(float), s->stream));
         s->prof.end(s->stream, PH_CLEAR, 0);
-        const bool drift_here = step && first == 0;
+        // with the brick sort the binning pass has applied the first drift already
+        const bool drift_here = step && first == 0 && !s->cur_perm;
         s->prof.begin(s->stream, PH_SCATTER);
         launch_scatter(s, drift_here ? s->mom : nullptr, float(dd1), g, ns);
         s->prof.end(s->stream, PH_SCATTER, 1);
@@ -1019,6 +1083,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         a.beta = float(beta);
         a.dd2 = float(dd2);
         a.err = s->err;
+        a.perm = s->cur_perm;
         s->prof.begin(s->stream, PH_GATHER);
         launch_gather(s, a, ns);
         s->prof.end(s->stream, PH_GATHER, 1);
@@ -1089,6 +1154,10 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         s->tiled = !(kind && std::strcmp(kind, "simple") == 0);
     }
     if (s->tiled) TRY(tiled_attrs(s->W, s->R));
+    {
+        const char* srt = std::getenv("DJB_SORT");
+        s->sorted = s->tiled && !(srt && std::strcmp(srt, "0") == 0);
+    }
     s->shifts = aa_shifts(cfg->antialias, 0.5 * s->L / s->res);
     s->nshift = int(s->shifts.size() / 3);
     const bool resample = cfg->n_resample > 1;
@@ -1164,6 +1233,26 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                 TRY(dmalloc(s, (void**)&s->fmesh[m][c], size_t(s->mesh_floats) * sizeof(float)));
     }
     TRY(dmalloc(s, (void**)&s->err, sizeof(int)));
+    if (s->sorted) {
+        // bricks of 16^3 cells; smaller when the box (brick + W + 2 + 2R nodes) would not
+        // stay well inside the periodic mesh (brick_rel needs res > box + 4)
+        int brick = 16, lgb = 4;
+        while (brick > 2 && (brick > s->res / 2 || brick + s->W + 2 + 2 * s->R + 4 >= s->res)) {
+            brick /= 2;
+            --lgb;
+        }
+        const int nb = (s->res + brick - 1) / brick;
+        s->sg = djb::SortGeom{s->res, brick, lgb, nb};
+        s->nbins = int64_t(nb) * nb * nb;
+        if (brick_smem(s, s->R) > size_t(kGatherBudget) * 4 || brick_smem(s, 0) > size_t(kScatterBudget) * 4)
+            return fail(DJB_ERR_INVALID, "brick box exceeds the shared-memory budget");
+        s->nscan = int((s->nbins + djb::kScanBlock - 1) / djb::kScanBlock);
+        TRY(dmalloc(s, (void**)&s->count, sizeof(unsigned) * size_t(s->nbins)));
+        TRY(dmalloc(s, (void**)&s->offset, sizeof(unsigned) * size_t(s->nbins)));
+        TRY(dmalloc(s, (void**)&s->bsum, sizeof(unsigned) * size_t(s->nscan)));
+        TRY(dmalloc(s, (void**)&s->keyrank, sizeof(uint2) * size_t(s->np)));
+        TRY(dmalloc(s, (void**)&s->perm, sizeof(int) * size_t(s->np)));
+    }
     CUDA_TRY(cudaMemset(s->err, 0, sizeof(int)));
     size_t work = 0;
     TRY(make_plan(&s->r2c, &s->have_r2c, res, CUFFT_R2C, s->stream, &work));
@@ -1412,6 +1501,7 @@ int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cu
     CUDA_TRY(cudaSetDevice(s->cfg.device));
     CUDA_TRY(cudaMemsetAsync(s->mesh[0], 0, size_t(s->mesh_floats) * sizeof(float), s->stream));
     GroupShifts g{};
+    s->cur_perm = nullptr;  // the P(k) deposit uses Lagrangian tiles
     launch_scatter_t<2, 1>(s, nullptr, 0.0f, g, s->mesh[0], nullptr);
     CUDA_TRY(cudaGetLastError());
     *mesh_out = s->mesh[0];

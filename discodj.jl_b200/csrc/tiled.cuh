@@ -1,7 +1,8 @@
 // Shared-memory tiled mass assignment and force interpolation.
 //
-// A CTA owns a Lagrangian tile of kTX x kTY x kTZ particles (consecutive i, j, k of
-// the particle lattice; no sort). Its particles' W-node stencils cover an Eulerian
+// A CTA owns a tile of 256 particles: either 256 consecutive entries of the brick
+// sort (`perm`, sort.cuh) or, without a sort, a Lagrangian tile of kTX x kTY x kTZ
+// particles (consecutive i, j, k of the particle lattice). Its particles' W-node stencils cover an Eulerian
 // box that the CTA sizes from a min/max reduction of their base nodes (relative to
 // the tile's first particle, periodic differences unwrapped). The box is processed
 // in z-chunks that fit the shared-memory budget:
@@ -135,20 +136,46 @@ struct FixScale {
 #define DJB_SCATTER_MIN_BLOCKS 2
 #endif
 
+// The particle a thread of the tile handles: the tile's sorted slot, or its lattice cell.
+struct TileParticle {
+    int i, j, k;
+    int64_t p;
+    bool active;
+};
+
+__device__ __forceinline__ TileParticle tile_particle(const int* __restrict__ perm, int n, int64_t np) {
+    TileParticle t;
+    const int tid = threadIdx.x;
+    if (perm) {
+        const int64_t slot = int64_t(blockIdx.x) * kTileThreads + tid;
+        t.active = slot < np;  // slot 0 of every tile exists, so thread 0 is active
+        t.p = t.active ? int64_t(perm[slot]) : 0;
+        t.i = int(t.p % n);
+        t.j = int((t.p / n) % n);
+        t.k = int(t.p / (int64_t(n) * n));
+    } else {
+        t.i = blockIdx.x * kTX + (tid % kTX);
+        t.j = blockIdx.y * kTY + ((tid / kTX) % kTY);
+        t.k = blockIdx.z * kTZ + (tid / (kTX * kTY));
+        t.active = (t.i < n) && (t.j < n) && (t.k < n);
+        t.p = t.active ? int64_t(t.i) + int64_t(n) * (t.j + int64_t(n) * t.k) : 0;
+    }
+    return t;
+}
+
 template <int W, int NS>
 __global__ void __launch_bounds__(kTileThreads, DJB_SCATTER_MIN_BLOCKS) k_scatter_tiled(
     float* __restrict__ psi, const float* __restrict__ mom, float dd1, const float* __restrict__ q1, int n,
     int64_t np, float L, int res, int pitch, GroupShifts sh, float* __restrict__ mesh0,
-    float* __restrict__ mesh1, int* err, int budget) {
+    float* __restrict__ mesh1, int* err, int budget, const int* __restrict__ perm) {
     extern __shared__ unsigned int sacc[];
     __shared__ int s_row[kMaxRows];
     __shared__ int s_col[kMaxCols];
     const int tid = threadIdx.x;
-    const int i = blockIdx.x * kTX + (tid % kTX);
-    const int j = blockIdx.y * kTY + ((tid / kTX) % kTY);
-    const int k = blockIdx.z * kTZ + (tid / (kTX * kTY));
-    const bool active = (i < n) && (j < n) && (k < n);
-    const int64_t p = active ? int64_t(i) + int64_t(n) * (j + int64_t(n) * k) : 0;
+    const TileParticle tp = tile_particle(perm, n, np);
+    const int i = tp.i, j = tp.j, k = tp.k;
+    const bool active = tp.active;
+    const int64_t p = tp.p;
     float X[3] = {0.0f, 0.0f, 0.0f};
     if (active) {
         float ps[3] = {psi[p], psi[p + np], psi[p + 2 * np]};
@@ -265,11 +292,10 @@ __global__ void __launch_bounds__(kTileThreads, DJB_GATHER_MIN_BLOCKS) k_gather_
     const int n = A.n;
     const int64_t np = A.np;
     const int res = A.res;
-    const int i = blockIdx.x * kTX + (tid % kTX);
-    const int j = blockIdx.y * kTY + ((tid / kTX) % kTY);
-    const int k = blockIdx.z * kTZ + (tid / (kTX * kTY));
-    const bool active = (i < n) && (j < n) && (k < n);
-    const int64_t p = active ? int64_t(i) + int64_t(n) * (j + int64_t(n) * k) : 0;
+    const TileParticle tp = tile_particle(A.perm, n, np);
+    const int i = tp.i, j = tp.j, k = tp.k;
+    const bool active = tp.active;
+    const int64_t p = tp.p;
     float ps[3] = {0.0f, 0.0f, 0.0f};
     float acc[3] = {0.0f, 0.0f, 0.0f};
     if (active) {

@@ -169,7 +169,7 @@ class PMSolver:
     def synchronize(self):
         check(lib.djb_synchronize(self._h))
 
-    PHASES = ("clear", "scatter", "resample", "r2c", "kspace", "c2r", "gather")
+    PHASES = ("clear", "scatter", "resample", "r2c", "kspace", "c2r", "gather", "sort")
 
     def profile(self, enable: bool = True):
         """Start (or stop) per-phase CUDA-event timing; resets the sums."""

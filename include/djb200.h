@@ -160,11 +160,11 @@ DJB_API int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wr
 /* Per-phase timing with CUDA events on the solver's stream (enable = 1) and launch
  * counts of this library's kernels. Phases: 0 mesh clear, 1 mass assignment,
  * 2 sheet resampling, 3 R2C, 4 k-space multiply, 5 C2R, 6 force interpolation
- * (fused kick-drift). Enabling or disabling resets the sums. */
+ * (fused kick-drift), 7 particle brick sort. Enabling or disabling resets the sums. */
 DJB_API int djb_solver_profile(djb_solver* s, int32_t enable);
 /* Reads and resets the sums: ms[phase] device milliseconds (0 when timing is off),
  * launches[phase] kernel launches of this library, calls[phase] phase executions.
- * nphase >= 7. */
+ * nphase >= 8. */
 DJB_API int djb_solver_profile_read(djb_solver* s, double* ms, int64_t* launches, int64_t* calls,
                                     int32_t nphase);
 /* Waits for the solver's queued work and reports a device-side error word, if any. */
