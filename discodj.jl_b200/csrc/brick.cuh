@@ -21,17 +21,24 @@ namespace djb {
 constexpr int kBrickRounds = 4;  // particles kept in registers per thread (interpolation)
 
 struct BrickList {
-    const unsigned* count;   // particles per brick
-    const unsigned* offset;  // block-local exclusive scan of count
+    const unsigned* offset;  // block-local exclusive scan of the key counts
     const unsigned* bsum;    // scan of the block totals
-    const int* perm;         // particles in brick order
+    const int* perm;         // particles in key order
     int nb;                  // bricks per axis
     int brick;               // cells per brick side
+    int nsub;                // sort keys per brick (2^3-cell sub-blocks)
+    int64_t nkeys;           // keys in total
+    unsigned np;             // particles
 };
 
+__device__ __forceinline__ unsigned key_start(const BrickList& bl, int64_t key) {
+    return key >= bl.nkeys ? bl.np : bl.offset[key] + bl.bsum[key / kScanBlock];
+}
+
+// Sorted range [start, start + cnt) of the particles of brick b.
 __device__ __forceinline__ void brick_range(const BrickList& bl, int b, unsigned& start, unsigned& cnt) {
-    cnt = bl.count[b];
-    start = bl.offset[b] + bl.bsum[b / kScanBlock];
+    start = key_start(bl, int64_t(b) * bl.nsub);
+    cnt = key_start(bl, int64_t(b + 1) * bl.nsub) - start;
 }
 
 // Box of brick b: origin B*b + lo - R - 1 per axis, S = B + W + 2 + 2R nodes per axis.
@@ -85,7 +92,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
         for (int t = tid; t < cells; t += kTileThreads) sacc[t] = 0u;
         __syncthreads();
         for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
-            const unsigned slot = r0 + tid;
+            // lanes 8 slots apart: particles of one cell land in different warps, which
+            // keeps same-address shared atomics out of a single instruction
+            const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
             if (slot >= cnt) continue;
             const int64_t p = bl.perm[start + slot];
             const int i = int(p % n), j = int((p / n) % n), k = int(p / (int64_t(n) * n));

@@ -817,7 +817,9 @@ dim3 tile_grid(int n) {
 }
 
 djb::BrickList brick_list(const djb_solver* s) {
-    return djb::BrickList{s->count, s->offset, s->bsum, s->perm, s->sg.nb, s->sg.brick};
+    const int hb = s->sg.hb;
+    return djb::BrickList{s->offset, s->bsum, s->perm, s->sg.nb, s->sg.brick, hb * hb * hb, s->nbins,
+                          unsigned(s->np)};
 }
 
 // Shared memory of the brick kernels: the fixed box, B + W + 2 (+ 2R) nodes per axis.
@@ -830,7 +832,8 @@ template <int W, int NS>
 void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, float* m0,
                       float* m1) {
     if (s->tiled && s->cur_perm) {  // brick-owned: the drift was applied by the binning pass
-        djb::k_scatter_brick<W, NS><<<unsigned(s->nbins), djb::kTileThreads, brick_smem(s, 0), s->stream>>>(
+        const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
+        djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, brick_smem(s, 0), s->stream>>>(
             s->psi, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err, brick_list(s));
         return;
     }
@@ -870,10 +873,11 @@ void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
     if (R > 0 && s->tiled && a.perm) {
         constexpr int RR = R > 0 ? R : 1;
         const size_t smem = brick_smem(s, RR);
+        const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         if (ns == 1)
-            djb::k_gather_brick<W, RR, 1><<<unsigned(s->nbins), djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
+            djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
         else
-            djb::k_gather_brick<W, RR, 2><<<unsigned(s->nbins), djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
+            djb::k_gather_brick<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
         return;
     }
     if (R > 0 && s->tiled) {
@@ -1242,8 +1246,11 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
             --lgb;
         }
         const int nb = (s->res + brick - 1) / brick;
-        s->sg = djb::SortGeom{s->res, brick, lgb, nb};
-        s->nbins = int64_t(nb) * nb * nb;
+        const int hb = brick > 2 ? brick / 2 : 1;
+        s->sg = djb::SortGeom{s->res, brick, lgb, nb, hb};
+        s->nbins = int64_t(nb) * nb * nb * hb * hb * hb;  // keys: bricks x 2^3-cell sub-blocks
+        if (s->nbins > int64_t(djb::kScanBlock) * djb::kScanThreads * 64)
+            return fail(DJB_ERR_INVALID, "mesh too large for the particle sort (%lld keys)", (long long)s->nbins);
         if (brick_smem(s, s->R) > size_t(kGatherBudget) * 4 || brick_smem(s, 0) > size_t(kScatterBudget) * 4)
             return fail(DJB_ERR_INVALID, "brick box exceeds the shared-memory budget");
         s->nscan = int((s->nbins + djb::kScanBlock - 1) / djb::kScanBlock);

@@ -23,20 +23,25 @@ struct SortGeom {
     int brick;   // cells per brick side (power of two)
     int lgb;     // log2(brick)
     int nb;      // bricks per axis
+    int hb;      // sub-blocks of 2 cells per brick side (brick / 2, at least 1)
 };
 
-// Linear index of the brick holding floor(g) (the shift-0 cell; the brick kernels'
-// boxes have one node of margin for the half-cell shift and odd-order rounding).
+// Sort key of the cell floor(g) (the shift-0 cell; the brick kernels' boxes have one
+// node of margin for the interlacing shifts and odd-order rounding): the linear brick
+// index, then the 2^3-cell sub-block inside the brick, so that particles of one cell
+// are consecutive in the sorted order.
 __device__ __forceinline__ uint32_t brick_key(const float X[3], float L, float resf, const SortGeom& sg, int* err) {
-    int bc[3];
+    int bc[3], sc[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float g = grid_coord(X[a], L, resf, err);
         int c = __float2int_rd(g);
         c = c < 0 ? 0 : (c >= sg.res ? sg.res - 1 : c);
         bc[a] = c >> sg.lgb;
+        sc[a] = (sg.hb > 1) ? ((c & (sg.brick - 1)) >> 1) : 0;
     }
-    return uint32_t((bc[2] * sg.nb + bc[1]) * sg.nb + bc[0]);
+    const uint32_t brick = uint32_t((bc[2] * sg.nb + bc[1]) * sg.nb + bc[0]);
+    return brick * uint32_t(sg.hb * sg.hb * sg.hb) + uint32_t((sc[2] * sg.hb + sc[1]) * sg.hb + sc[0]);
 }
 
 // Applies the first drift Ψ <- Ψ + dd1·Mom when `mom` is given (written back), then
