@@ -15,6 +15,7 @@
 
 #include "tiled.cuh"
 #include "sort.cuh"
+#include "tma.cuh"
 
 namespace djb {
 
@@ -29,6 +30,7 @@ struct BrickList {
     int nsub;                // sort keys per brick (2^3-cell sub-blocks)
     int64_t nkeys;           // keys in total
     unsigned np;             // particles
+    int sx;                  // interpolation box width along x (gather_box)
 };
 
 __device__ __forceinline__ unsigned key_start(const BrickList& bl, int64_t key) {
@@ -138,11 +140,63 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
 }
 
 // ── force interpolation (finite-difference gradient of order 2R) ─────────────
+// Interpolation box of brick b: y and z as brick_box (S = B + W + 2 + 2R nodes); the x
+// origin is rounded down to a multiple of 4 nodes so that every box row starts on a
+// 16-byte boundary of a dense mesh, and the box is bl.sx nodes wide (a multiple of 4,
+// at least S + 3). Shared memory holds the box densely, [z][y][x] with rows of sx floats.
+__device__ __forceinline__ TileBox gather_box(const BrickList& bl, int b, int lo_minus_r, int S) {
+    TileBox box = brick_box(bl, b, lo_minus_r, S);
+    box.o[0] &= ~3;
+    box.S[0] = bl.sx;
+    box.P = bl.sx;
+    box.plane = bl.sx * S;
+    return box;
+}
+
+__device__ __forceinline__ bool box_inside(const TileBox& box, int res) {
+    return box.o[0] >= 0 && box.o[0] + box.S[0] <= res && box.o[1] >= 0 && box.o[1] + box.S[1] <= res &&
+           box.o[2] >= 0 && box.o[2] + box.S[2] <= res;
+}
+
+// Stages the potential over `box` with asynchronous copies that take the periodic wrap
+// per element: 16-byte chunks when every row of the mesh starts on a 16-byte boundary
+// (`vec`: pitch and res multiples of 4; chunks never straddle the wrap), else floats.
+__device__ __forceinline__ void stage_box_wrapped(float* sbox, const float* __restrict__ phi, const TileBox& box,
+                                                  int res, int pitch, bool vec) {
+    const int S1 = box.S[1];
+    FastDiv fy;
+    fy.init(S1);
+    const int per = vec ? 4 : 1;
+    const int cpr = box.S[0] / per;  // copies per row
+    FastDiv fc;
+    fc.init(cpr);
+    const int total = cpr * S1 * box.S[2];
+    for (int t = threadIdx.x; t < total; t += kTileThreads) {
+        const int r = fc.div(t);
+        const int c = t - r * cpr;
+        const int z = fy.div(r);
+        const int y = r - z * S1;
+        const int gx = wrap2(box.o[0] + per * c, res);
+        const int gy = wrap2(box.o[1] + y, res);
+        const int gz = wrap2(box.o[2] + z, res);
+        const float* src = phi + (int64_t(gz) * res + gy) * pitch + gx;
+        const unsigned sa = smem_u32(sbox + r * box.S[0] + per * c);
+        if (vec)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src));
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src));
+    }
+    asm volatile("cp.async.wait_all;\n" ::);
+}
+
+// `tma` != 0: the potentials are dense [res]^3 meshes (pitch == res) described by tm0/tm1
+// (box sx x S x S); boxes that do not wrap are then fetched with one bulk tensor copy.
 template <int W, int R, int NS>
-__global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, BrickList bl) {
-    extern __shared__ float sbox[];
-    __shared__ int s_row[kMaxRows];
-    __shared__ int s_col[kMaxCols];
+__global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, BrickList bl,
+                                                                  const __grid_constant__ CUtensorMap tm0,
+                                                                  const __grid_constant__ CUtensorMap tm1, int tma) {
+    extern __shared__ __align__(128) float sbox[];
+    __shared__ __align__(8) uint64_t s_bar;
     constexpr int E = W + 2 * R;
     const int b = blockIdx.x;
     unsigned start, cnt;
@@ -152,13 +206,13 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, 
     const int n = A.n;
     const int64_t np = A.np;
     const int res = A.res;
-    const TileBox box = brick_box(bl, b, WLo<W>::v - R, bl.brick + W + 2 + 2 * R);
-    box_columns(box, res, s_col);
-    chunk_rows(box, res, 0, box.S[2], s_row);
-    __syncthreads();  // the row and column tables are read by every thread below
-    FastDiv fp;
-    fp.init(box.P);
-    const int cells = box.plane * box.S[2];
+    const TileBox box = gather_box(bl, b, WLo<W>::v - R, bl.brick + W + 2 + 2 * R);
+    const bool bulk = tma && box_inside(box, res);
+    const bool vec = ((A.pitch | res) & 3) == 0;
+    const unsigned box_bytes = unsigned(box.plane) * unsigned(box.S[2]) * 4u;
+    if (bulk && tid == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    unsigned parity = 0;
     const float resf = float(res);
     const float cc[4] = {0.0f, A.c1, A.c2, A.c3};
     for (unsigned sr = 0; sr < cnt; sr += kTileThreads * kBrickRounds) {
@@ -185,18 +239,23 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, 
         }
 #pragma unroll 1
         for (int g = 0; g < NS; ++g) {
-            const float* phi = (g == 0) ? A.mesh[0] : A.mesh[NS > 1 ? 1 : 0];
             const Shift3 sgs = (g == 0) ? A.sh.s[0] : A.sh.s[NS > 1 ? 1 : 0];
-            for (int t = tid; t < cells; t += kTileThreads) {
-                const int r = fp.div(t);
-                const int x = t - r * box.P;
-                if (x >= box.S[0]) continue;
-                const float* src = phi + int64_t(s_row[r]) * A.pitch + s_col[x];
-                const unsigned sa = unsigned(__cvta_generic_to_shared(sbox + t));
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src));
+            if (bulk) {
+                if (tid == 0) {
+                    fence_proxy_async_smem();  // the previous shift's reads precede the refill
+                    mbar_arrive_expect_tx(&s_bar, box_bytes);
+                    tma_load_3d(sbox, (g == 0) ? &tm0 : &tm1, box.o[0], box.o[1], box.o[2], &s_bar);
+                }
+                const bool ok = mbar_wait(&s_bar, parity);
+                parity ^= 1u;
+                if (__syncthreads_or(!ok)) {  // the copy never completed: report, do not spin
+                    if (tid == 0) atomicOr(A.err, 8);
+                    return;
+                }
+            } else {
+                stage_box_wrapped(sbox, (g == 0) ? A.mesh[0] : A.mesh[NS > 1 ? 1 : 0], box, res, A.pitch, vec);
+                __syncthreads();
             }
-            asm volatile("cp.async.wait_all;\n" ::);
-            __syncthreads();
 #pragma unroll 1
             for (int r = 0; r < kBrickRounds; ++r) {
                 if (pr[r] < 0) continue;

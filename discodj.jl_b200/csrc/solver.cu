@@ -14,6 +14,8 @@
 //                  the potential inside the gather; the last group finishes the
 //                  mean over shifts, the kick Mom = a*Mom + b*acc and the drift
 //                  Psi += dd2*Mom
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -193,21 +195,28 @@ __device__ __forceinline__ float kphi(const double* __restrict__ T, const double
 }
 
 // fd <- Kφ·fd in place on a half spectrum [kz][ky][kx], kx in [0, res/2] (pm.jl:317-320,632).
+// Grid (ceil(res / kSpecRows), res): a block takes kSpecRows rows of one kz plane as one
+// flat run of kSpecRows·nh modes, so the row index is a 32-bit multiply-high division
+// (exact: e·nh < 2^32).
+constexpr int kSpecRows = 8;
 __global__ void __launch_bounds__(kThreads) k_kspace_mul(float2* __restrict__ f, int res,
                                                           const double* __restrict__ T,
                                                           const double* __restrict__ M, double s0) {
     const int nh = res / 2 + 1;
-    const int64_t total = int64_t(res) * res * nh;
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-         t += int64_t(gridDim.x) * blockDim.x) {
-        const int kx = int(t % nh);
-        const int ky = int((t / nh) % res);
-        const int kz = int(t / (int64_t(nh) * res));
-        const float K = kphi(T, M, s0, kx, ky, kz);
-        float2 v = f[t];
+    const int kz = blockIdx.y;
+    const int ky0 = blockIdx.x * kSpecRows;
+    const int nrow = min(kSpecRows, res - ky0);
+    const int cnt = nrow * nh;
+    const unsigned inv = 0xffffffffu / unsigned(nh) + 1u;
+    float2* __restrict__ run = f + (int64_t(kz) * res + ky0) * nh;
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        const int rl = int(__umulhi(unsigned(e), inv));
+        const int kx = e - rl * nh;
+        const float K = kphi(T, M, s0, kx, ky0 + rl, kz);
+        float2 v = run[e];
         v.x *= K;
         v.y *= K;
-        f[t] = v;
+        run[e] = v;
     }
 }
 
@@ -700,14 +709,21 @@ struct djb_solver {
 
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    cufftHandle r2c = 0, c2r = 0, r2c_n = 0, c2r_n = 0;
-    bool have_r2c = false, have_c2r = false, have_r2c_n = false, have_c2r_n = false;
+    cufftHandle r2c = 0, c2r = 0, r2c_n = 0, c2r_n = 0, c2r_d = 0;
+    bool have_r2c = false, have_c2r = false, have_r2c_n = false, have_c2r_n = false, have_c2r_d = false;
 
     float* psi = nullptr;
     float* mom = nullptr;
     float* acc = nullptr;
     float* q1 = nullptr;
     float* mesh[kMaxGroup] = {nullptr, nullptr};
+    // dense [res]^3 potentials (finite-difference gradients, res % 4 == 0, not lean): the
+    // C2R writes them out of place, and the brick interpolation fetches its boxes from
+    // them with bulk tensor copies described by `tmap`
+    float* phi[kMaxGroup] = {nullptr, nullptr};
+    CUtensorMap tmap[kMaxGroup];
+    bool tma = false;
+    int gsx = 0;  // interpolation box width along x (brick kernels)
     float* fmesh[kMaxGroup][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     double* lapT = nullptr;
     double* makT = nullptr;
@@ -819,13 +835,53 @@ dim3 tile_grid(int n) {
 djb::BrickList brick_list(const djb_solver* s) {
     const int hb = s->sg.hb;
     return djb::BrickList{s->offset, s->bsum, s->perm, s->sg.nb, s->sg.brick, hb * hb * hb, s->nbins,
-                          unsigned(s->np)};
+                          unsigned(s->np), s->gsx};
 }
 
-// Shared memory of the brick kernels: the fixed box, B + W + 2 (+ 2R) nodes per axis.
+// Shared memory of the brick mass assignment: the fixed box, B + W + 2 nodes per axis.
 size_t brick_smem(const djb_solver* s, int halo) {
     const int S = s->sg.brick + s->W + 2 + 2 * halo;
     return size_t(S | 1) * S * S * 4;
+}
+
+// Interpolation box width along x for bricks of `brick` cells: the S = B + W + 2 + 2R
+// nodes of a box start anywhere in a 16-byte group after the rounded-down origin, so
+// S + 3 nodes rounded up to a multiple of 4; a width of 4 mod 8 keeps the rows of one
+// plane on different shared-memory banks.
+int gather_sx(int brick, int W, int R) {
+    int sx = (brick + W + 2 + 2 * R + 6) & ~3;
+    if (sx % 8 == 0) sx += 4;
+    return sx;
+}
+
+size_t gather_smem(const djb_solver* s) {
+    const int S = s->sg.brick + s->W + 2 + 2 * s->R;
+    return size_t(s->gsx) * S * S * 4;
+}
+
+// 2 CTAs of the brick interpolation per SM: 228 KB of shared memory less 1 KB per CTA
+// reserved by the runtime and the kernel's static barrier.
+constexpr int kBrickGatherMax = 113 * 1024;
+
+// Tensor map of a dense [res]^3 float mesh with boxes of sx x S x S elements.
+int make_tmap(CUtensorMap* m, const float* base, int res, int sx, int S) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[3] = {cuuint64_t(res), cuuint64_t(res), cuuint64_t(res)};
+    const cuuint64_t strides[2] = {cuuint64_t(res) * 4, cuuint64_t(res) * res * 4};
+    const cuuint32_t box[3] = {cuuint32_t(sx), cuuint32_t(S), cuuint32_t(S)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+    return DJB_OK;
 }
 
 template <int W, int NS>
@@ -872,12 +928,15 @@ template <int W, int R>
 void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
     if (R > 0 && s->tiled && a.perm) {
         constexpr int RR = R > 0 ? R : 1;
-        const size_t smem = brick_smem(s, RR);
+        const size_t smem = gather_smem(s);
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
+        const int tma = (s->tma && a.mesh[0] == s->phi[0]) ? 1 : 0;
         if (ns == 1)
-            djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
+            djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
+                a, brick_list(s), s->tmap[0], s->tmap[0], tma);
         else
-            djb::k_gather_brick<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(a, brick_list(s));
+            djb::k_gather_brick<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
+                a, brick_list(s), s->tmap[0], s->tmap[1], tma);
         return;
     }
     if (R > 0 && s->tiled) {
@@ -901,8 +960,14 @@ int tiled_attrs_wr() {
     const int smem = kGatherBudget * int(sizeof(float));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kBrickGatherMax));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kBrickGatherMax));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  int(cudaSharedmemCarveoutMaxShared)));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  int(cudaSharedmemCarveoutMaxShared)));
     return DJB_OK;
 }
 
@@ -1039,11 +1104,13 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             s->prof.end(s->stream, PH_R2C, 0);
             if (!ik) {
                 s->prof.begin(s->stream, PH_KSPACE);
-                djb::k_kspace_mul<<<grid_for(nspec), kThreads, 0, s->stream>>>(
+                djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)),
+                                    kThreads, 0, s->stream>>>(
                     reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
                 s->prof.end(s->stream, PH_KSPACE, 1);
                 s->prof.begin(s->stream, PH_C2R);
-                CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
+                if (s->phi[m]) CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+                else CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
                 s->prof.end(s->stream, PH_C2R, 0);
             } else {
                 s->prof.begin(s->stream, PH_KSPACE);
@@ -1065,7 +1132,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         a.acc = s->acc;
         a.q1 = s->q1;
         for (int m = 0; m < ns; ++m) {
-            a.mesh[m] = ik ? s->fmesh[m][0] : s->mesh[m];
+            a.mesh[m] = ik ? s->fmesh[m][0] : (s->phi[m] ? s->phi[m] : s->mesh[m]);
             a.meshy[m] = ik ? s->fmesh[m][1] : nullptr;
             a.meshz[m] = ik ? s->fmesh[m][2] : nullptr;
         }
@@ -1074,7 +1141,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         a.np = s->np;
         a.L = s->Lf;
         a.res = s->res;
-        a.pitch = s->pitch;
+        a.pitch = (!ik && s->phi[0]) ? s->res : s->pitch;
         a.c1 = s->c1;
         a.c2 = s->c2;
         a.c3 = s->c3;
@@ -1131,6 +1198,7 @@ void release(djb_solver* s) {
     if (s->have_c2r) cufftDestroy(s->c2r);
     if (s->have_r2c_n) cufftDestroy(s->r2c_n);
     if (s->have_c2r_n) cufftDestroy(s->c2r_n);
+    if (s->have_c2r_d) cufftDestroy(s->c2r_d);
     for (void* p : s->allocs) cudaFree(p);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     if (prev >= 0) cudaSetDevice(prev);
@@ -1238,20 +1306,22 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
     }
     TRY(dmalloc(s, (void**)&s->err, sizeof(int)));
     if (s->sorted) {
-        // bricks of 16^3 cells; smaller when the box (brick + W + 2 + 2R nodes) would not
-        // stay well inside the periodic mesh (brick_rel needs res > box + 4)
+        // bricks of 16^3 cells; smaller when a box (brick + W + 2 + 2R nodes, sx along x)
+        // would not stay well inside the periodic mesh (box_rel needs res > extent + 4)
         int brick = 16, lgb = 4;
-        while (brick > 2 && (brick > s->res / 2 || brick + s->W + 2 + 2 * s->R + 4 >= s->res)) {
+        while (brick > 2 && (brick > s->res / 2 || brick + s->W + 2 + 2 * s->R + 4 >= s->res ||
+                             (s->R > 0 && gather_sx(brick, s->W, s->R) + 4 >= s->res))) {
             brick /= 2;
             --lgb;
         }
+        s->gsx = gather_sx(brick, s->W, s->R);
         const int nb = (s->res + brick - 1) / brick;
         const int hb = brick > 2 ? brick / 2 : 1;
         s->sg = djb::SortGeom{s->res, brick, lgb, nb, hb};
         s->nbins = int64_t(nb) * nb * nb * hb * hb * hb;  // keys: bricks x 2^3-cell sub-blocks
         if (s->nbins > int64_t(djb::kScanBlock) * djb::kScanThreads * 64)
             return fail(DJB_ERR_INVALID, "mesh too large for the particle sort (%lld keys)", (long long)s->nbins);
-        if (brick_smem(s, s->R) > size_t(kGatherBudget) * 4 || brick_smem(s, 0) > size_t(kScatterBudget) * 4)
+        if (gather_smem(s) > size_t(kBrickGatherMax) || brick_smem(s, 0) > size_t(kScatterBudget) * 4)
             return fail(DJB_ERR_INVALID, "brick box exceeds the shared-memory budget");
         s->nscan = int((s->nbins + djb::kScanBlock - 1) / djb::kScanBlock);
         TRY(dmalloc(s, (void**)&s->count, sizeof(unsigned) * size_t(s->nbins)));
@@ -1266,6 +1336,26 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
     s->bytes += int64_t(work);
     TRY(make_plan(&s->c2r, &s->have_c2r, res, CUFFT_C2R, s->stream, &work));
     s->bytes += int64_t(work);
+    if (!ik && !cfg->lean && res % 4 == 0) {
+        // dense potentials written by an out-of-place C2R from the (padded) spectrum
+        for (int m = 0; m < s->group; ++m)
+            TRY(dmalloc(s, (void**)&s->phi[m], sizeof(float) * size_t(res) * res * res));
+        CUFFT_TRY(cufftCreate(&s->c2r_d));
+        s->have_c2r_d = true;
+        long long dims[3] = {res, res, res};
+        long long cembed[3] = {res, res, res / 2 + 1};
+        long long dembed[3] = {res, res, res};
+        CUFFT_TRY(cufftMakePlanMany64(s->c2r_d, 3, dims, cembed, 1, cembed[0] * cembed[1] * cembed[2], dembed, 1,
+                                      dembed[0] * dembed[1] * dembed[2], CUFFT_C2R, 1, &work));
+        CUFFT_TRY(cufftSetStream(s->c2r_d, s->stream));
+        s->bytes += int64_t(work);
+        const int S = s->sg.brick + s->W + 2 + 2 * s->R;
+        if (s->sorted && s->gsx <= res && S <= res) {
+            for (int m = 0; m < s->group; ++m) TRY(make_tmap(&s->tmap[m], s->phi[m], res, s->gsx, S));
+            for (int m = s->group; m < kMaxGroup; ++m) s->tmap[m] = s->tmap[0];
+            s->tma = true;
+        }
+    }
     if (resample) {
         const int n = s->n, nh = n / 2 + 1;
         const int64_t nspec = int64_t(n) * n * nh;
@@ -1337,6 +1427,7 @@ int djb_solver_set_stream(djb_solver* s, void* stream) {
     if (s->have_c2r) CUFFT_TRY(cufftSetStream(s->c2r, s->stream));
     if (s->have_r2c_n) CUFFT_TRY(cufftSetStream(s->r2c_n, s->stream));
     if (s->have_c2r_n) CUFFT_TRY(cufftSetStream(s->c2r_n, s->stream));
+    if (s->have_c2r_d) CUFFT_TRY(cufftSetStream(s->c2r_d, s->stream));
     return DJB_OK;
 }
 
