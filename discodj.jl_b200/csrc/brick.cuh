@@ -30,7 +30,8 @@ struct BrickList {
     int nsub;                // sort keys per brick (2^3-cell sub-blocks)
     int64_t nkeys;           // keys in total
     unsigned np;             // particles
-    int sx;                  // interpolation box width along x (gather_box)
+    int sx;                  // interpolation box width along x (aligned_box)
+    int ssx;                 // mass-assignment box width along x
 };
 
 __device__ __forceinline__ unsigned key_start(const BrickList& bl, int64_t key) {
@@ -65,33 +66,75 @@ __device__ __forceinline__ int box_rel(int node, int origin, int res) {
     return v;
 }
 
+// Box of brick b with the x origin rounded down to a multiple of 4 nodes (so that
+// every row starts on a 16-byte boundary of a dense mesh) and `sx` nodes along x (a
+// multiple of 4, at least S + 3); y and z as brick_box. Shared memory holds the box
+// densely, [z][y][x] with rows of sx elements.
+__device__ __forceinline__ TileBox aligned_box(const BrickList& bl, int b, int lo_minus_r, int S, int sx) {
+    TileBox box = brick_box(bl, b, lo_minus_r, S);
+    box.o[0] &= ~3;
+    box.S[0] = sx;
+    box.P = sx;
+    box.plane = sx * S;
+    return box;
+}
+
+__device__ __forceinline__ bool box_inside(const TileBox& box, int res) {
+    return box.o[0] >= 0 && box.o[0] + box.S[0] <= res && box.o[1] >= 0 && box.o[1] + box.S[1] <= res &&
+           box.o[2] >= 0 && box.o[2] + box.S[2] <= res;
+}
+
+// Walks the box in copies of `per` elements (4 when `vec`: pitch and res multiples of 4,
+// so a 16-byte group never straddles the periodic wrap; else 1) and calls
+// f(shared offset, global offset) with the wrapped global element offset.
+template <class F>
+__device__ __forceinline__ void for_box_wrapped(const TileBox& box, int res, int pitch, bool vec, F f) {
+    const int S1 = box.S[1];
+    FastDiv fy;
+    fy.init(S1);
+    const int per = vec ? 4 : 1;
+    const int cpr = box.S[0] / per;  // copies per row
+    FastDiv fc;
+    fc.init(cpr);
+    const int total = cpr * S1 * box.S[2];
+    for (int t = threadIdx.x; t < total; t += kTileThreads) {
+        const int r = fc.div(t);
+        const int c = t - r * cpr;
+        const int z = fy.div(r);
+        const int y = r - z * S1;
+        const int gx = wrap2(box.o[0] + per * c, res);
+        const int gy = wrap2(box.o[1] + y, res);
+        const int gz = wrap2(box.o[2] + z, res);
+        f(r * box.S[0] + per * c, (int64_t(gz) * res + gy) * pitch + gx);
+    }
+}
+
 // ── mass assignment ───────────────────────────────────────────────────────────
+// Box: B + W + 2 nodes per axis (bl.ssx along x). `tma` != 0: the meshes are dense
+// [res]^3 (pitch == res) described by tm0/tm1 with boxes of ssx x S x S; boxes that do
+// not wrap are then added to the mesh with one bulk tensor reduction.
 template <int W, int NS>
 __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
-    GroupShifts sh, float* __restrict__ mesh0, float* __restrict__ mesh1, int* err, BrickList bl) {
-    extern __shared__ unsigned int sacc[];
-    __shared__ int s_row[kMaxRows];
-    __shared__ int s_col[kMaxCols];
+    GroupShifts sh, float* __restrict__ mesh0, float* __restrict__ mesh1, int* err, BrickList bl,
+    const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1, int tma) {
+    extern __shared__ __align__(128) unsigned int sacc[];
     const int b = blockIdx.x;
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
     if (cnt == 0) return;
     const int tid = threadIdx.x;
-    constexpr int S_EXT = W + 2;  // box = brick + W + 2 nodes
-    const TileBox box = brick_box(bl, b, WLo<W>::v, bl.brick + S_EXT);
+    const TileBox box = aligned_box(bl, b, WLo<W>::v, bl.brick + W + 2, bl.ssx);
+    const bool bulk = tma && box_inside(box, res);
+    const bool vec = ((pitch | res) & 3) == 0;
     const float resf = float(res);
-    box_columns(box, res, s_col);
-    chunk_rows(box, res, 0, box.S[2], s_row);
-    __syncthreads();  // the row and column tables are read by every thread below
-    FastDiv fp;
-    fp.init(box.P);
-    const int cells = box.plane * box.S[2];
+    const int cells = box.plane * box.S[2];  // a multiple of 4
 #pragma unroll 1
     for (int g = 0; g < NS; ++g) {
         float* mesh = (g == 0) ? mesh0 : mesh1;
         const Shift3 sg = (g == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
-        for (int t = tid; t < cells; t += kTileThreads) sacc[t] = 0u;
+        for (int t = 4 * tid; t < cells; t += 4 * kTileThreads)
+            *reinterpret_cast<uint4*>(sacc + t) = make_uint4(0u, 0u, 0u, 0u);
         __syncthreads();
         for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
             // lanes 8 slots apart: particles of one cell land in different warps, which
@@ -128,64 +171,50 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
                 }
         }
         __syncthreads();
-        for (int t = tid; t < cells; t += kTileThreads) {
-            const unsigned int v = sacc[t];
-            if (v == 0u) continue;
-            const int r = fp.div(t);
-            const int x = t - r * box.P;
-            atomicAdd(mesh + int64_t(s_row[r]) * pitch + s_col[x], __uint2float_rn(v) * FixScale<W>::down);
+        if (bulk) {
+            // fixed point -> float in place, then one bulk reduction of the whole box
+            for (int t = 4 * tid; t < cells; t += 4 * kTileThreads) {
+                const uint4 v = *reinterpret_cast<const uint4*>(sacc + t);
+                *reinterpret_cast<float4*>(sacc + t) =
+                    make_float4(__uint2float_rn(v.x) * FixScale<W>::down, __uint2float_rn(v.y) * FixScale<W>::down,
+                                __uint2float_rn(v.z) * FixScale<W>::down, __uint2float_rn(v.w) * FixScale<W>::down);
+            }
+            fence_proxy_async_smem();  // the conversions are read by the bulk copy below
+            __syncthreads();
+            if (tid == 0) {
+                tma_reduce_add_3d((g == 0) ? &tm0 : &tm1, box.o[0], box.o[1], box.o[2], sacc);
+                bulk_commit_and_wait_read();
+            }
+            __syncthreads();  // the box may be cleared again
+        } else {
+            for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
+                if (vec) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(sacc + so);
+                    if ((v.x | v.y | v.z | v.w) == 0u) return;
+                    red_add_v4(mesh + go, __uint2float_rn(v.x) * FixScale<W>::down,
+                               __uint2float_rn(v.y) * FixScale<W>::down, __uint2float_rn(v.z) * FixScale<W>::down,
+                               __uint2float_rn(v.w) * FixScale<W>::down);
+                } else {
+                    const unsigned v = sacc[so];
+                    if (v != 0u) atomicAdd(mesh + go, __uint2float_rn(v) * FixScale<W>::down);
+                }
+            });
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
 // ── force interpolation (finite-difference gradient of order 2R) ─────────────
-// Interpolation box of brick b: y and z as brick_box (S = B + W + 2 + 2R nodes); the x
-// origin is rounded down to a multiple of 4 nodes so that every box row starts on a
-// 16-byte boundary of a dense mesh, and the box is bl.sx nodes wide (a multiple of 4,
-// at least S + 3). Shared memory holds the box densely, [z][y][x] with rows of sx floats.
-__device__ __forceinline__ TileBox gather_box(const BrickList& bl, int b, int lo_minus_r, int S) {
-    TileBox box = brick_box(bl, b, lo_minus_r, S);
-    box.o[0] &= ~3;
-    box.S[0] = bl.sx;
-    box.P = bl.sx;
-    box.plane = bl.sx * S;
-    return box;
-}
-
-__device__ __forceinline__ bool box_inside(const TileBox& box, int res) {
-    return box.o[0] >= 0 && box.o[0] + box.S[0] <= res && box.o[1] >= 0 && box.o[1] + box.S[1] <= res &&
-           box.o[2] >= 0 && box.o[2] + box.S[2] <= res;
-}
-
-// Stages the potential over `box` with asynchronous copies that take the periodic wrap
-// per element: 16-byte chunks when every row of the mesh starts on a 16-byte boundary
-// (`vec`: pitch and res multiples of 4; chunks never straddle the wrap), else floats.
+// Stages the potential over `box` with asynchronous copies that take the periodic wrap.
 __device__ __forceinline__ void stage_box_wrapped(float* sbox, const float* __restrict__ phi, const TileBox& box,
                                                   int res, int pitch, bool vec) {
-    const int S1 = box.S[1];
-    FastDiv fy;
-    fy.init(S1);
-    const int per = vec ? 4 : 1;
-    const int cpr = box.S[0] / per;  // copies per row
-    FastDiv fc;
-    fc.init(cpr);
-    const int total = cpr * S1 * box.S[2];
-    for (int t = threadIdx.x; t < total; t += kTileThreads) {
-        const int r = fc.div(t);
-        const int c = t - r * cpr;
-        const int z = fy.div(r);
-        const int y = r - z * S1;
-        const int gx = wrap2(box.o[0] + per * c, res);
-        const int gy = wrap2(box.o[1] + y, res);
-        const int gz = wrap2(box.o[2] + z, res);
-        const float* src = phi + (int64_t(gz) * res + gy) * pitch + gx;
-        const unsigned sa = smem_u32(sbox + r * box.S[0] + per * c);
+    for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
+        const unsigned sa = smem_u32(sbox + so);
         if (vec)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(phi + go));
         else
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src));
-    }
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(phi + go));
+    });
     asm volatile("cp.async.wait_all;\n" ::);
 }
 
@@ -206,7 +235,7 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, 
     const int n = A.n;
     const int64_t np = A.np;
     const int res = A.res;
-    const TileBox box = gather_box(bl, b, WLo<W>::v - R, bl.brick + W + 2 + 2 * R);
+    const TileBox box = aligned_box(bl, b, WLo<W>::v - R, bl.brick + W + 2 + 2 * R, bl.sx);
     const bool bulk = tma && box_inside(box, res);
     const bool vec = ((A.pitch | res) & 3) == 0;
     const unsigned box_bytes = unsigned(box.plane) * unsigned(box.S[2]) * 4u;

@@ -709,21 +709,26 @@ struct djb_solver {
 
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    cufftHandle r2c = 0, c2r = 0, r2c_n = 0, c2r_n = 0, c2r_d = 0;
-    bool have_r2c = false, have_c2r = false, have_r2c_n = false, have_c2r_n = false, have_c2r_d = false;
+    cufftHandle r2c = 0, c2r = 0, r2c_n = 0, c2r_n = 0, r2c_d = 0, c2r_d = 0;
+    bool have_r2c = false, have_c2r = false, have_r2c_n = false, have_c2r_n = false, have_r2c_d = false,
+         have_c2r_d = false;
 
     float* psi = nullptr;
     float* mom = nullptr;
     float* acc = nullptr;
     float* q1 = nullptr;
     float* mesh[kMaxGroup] = {nullptr, nullptr};
-    // dense [res]^3 potentials (finite-difference gradients, res % 4 == 0, not lean): the
-    // C2R writes them out of place, and the brick interpolation fetches its boxes from
-    // them with bulk tensor copies described by `tmap`
+    // dense [res]^3 meshes (finite-difference gradients, res % 4 == 0, not lean): the
+    // mass assignment writes the density here, an out-of-place R2C takes it to the
+    // spectrum in `mesh`, and an out-of-place C2R brings the potential back. The brick
+    // kernels add their boxes to them and fetch their boxes from them with bulk tensor
+    // copies described by `tmap_s` (mass-assignment boxes) and `tmap` (interpolation).
     float* phi[kMaxGroup] = {nullptr, nullptr};
     CUtensorMap tmap[kMaxGroup];
+    CUtensorMap tmap_s[kMaxGroup];
     bool tma = false;
     int gsx = 0;  // interpolation box width along x (brick kernels)
+    int ssx = 0;  // mass-assignment box width along x
     float* fmesh[kMaxGroup][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     double* lapT = nullptr;
     double* makT = nullptr;
@@ -835,24 +840,27 @@ dim3 tile_grid(int n) {
 djb::BrickList brick_list(const djb_solver* s) {
     const int hb = s->sg.hb;
     return djb::BrickList{s->offset, s->bsum, s->perm, s->sg.nb, s->sg.brick, hb * hb * hb, s->nbins,
-                          unsigned(s->np), s->gsx};
+                          unsigned(s->np), s->gsx, s->ssx};
 }
 
-// Shared memory of the brick mass assignment: the fixed box, B + W + 2 nodes per axis.
-size_t brick_smem(const djb_solver* s, int halo) {
-    const int S = s->sg.brick + s->W + 2 + 2 * halo;
-    return size_t(S | 1) * S * S * 4;
-}
-
-// Interpolation box width along x for bricks of `brick` cells: the S = B + W + 2 + 2R
-// nodes of a box start anywhere in a 16-byte group after the rounded-down origin, so
-// S + 3 nodes rounded up to a multiple of 4; a width of 4 mod 8 keeps the rows of one
-// plane on different shared-memory banks.
+// Box width along x for bricks of `brick` cells and boxes of S = B + W + 2 + 2R nodes
+// (R = 0 for the mass assignment): the box starts anywhere in a 16-byte group after the
+// rounded-down origin, so S + 3 nodes rounded up to a multiple of 4; a width of 4 mod 8
+// keeps the rows of one plane on different shared-memory banks.
 int gather_sx(int brick, int W, int R) {
     int sx = (brick + W + 2 + 2 * R + 6) & ~3;
     if (sx % 8 == 0) sx += 4;
     return sx;
 }
+
+size_t scatter_smem(const djb_solver* s) {
+    const int S = s->sg.brick + s->W + 2;
+    return size_t(s->ssx) * S * S * 4;
+}
+
+// The density mesh of group member m (dense when the solver has dense meshes) and its pitch.
+float* rho_mesh(const djb_solver* s, int m) { return s->phi[m] ? s->phi[m] : s->mesh[m]; }
+int rho_pitch(const djb_solver* s) { return s->phi[0] ? s->res : s->pitch; }
 
 size_t gather_smem(const djb_solver* s) {
     const int S = s->sg.brick + s->W + 2 + 2 * s->R;
@@ -884,44 +892,50 @@ int make_tmap(CUtensorMap* m, const float* base, int res, int sx, int S) {
     return DJB_OK;
 }
 
+// Mass assignment into m0 (and m1) of row pitch `pitch`; `dense`: m0/m1 are the
+// solver's dense meshes (bulk tensor reductions allowed).
 template <int W, int NS>
-void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, float* m0,
-                      float* m1) {
+void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, float* m0, float* m1,
+                      int pitch, bool dense) {
     if (s->tiled && s->cur_perm) {  // brick-owned: the drift was applied by the binning pass
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
-        djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, brick_smem(s, 0), s->stream>>>(
-            s->psi, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err, brick_list(s));
+        const int tma = (dense && s->tma) ? 1 : 0;
+        djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, scatter_smem(s), s->stream>>>(
+            s->psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, m0, m1, s->err, brick_list(s), s->tmap_s[0],
+            s->tmap_s[NS > 1 ? 1 : 0], tma);
         return;
     }
     if (s->tiled) {
         const dim3 grid = s->cur_perm ? dim3(unsigned((s->np + djb::kTileThreads - 1) / djb::kTileThreads))
                                       : tile_grid(s->n);
         djb::k_scatter_tiled<W, NS><<<grid, djb::kTileThreads, kScatterBudget * sizeof(unsigned int), s->stream>>>(
-            s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err, kScatterBudget,
+            s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, m0, m1, s->err, kScatterBudget,
             s->cur_perm);
         return;
     }
     djb::k_scatter<W, NS><<<blocks(s->np), kThreads, 0, s->stream>>>(
-        s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res, s->pitch, g, m0, m1, s->err);
+        s->psi, mom, dd1, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, m0, m1, s->err);
 }
 
 void launch_scatter(djb_solver* s, const float* mom, float dd1, const GroupShifts& g, int ns) {
-    float* m0 = s->mesh[0];
-    float* m1 = s->mesh[1];
-#define DJB_SC(W_)                                                        \
-    if (s->W == W_) {                                                      \
-        if (ns == 1) launch_scatter_t<W_, 1>(s, mom, dd1, g, m0, m1);       \
-        else launch_scatter_t<W_, 2>(s, mom, dd1, g, m0, m1);               \
+    float* m0 = rho_mesh(s, 0);
+    float* m1 = rho_mesh(s, 1);
+    const int pitch = rho_pitch(s);
+    const bool dense = s->phi[0] != nullptr;
+#define DJB_SC(W_)                                                                 \
+    if (s->W == W_) {                                                               \
+        if (ns == 1) launch_scatter_t<W_, 1>(s, mom, dd1, g, m0, m1, pitch, dense);  \
+        else launch_scatter_t<W_, 2>(s, mom, dd1, g, m0, m1, pitch, dense);          \
     }
     DJB_SC(2) DJB_SC(3) DJB_SC(4)
 #undef DJB_SC
 }
 
-void launch_scatter_positions(djb_solver* s, const float* xr, int64_t count, float* mesh) {
+void launch_scatter_positions(djb_solver* s, const float* xr, int64_t count, float* mesh, int pitch) {
     const int b = blocks(count);
-    if (s->W == 2) djb::k_scatter_positions<2><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, s->pitch, mesh, s->err);
-    if (s->W == 3) djb::k_scatter_positions<3><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, s->pitch, mesh, s->err);
-    if (s->W == 4) djb::k_scatter_positions<4><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, s->pitch, mesh, s->err);
+    if (s->W == 2) djb::k_scatter_positions<2><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, pitch, mesh, s->err);
+    if (s->W == 3) djb::k_scatter_positions<3><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, pitch, mesh, s->err);
+    if (s->W == 4) djb::k_scatter_positions<4><<<b, kThreads, 0, s->stream>>>(xr, count, count, s->Lf, s->res, pitch, mesh, s->err);
 }
 
 template <int W, int R>
@@ -1036,7 +1050,7 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
                 djb::k_place<<<grid_for(np), kThreads, 0, s->stream>>>(
                     s->rb, s->q1, n, np, s->Lf, float(d[c] * s->cfg.boxsize / n), c, s->xr);
             }
-            launch_scatter_positions(s, s->xr, np, mesh);
+            launch_scatter_positions(s, s->xr, np, mesh, rho_pitch(s));
         }
         (void)nreal;
     } else {
@@ -1047,7 +1061,7 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
                 s->rb, s->q1, n, np, s->Lf, float(d[0]), float(d[1]), float(d[2]),
                 float(d[0] * s->cfg.boxsize / n), float(d[1] * s->cfg.boxsize / n),
                 float(d[2] * s->cfg.boxsize / n), s->xr);
-            launch_scatter_positions(s, s->xr, np, mesh);
+            launch_scatter_positions(s, s->xr, np, mesh, rho_pitch(s));
         }
     }
     return DJB_OK;
@@ -1083,8 +1097,9 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         const int ns = std::min(s->group, s->nshift - first);
         const GroupShifts g = group_shifts(s, first, ns);
         s->prof.begin(s->stream, PH_CLEAR);
+        const size_t rho_floats = s->phi[0] ? size_t(s->res) * s->res * s->res : size_t(s->mesh_floats);
         for (int m = 0; m < ns; ++m)
-            CUDA_TRY(cudaMemsetAsync(s->mesh[m], 0, size_t(s->mesh_floats) * sizeof(float), s->stream));
+            CUDA_TRY(cudaMemsetAsync(rho_mesh(s, m), 0, rho_floats * sizeof(float), s->stream));
         s->prof.end(s->stream, PH_CLEAR, 0);
         // with the brick sort the binning pass has applied the first drift already
         const bool drift_here = step && first == 0 && !s->cur_perm;
@@ -1093,14 +1108,15 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         s->prof.end(s->stream, PH_SCATTER, 1);
         if (resample) {
             s->prof.begin(s->stream, PH_RESAMPLE);
-            TRY(resample_deposit(s, first, s->mesh[0]));
+            TRY(resample_deposit(s, first, rho_mesh(s, 0)));
             s->prof.end(s->stream, PH_RESAMPLE, 0);
         }
         for (int m = 0; m < ns; ++m) {
             float* mesh = s->mesh[m];
             cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
             s->prof.begin(s->stream, PH_R2C);
-            CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
+            if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
+            else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
             s->prof.end(s->stream, PH_R2C, 0);
             if (!ik) {
                 s->prof.begin(s->stream, PH_KSPACE);
@@ -1199,6 +1215,7 @@ void release(djb_solver* s) {
     if (s->have_r2c_n) cufftDestroy(s->r2c_n);
     if (s->have_c2r_n) cufftDestroy(s->c2r_n);
     if (s->have_c2r_d) cufftDestroy(s->c2r_d);
+    if (s->have_r2c_d) cufftDestroy(s->r2c_d);
     for (void* p : s->allocs) cudaFree(p);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     if (prev >= 0) cudaSetDevice(prev);
@@ -1310,18 +1327,19 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         // would not stay well inside the periodic mesh (box_rel needs res > extent + 4)
         int brick = 16, lgb = 4;
         while (brick > 2 && (brick > s->res / 2 || brick + s->W + 2 + 2 * s->R + 4 >= s->res ||
-                             (s->R > 0 && gather_sx(brick, s->W, s->R) + 4 >= s->res))) {
+                             gather_sx(brick, s->W, s->R) + 4 >= s->res)) {
             brick /= 2;
             --lgb;
         }
         s->gsx = gather_sx(brick, s->W, s->R);
+        s->ssx = gather_sx(brick, s->W, 0);
         const int nb = (s->res + brick - 1) / brick;
         const int hb = brick > 2 ? brick / 2 : 1;
         s->sg = djb::SortGeom{s->res, brick, lgb, nb, hb};
         s->nbins = int64_t(nb) * nb * nb * hb * hb * hb;  // keys: bricks x 2^3-cell sub-blocks
         if (s->nbins > int64_t(djb::kScanBlock) * djb::kScanThreads * 64)
             return fail(DJB_ERR_INVALID, "mesh too large for the particle sort (%lld keys)", (long long)s->nbins);
-        if (gather_smem(s) > size_t(kBrickGatherMax) || brick_smem(s, 0) > size_t(kScatterBudget) * 4)
+        if (gather_smem(s) > size_t(kBrickGatherMax) || scatter_smem(s) > size_t(kScatterBudget) * 4)
             return fail(DJB_ERR_INVALID, "brick box exceeds the shared-memory budget");
         s->nscan = int((s->nbins + djb::kScanBlock - 1) / djb::kScanBlock);
         TRY(dmalloc(s, (void**)&s->count, sizeof(unsigned) * size_t(s->nbins)));
@@ -1349,10 +1367,23 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                       dembed[0] * dembed[1] * dembed[2], CUFFT_C2R, 1, &work));
         CUFFT_TRY(cufftSetStream(s->c2r_d, s->stream));
         s->bytes += int64_t(work);
+        CUFFT_TRY(cufftCreate(&s->r2c_d));
+        s->have_r2c_d = true;
+        CUFFT_TRY(cufftMakePlanMany64(s->r2c_d, 3, dims, dembed, 1, dembed[0] * dembed[1] * dembed[2], cembed, 1,
+                                      cembed[0] * cembed[1] * cembed[2], CUFFT_R2C, 1, &work));
+        CUFFT_TRY(cufftSetStream(s->r2c_d, s->stream));
+        s->bytes += int64_t(work);
         const int S = s->sg.brick + s->W + 2 + 2 * s->R;
+        const int Ss = s->sg.brick + s->W + 2;
         if (s->sorted && s->gsx <= res && S <= res) {
-            for (int m = 0; m < s->group; ++m) TRY(make_tmap(&s->tmap[m], s->phi[m], res, s->gsx, S));
-            for (int m = s->group; m < kMaxGroup; ++m) s->tmap[m] = s->tmap[0];
+            for (int m = 0; m < s->group; ++m) {
+                TRY(make_tmap(&s->tmap[m], s->phi[m], res, s->gsx, S));
+                TRY(make_tmap(&s->tmap_s[m], s->phi[m], res, s->ssx, Ss));
+            }
+            for (int m = s->group; m < kMaxGroup; ++m) {
+                s->tmap[m] = s->tmap[0];
+                s->tmap_s[m] = s->tmap_s[0];
+            }
             s->tma = true;
         }
     }
@@ -1428,6 +1459,7 @@ int djb_solver_set_stream(djb_solver* s, void* stream) {
     if (s->have_r2c_n) CUFFT_TRY(cufftSetStream(s->r2c_n, s->stream));
     if (s->have_c2r_n) CUFFT_TRY(cufftSetStream(s->c2r_n, s->stream));
     if (s->have_c2r_d) CUFFT_TRY(cufftSetStream(s->c2r_d, s->stream));
+    if (s->have_r2c_d) CUFFT_TRY(cufftSetStream(s->r2c_d, s->stream));
     return DJB_OK;
 }
 
@@ -1600,7 +1632,7 @@ int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cu
     CUDA_TRY(cudaMemsetAsync(s->mesh[0], 0, size_t(s->mesh_floats) * sizeof(float), s->stream));
     GroupShifts g{};
     s->cur_perm = nullptr;  // the P(k) deposit uses Lagrangian tiles
-    launch_scatter_t<2, 1>(s, nullptr, 0.0f, g, s->mesh[0], nullptr);
+    launch_scatter_t<2, 1>(s, nullptr, 0.0f, g, s->mesh[0], nullptr, s->pitch, false);
     CUDA_TRY(cudaGetLastError());
     *mesh_out = s->mesh[0];
     *res = s->res;

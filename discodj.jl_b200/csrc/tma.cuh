@@ -1,8 +1,10 @@
-// Tensor-memory-accelerator (TMA) bulk copies of mesh boxes into shared memory.
+// Tensor-memory-accelerator (TMA) bulk copies between mesh boxes and shared memory.
 //
-// One thread issues `cp.async.bulk.tensor.3d` for a whole box and arms an mbarrier
-// with the box's byte count; every thread of the CTA waits on the barrier's phase.
-// The copies read this GPU's own memory only and use no cluster multicast.
+// Loads: one thread issues `cp.async.bulk.tensor.3d` for a whole box and arms an
+// mbarrier with the box's byte count; every thread of the CTA waits on the barrier's
+// phase. Reductions: one thread issues `cp.reduce.async.bulk.tensor.3d ... .add` of a
+// whole box and waits for its source reads (bulk group). The copies touch this GPU's
+// own memory only and use no cluster multicast.
 // Waits are bounded (about one second of SM clock); a wait that runs out reports it
 // to the caller, which sets the device error word instead of spinning forever.
 #pragma once
@@ -40,6 +42,30 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
         : "memory");
+}
+
+// Element-wise float add of the shared-memory box at `src` (16-byte aligned, laid out
+// as the map's box) into global memory at box coordinates (x, y, z) of `map`; the
+// coordinates are non-negative and the box lies inside the tensor.
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+        : "memory");
+}
+
+// Commits this thread's bulk operations and waits until their shared-memory sources
+// have been read (the shared memory may then be overwritten or released).
+__device__ __forceinline__ void bulk_commit_and_wait_read() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Vector float reduction of four consecutive floats at a 16-byte aligned address.
+__device__ __forceinline__ void red_add_v4(float* dst, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
 }
 
 // Waits for the barrier phase with the given parity; false when about 2^31 SM clock
