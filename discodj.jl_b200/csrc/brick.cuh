@@ -79,6 +79,10 @@ __device__ __forceinline__ TileBox aligned_box(const BrickList& bl, int b, int l
     return box;
 }
 
+// Elements reserved per box in shared memory: a multiple of 32 (128 bytes, the alignment
+// of a bulk tensor copy's shared-memory operand).
+__host__ __device__ __forceinline__ int box_stride(int cells) { return (cells + 31) & ~31; }
+
 __device__ __forceinline__ bool box_inside(const TileBox& box, int res) {
     return box.o[0] >= 0 && box.o[0] + box.S[0] <= res && box.o[1] >= 0 && box.o[1] + box.S[1] <= res &&
            box.o[2] >= 0 && box.o[2] + box.S[2] <= res;
@@ -110,9 +114,10 @@ __device__ __forceinline__ void for_box_wrapped(const TileBox& box, int res, int
 }
 
 // ── mass assignment ───────────────────────────────────────────────────────────
-// Box: B + W + 2 nodes per axis (bl.ssx along x). `tma` != 0: the meshes are dense
+// Box: B + W + 2 nodes per axis (bl.ssx along x); one box per shift of the group, all
+// filled in one pass over the brick's particles. `tma` != 0: the meshes are dense
 // [res]^3 (pitch == res) described by tm0/tm1 with boxes of ssx x S x S; boxes that do
-// not wrap are then added to the mesh with one bulk tensor reduction.
+// not wrap are then added to the mesh with one bulk tensor reduction each.
 template <int W, int NS>
 __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
@@ -125,25 +130,29 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
     if (cnt == 0) return;
     const int tid = threadIdx.x;
     const TileBox box = aligned_box(bl, b, WLo<W>::v, bl.brick + W + 2, bl.ssx);
-    const bool bulk = tma && box_inside(box, res);
+    const bool bulk = tma && box_inside(box, res) && (smem_u32(sacc) & 127u) == 0u;
     const bool vec = ((pitch | res) & 3) == 0;
     const float resf = float(res);
     const int cells = box.plane * box.S[2];  // a multiple of 4
+    const int stride = box_stride(cells);    // boxes start on 128-byte boundaries (bulk tensor copies)
+    for (int t = 4 * tid; t < NS * stride; t += 4 * kTileThreads)
+        *reinterpret_cast<uint4*>(sacc + t) = make_uint4(0u, 0u, 0u, 0u);
+    LatticeDiv ld;
+    ld.init(n);
+    __syncthreads();
+    for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
+        // lanes 8 slots apart: particles of one cell land in different warps, which
+        // keeps same-address shared atomics out of a single instruction
+        const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
+        if (slot >= cnt) continue;
+        const int64_t p = bl.perm[start + slot];
+        int i, j, k;
+        ld.ijk(p, i, j, k);
+        const float X[3] = {psi[p] + q1[i], psi[p + np] + q1[j], psi[p + 2 * np] + q1[k]};
 #pragma unroll 1
-    for (int g = 0; g < NS; ++g) {
-        float* mesh = (g == 0) ? mesh0 : mesh1;
-        const Shift3 sg = (g == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
-        for (int t = 4 * tid; t < cells; t += 4 * kTileThreads)
-            *reinterpret_cast<uint4*>(sacc + t) = make_uint4(0u, 0u, 0u, 0u);
-        __syncthreads();
-        for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
-            // lanes 8 slots apart: particles of one cell land in different warps, which
-            // keeps same-address shared atomics out of a single instruction
-            const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
-            if (slot >= cnt) continue;
-            const int64_t p = bl.perm[start + slot];
-            const int i = int(p % n), j = int((p / n) % n), k = int(p / (int64_t(n) * n));
-            const float X[3] = {psi[p] + q1[i], psi[p + np] + q1[j], psi[p + 2 * np] + q1[k]};
+        for (int g = 0; g < NS; ++g) {
+            const Shift3 sg = (g == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
+            unsigned int* acc = sacc + g * stride;
             float w[3][W];
             int d[3];
 #pragma unroll
@@ -163,48 +172,52 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
             for (int c = 0; c < W; ++c)
 #pragma unroll
                 for (int bb = 0; bb < W; ++bb) {
-                    unsigned int* row = sacc + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+                    unsigned int* row = acc + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
                     const float wyz = w[1][bb];
 #pragma unroll
                     for (int a = 0; a < W; ++a)
                         atomicAdd(row + a, __float2uint_rn(w[0][a] * wyz * w[2][c] * FixScale<W>::up));
                 }
         }
+    }
+    __syncthreads();
+    if (bulk) {
+        // fixed point -> float in place, then one bulk reduction per box
+        for (int t = 4 * tid; t < NS * stride; t += 4 * kTileThreads) {
+            const uint4 v = *reinterpret_cast<const uint4*>(sacc + t);
+            *reinterpret_cast<float4*>(sacc + t) =
+                make_float4(__uint2float_rn(v.x) * FixScale<W>::down, __uint2float_rn(v.y) * FixScale<W>::down,
+                            __uint2float_rn(v.z) * FixScale<W>::down, __uint2float_rn(v.w) * FixScale<W>::down);
+        }
+        fence_proxy_async_smem();  // the conversions are read by the bulk copies below
         __syncthreads();
-        if (bulk) {
-            // fixed point -> float in place, then one bulk reduction of the whole box
-            for (int t = 4 * tid; t < cells; t += 4 * kTileThreads) {
-                const uint4 v = *reinterpret_cast<const uint4*>(sacc + t);
-                *reinterpret_cast<float4*>(sacc + t) =
-                    make_float4(__uint2float_rn(v.x) * FixScale<W>::down, __uint2float_rn(v.y) * FixScale<W>::down,
-                                __uint2float_rn(v.z) * FixScale<W>::down, __uint2float_rn(v.w) * FixScale<W>::down);
-            }
-            fence_proxy_async_smem();  // the conversions are read by the bulk copy below
-            __syncthreads();
-            if (tid == 0) {
-                tma_reduce_add_3d((g == 0) ? &tm0 : &tm1, box.o[0], box.o[1], box.o[2], sacc);
-                bulk_commit_and_wait_read();
-            }
-            __syncthreads();  // the box may be cleared again
-        } else {
+        if (tid == 0) {
+            tma_reduce_add_3d(&tm0, box.o[0], box.o[1], box.o[2], sacc);
+            if (NS > 1) tma_reduce_add_3d(&tm1, box.o[0], box.o[1], box.o[2], sacc + stride);
+            bulk_commit_and_wait_read();  // shared memory stays allocated until read
+        }
+        __syncthreads();
+    } else {
+#pragma unroll 1
+        for (int g = 0; g < NS; ++g) {
+            float* mesh = (g == 0) ? mesh0 : mesh1;
+            const unsigned int* acc = sacc + g * stride;
             for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
                 if (vec) {
-                    const uint4 v = *reinterpret_cast<const uint4*>(sacc + so);
+                    const uint4 v = *reinterpret_cast<const uint4*>(acc + so);
                     if ((v.x | v.y | v.z | v.w) == 0u) return;
                     red_add_v4(mesh + go, __uint2float_rn(v.x) * FixScale<W>::down,
                                __uint2float_rn(v.y) * FixScale<W>::down, __uint2float_rn(v.z) * FixScale<W>::down,
                                __uint2float_rn(v.w) * FixScale<W>::down);
                 } else {
-                    const unsigned v = sacc[so];
+                    const unsigned v = acc[so];
                     if (v != 0u) atomicAdd(mesh + go, __uint2float_rn(v) * FixScale<W>::down);
                 }
             });
-            __syncthreads();
         }
     }
 }
 
-// ── force interpolation (finite-difference gradient of order 2R) ─────────────
 // Stages the potential over `box` with asynchronous copies that take the periodic wrap.
 __device__ __forceinline__ void stage_box_wrapped(float* sbox, const float* __restrict__ phi, const TileBox& box,
                                                   int res, int pitch, bool vec) {
@@ -236,7 +249,7 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, 
     const int64_t np = A.np;
     const int res = A.res;
     const TileBox box = aligned_box(bl, b, WLo<W>::v - R, bl.brick + W + 2 + 2 * R, bl.sx);
-    const bool bulk = tma && box_inside(box, res);
+    const bool bulk = tma && box_inside(box, res) && (smem_u32(sbox) & 127u) == 0u;
     const bool vec = ((A.pitch | res) & 3) == 0;
     const unsigned box_bytes = unsigned(box.plane) * unsigned(box.S[2]) * 4u;
     if (bulk && tid == 0) mbar_init(&s_bar, 1);
@@ -244,6 +257,8 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, 
     unsigned parity = 0;
     const float resf = float(res);
     const float cc[4] = {0.0f, A.c1, A.c2, A.c3};
+    LatticeDiv ld;
+    ld.init(n);
     for (unsigned sr = 0; sr < cnt; sr += kTileThreads * kBrickRounds) {
         // the particles of this super-round stay in registers across the shifts
         int64_t pr[kBrickRounds];
@@ -288,8 +303,8 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, 
 #pragma unroll 1
             for (int r = 0; r < kBrickRounds; ++r) {
                 if (pr[r] < 0) continue;
-                const int64_t p = pr[r];
-                const int i = int(p % n), j = int((p / n) % n), k = int(p / (int64_t(n) * n));
+                int i, j, k;
+                ld.ijk(pr[r], i, j, k);
                 const float X[3] = {ps[r][0] + A.q1[i], ps[r][1] + A.q1[j], ps[r][2] + A.q1[k]};
                 float w[3][W], u[3][E];
                 int d[3];

@@ -71,6 +71,24 @@ __device__ __forceinline__ float grid_coord(float x, float L, float resf, int* e
     return g;
 }
 
+// Lattice indices (i, j, k) of particle p = i + n (j + n k) by 64-bit multiply-high with
+// m = ceil(2^64 / n): exact for p < 2^64 / n, i.e. for every particle (n >= 2).
+struct LatticeDiv {
+    uint64_t m;
+    unsigned n;
+    __device__ __forceinline__ void init(int nn) {
+        n = unsigned(nn);
+        m = ~0ull / n + 1ull;
+    }
+    __device__ __forceinline__ void ijk(int64_t p, int& i, int& j, int& k) const {
+        const uint64_t q = __umul64hi(uint64_t(p), m);
+        const uint64_t r = __umul64hi(q, m);
+        i = int(uint64_t(p) - q * n);
+        j = int(q - r * n);
+        k = int(r);
+    }
+};
+
 // Weights and wrapped node indices along one axis.
 template <int W>
 __device__ __forceinline__ void axis_weights(float g, int res, float* w, int* idx) {

@@ -853,9 +853,10 @@ int gather_sx(int brick, int W, int R) {
     return sx;
 }
 
+// Per shift of a group: one box, rounded up to 128 bytes (djb::box_stride).
 size_t scatter_smem(const djb_solver* s) {
     const int S = s->sg.brick + s->W + 2;
-    return size_t(s->ssx) * S * S * 4;
+    return size_t(djb::box_stride(s->ssx * S * S)) * 4;
 }
 
 // The density mesh of group member m (dense when the solver has dense meshes) and its pitch.
@@ -867,9 +868,9 @@ size_t gather_smem(const djb_solver* s) {
     return size_t(s->gsx) * S * S * 4;
 }
 
-// 2 CTAs of the brick interpolation per SM: 228 KB of shared memory less 1 KB per CTA
-// reserved by the runtime and the kernel's static barrier.
-constexpr int kBrickGatherMax = 113 * 1024;
+// Dynamic shared memory of a brick kernel, 2 CTAs per SM: 228 KB of shared memory
+// less 1 KB per CTA reserved by the runtime and the kernel's static barrier.
+constexpr int kBrickSmemMax = 113 * 1024;
 
 // Tensor map of a dense [res]^3 float mesh with boxes of sx x S x S elements.
 int make_tmap(CUtensorMap* m, const float* base, int res, int sx, int S) {
@@ -900,7 +901,7 @@ void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShi
     if (s->tiled && s->cur_perm) {  // brick-owned: the drift was applied by the binning pass
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const int tma = (dense && s->tma) ? 1 : 0;
-        djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, scatter_smem(s), s->stream>>>(
+        djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, NS * scatter_smem(s), s->stream>>>(
             s->psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, m0, m1, s->err, brick_list(s), s->tmap_s[0],
             s->tmap_s[NS > 1 ? 1 : 0], tma);
         return;
@@ -975,9 +976,9 @@ int tiled_attrs_wr() {
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_tiled<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kBrickGatherMax));
+                                  kBrickSmemMax));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kBrickGatherMax));
+                                  kBrickSmemMax));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   int(cudaSharedmemCarveoutMaxShared)));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -990,8 +991,14 @@ int scatter_attrs_w() {
     const int smem = kScatterBudget * int(sizeof(unsigned int));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_tiled<W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_tiled<W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kBrickSmemMax));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kBrickSmemMax));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  int(cudaSharedmemCarveoutMaxShared)));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  int(cudaSharedmemCarveoutMaxShared)));
     return DJB_OK;
 }
 
@@ -1339,7 +1346,7 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         s->nbins = int64_t(nb) * nb * nb * hb * hb * hb;  // keys: bricks x 2^3-cell sub-blocks
         if (s->nbins > int64_t(djb::kScanBlock) * djb::kScanThreads * 64)
             return fail(DJB_ERR_INVALID, "mesh too large for the particle sort (%lld keys)", (long long)s->nbins);
-        if (gather_smem(s) > size_t(kBrickGatherMax) || scatter_smem(s) > size_t(kScatterBudget) * 4)
+        if (gather_smem(s) > size_t(kBrickSmemMax) || s->group * scatter_smem(s) > size_t(kBrickSmemMax))
             return fail(DJB_ERR_INVALID, "brick box exceeds the shared-memory budget");
         s->nscan = int((s->nbins + djb::kScanBlock - 1) / djb::kScanBlock);
         TRY(dmalloc(s, (void**)&s->count, sizeof(unsigned) * size_t(s->nbins)));

@@ -52,7 +52,10 @@ __global__ void __launch_bounds__(256) k_bin(float* __restrict__ psi, const floa
                                              uint2* __restrict__ keyrank, int* err) {
     const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= np) return;
-    const int i = int(p % n), j = int((p / n) % n), k = int(p / (int64_t(n) * n));
+    LatticeDiv ld;
+    ld.init(n);
+    int i, j, k;
+    ld.ijk(p, i, j, k);
     float X[3] = {psi[p], psi[p + np], psi[p + 2 * np]};
     if (mom) {
 #pragma unroll

@@ -150,9 +150,9 @@ __device__ __forceinline__ TileParticle tile_particle(const int* __restrict__ pe
         const int64_t slot = int64_t(blockIdx.x) * kTileThreads + tid;
         t.active = slot < np;  // slot 0 of every tile exists, so thread 0 is active
         t.p = t.active ? int64_t(perm[slot]) : 0;
-        t.i = int(t.p % n);
-        t.j = int((t.p / n) % n);
-        t.k = int(t.p / (int64_t(n) * n));
+        LatticeDiv ld;
+        ld.init(n);
+        ld.ijk(t.p, t.i, t.j, t.k);
     } else {
         t.i = blockIdx.x * kTX + (tid % kTX);
         t.j = blockIdx.y * kTY + ((tid / kTX) % kTY);
