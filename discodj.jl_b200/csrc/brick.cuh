@@ -1,12 +1,17 @@
 // Brick-owned mass assignment and force interpolation.
 //
-// The particles are binned by the B^3-cell brick holding their (drifted) shift-0
-// base node (sort.cuh, linear brick order). One CTA owns one brick and every
-// particle binned into it. The brick's Eulerian box is known in advance:
-//   mass assignment  : nodes [B*b + lo - 1, B*b + B + W + 1), i.e. B + W + 2 per axis:
-//                      one node of margin on each side for the interlacing shifts
-//                      (+h/2, and -h/4 with antialias = 3) and odd-order rounding;
-//   interpolation    : the same box widened by the finite-difference halo R.
+// The particles are binned by the B^3-cell brick holding their (drifted) cell
+// floor(g) (sort.cuh, linear brick order). One CTA owns one brick and every particle
+// binned into it. The brick's Eulerian box is known in advance. The host bounds the
+// base node of a particle relative to its cell over the configuration's shifts, to
+// [lo, hi] (0 and 0 or 1 for shift 0; for a shift s the floor or round-to-nearest of
+// [c + s, c + 1 + s) widened by 0.01 cells of round-off, and by one more node below
+// for the ties of round-to-nearest). Then per axis:
+//   mass assignment  : nodes [B*b + lo + lo_W, B*b + B - 1 + hi + lo_W + W), i.e.
+//                      B + hi - lo + W - 1 nodes (BrickList::sos, sSs);
+//   interpolation    : the same box widened by the finite-difference halo R (so, sS).
+// A particle outside its box (the binning and the kernel disagree) sets error bit 2
+// and is clamped into the box.
 // An empty brick costs one read of its count; a dense brick loops over its particles
 // in rounds of 256 while its box stays in shared memory. The staged volume per step
 // is (number of non-empty bricks) x (box volume), independent of how far particles
@@ -19,7 +24,10 @@
 
 namespace djb {
 
-constexpr int kBrickRounds = 4;  // particles kept in registers per thread (interpolation)
+#ifndef DJB_BRICK_ROUNDS
+#define DJB_BRICK_ROUNDS 4
+#endif
+constexpr int kBrickRounds = DJB_BRICK_ROUNDS;  // particles kept per thread across the shifts (interpolation)
 
 struct BrickList {
     const unsigned* offset;  // block-local exclusive scan of the key counts
@@ -30,8 +38,12 @@ struct BrickList {
     int nsub;                // sort keys per brick (2^3-cell sub-blocks)
     int64_t nkeys;           // keys in total
     unsigned np;             // particles
-    int sx;                  // interpolation box width along x (aligned_box)
-    int ssx;                 // mass-assignment box width along x
+    int sx;                  // interpolation box: width along x (aligned_box),
+    int sS;                  //   extent along y and z,
+    int so;                  //   first node relative to the brick's first cell
+    int ssx;                 // mass-assignment box: width along x,
+    int sSs;                 //   extent along y and z,
+    int sos;                 //   first node relative to the brick's first cell
 };
 
 __device__ __forceinline__ unsigned key_start(const BrickList& bl, int64_t key) {
@@ -44,13 +56,13 @@ __device__ __forceinline__ void brick_range(const BrickList& bl, int b, unsigned
     cnt = key_start(bl, int64_t(b + 1) * bl.nsub) - start;
 }
 
-// Box of brick b: origin B*b + lo - R - 1 per axis, S = B + W + 2 + 2R nodes per axis.
-__device__ __forceinline__ TileBox brick_box(const BrickList& bl, int b, int lo_minus_r, int S) {
+// Box of brick b: origin B*b + first per axis, S nodes per axis.
+__device__ __forceinline__ TileBox brick_box(const BrickList& bl, int b, int first, int S) {
     TileBox box;
     const int bx = b % bl.nb, by = (b / bl.nb) % bl.nb, bz = b / (bl.nb * bl.nb);
-    box.o[0] = bx * bl.brick + lo_minus_r - 1;
-    box.o[1] = by * bl.brick + lo_minus_r - 1;
-    box.o[2] = bz * bl.brick + lo_minus_r - 1;
+    box.o[0] = bx * bl.brick + first;
+    box.o[1] = by * bl.brick + first;
+    box.o[2] = bz * bl.brick + first;
     box.S[0] = box.S[1] = box.S[2] = S;
     box.P = S | 1;
     box.plane = box.P * S;
@@ -58,7 +70,7 @@ __device__ __forceinline__ TileBox brick_box(const BrickList& bl, int b, int lo_
 }
 
 // Offset of a node from the box origin, periodic differences taken in [-4, res - 4):
-// valid offsets lie in [-1, B + W + 2R + 1] and res > B + W + 2R + 6 (brick <= res/2).
+// valid offsets lie in [0, sx - 1] and res > sx + 4 (the host sizes the bricks so).
 __device__ __forceinline__ int box_rel(int node, int origin, int res) {
     int v = (node - origin) % res;
     if (v < -4) v += res;
@@ -68,10 +80,10 @@ __device__ __forceinline__ int box_rel(int node, int origin, int res) {
 
 // Box of brick b with the x origin rounded down to a multiple of 4 nodes (so that
 // every row starts on a 16-byte boundary of a dense mesh) and `sx` nodes along x (a
-// multiple of 4, at least S + 3); y and z as brick_box. Shared memory holds the box
-// densely, [z][y][x] with rows of sx elements.
-__device__ __forceinline__ TileBox aligned_box(const BrickList& bl, int b, int lo_minus_r, int S, int sx) {
-    TileBox box = brick_box(bl, b, lo_minus_r, S);
+// multiple of 4 covering the S nodes after the rounding); y and z as brick_box.
+// Shared memory holds the box densely, [z][y][x] with rows of sx elements.
+__device__ __forceinline__ TileBox aligned_box(const BrickList& bl, int b, int first, int S, int sx) {
+    TileBox box = brick_box(bl, b, first, S);
     box.o[0] &= ~3;
     box.S[0] = sx;
     box.P = sx;
@@ -129,7 +141,7 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
     brick_range(bl, b, start, cnt);
     if (cnt == 0) return;
     const int tid = threadIdx.x;
-    const TileBox box = aligned_box(bl, b, WLo<W>::v, bl.brick + W + 2, bl.ssx);
+    const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
     const bool bulk = tma && box_inside(box, res) && (smem_u32(sacc) & 127u) == 0u;
     const bool vec = ((pitch | res) & 3) == 0;
     const float resf = float(res);
@@ -248,7 +260,7 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, 
     const int n = A.n;
     const int64_t np = A.np;
     const int res = A.res;
-    const TileBox box = aligned_box(bl, b, WLo<W>::v - R, bl.brick + W + 2 + 2 * R, bl.sx);
+    const TileBox box = aligned_box(bl, b, bl.so, bl.sS, bl.sx);
     const bool bulk = tma && box_inside(box, res) && (smem_u32(sbox) & 127u) == 0u;
     const bool vec = ((A.pitch | res) & 3) == 0;
     const unsigned box_bytes = unsigned(box.plane) * unsigned(box.S[2]) * 4u;

@@ -727,8 +727,10 @@ struct djb_solver {
     CUtensorMap tmap[kMaxGroup];
     CUtensorMap tmap_s[kMaxGroup];
     bool tma = false;
-    int gsx = 0;  // interpolation box width along x (brick kernels)
-    int ssx = 0;  // mass-assignment box width along x
+    // brick boxes (brick.cuh): width along x, extent along y and z, first node relative
+    // to the brick's first cell; g = interpolation, s = mass assignment
+    int gsx = 0, gS = 0, gfirst = 0;
+    int ssx = 0, sS = 0, sfirst = 0;
     float* fmesh[kMaxGroup][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     double* lapT = nullptr;
     double* makT = nullptr;
@@ -840,33 +842,69 @@ dim3 tile_grid(int n) {
 djb::BrickList brick_list(const djb_solver* s) {
     const int hb = s->sg.hb;
     return djb::BrickList{s->offset, s->bsum, s->perm, s->sg.nb, s->sg.brick, hb * hb * hb, s->nbins,
-                          unsigned(s->np), s->gsx, s->ssx};
+                          unsigned(s->np), s->gsx, s->gS, s->gfirst, s->ssx, s->sS, s->sfirst};
 }
 
-// Box width along x for bricks of `brick` cells and boxes of S = B + W + 2 + 2R nodes
-// (R = 0 for the mass assignment): the box starts anywhere in a 16-byte group after the
-// rounded-down origin, so S + 3 nodes rounded up to a multiple of 4; a width of 4 mod 8
-// keeps the rows of one plane on different shared-memory banks.
-int gather_sx(int brick, int W, int R) {
-    int sx = (brick + W + 2 + 2 * R + 6) & ~3;
+// Range [lo, hi] of a particle's base node relative to the cell floor(g) that bins it,
+// over the configuration's shifts (grid units). Shift 0 reproduces the binning's own
+// coordinate, so the base is the cell (even orders) or the cell or the next node (odd
+// orders round to nearest). Other shifts: the floor (or round-to-nearest) over
+// [c + s, c + 1 + s), widened by 0.01 cells for the round-off of mod(X + s, L) and, for
+// round-to-nearest, by one node below for ties rounded to even.
+void base_range(const djb_solver* s, int& lo, int& hi) {
+    const bool odd = (s->W % 2) != 0;
+    const double d = odd ? 0.5 : 0.0, eps = 0.01;
+    lo = 0;
+    hi = 0;
+    for (size_t i = 0; i < s->shifts.size(); ++i) {
+        const double sg = s->shifts[i] * s->res / s->L;
+        int l, h;
+        if (sg == 0.0) {
+            l = 0;
+            h = odd ? 1 : 0;
+        } else {
+            l = int(std::floor(sg + d - eps)) - (odd ? 1 : 0);
+            h = int(std::floor(sg + d + 1.0 + eps));
+        }
+        lo = (i == 0) ? l : std::min(lo, l);
+        hi = (i == 0) ? h : std::max(hi, h);
+    }
+}
+
+// Width along x of a box of S nodes whose first node lies `first` nodes from a brick
+// origin: rounded down to a 16-byte group the box starts up to 3 nodes earlier (exactly
+// first & 3 when bricks are multiples of 4 cells); rounded up to a multiple of 4, and to
+// 4 mod 8, which keeps the rows of one plane on different shared-memory banks.
+int box_sx(int brick, int S, int first) {
+    const int off = (brick % 4 == 0) ? (first & 3) : 3;
+    int sx = (S + off + 3) & ~3;
     if (sx % 8 == 0) sx += 4;
     return sx;
 }
 
+// Brick box geometry for bricks of `brick` cells (mass assignment and interpolation).
+void brick_boxes(djb_solver* s, int brick) {
+    int lo, hi;
+    base_range(s, lo, hi);
+    const int lw = (s->W == 2) ? 0 : -1;  // lowest stencil offset (pm.jl:53-55)
+    s->sS = brick + (hi - lo) + s->W - 1;
+    s->sfirst = lo + lw;
+    s->ssx = box_sx(brick, s->sS, s->sfirst);
+    s->gS = s->sS + 2 * s->R;
+    s->gfirst = s->sfirst - s->R;
+    s->gsx = box_sx(brick, s->gS, s->gfirst);
+}
+
 // Per shift of a group: one box, rounded up to 128 bytes (djb::box_stride).
 size_t scatter_smem(const djb_solver* s) {
-    const int S = s->sg.brick + s->W + 2;
-    return size_t(djb::box_stride(s->ssx * S * S)) * 4;
+    return size_t(djb::box_stride(s->ssx * s->sS * s->sS)) * 4;
 }
 
 // The density mesh of group member m (dense when the solver has dense meshes) and its pitch.
 float* rho_mesh(const djb_solver* s, int m) { return s->phi[m] ? s->phi[m] : s->mesh[m]; }
 int rho_pitch(const djb_solver* s) { return s->phi[0] ? s->res : s->pitch; }
 
-size_t gather_smem(const djb_solver* s) {
-    const int S = s->sg.brick + s->W + 2 + 2 * s->R;
-    return size_t(s->gsx) * S * S * 4;
-}
+size_t gather_smem(const djb_solver* s) { return size_t(s->gsx) * s->gS * s->gS * 4; }
 
 // Dynamic shared memory of a brick kernel, 2 CTAs per SM: 228 KB of shared memory
 // less 1 KB per CTA reserved by the runtime and the kernel's static barrier.
@@ -1330,16 +1368,15 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
     }
     TRY(dmalloc(s, (void**)&s->err, sizeof(int)));
     if (s->sorted) {
-        // bricks of 16^3 cells; smaller when a box (brick + W + 2 + 2R nodes, sx along x)
-        // would not stay well inside the periodic mesh (box_rel needs res > extent + 4)
+        // bricks of 16^3 cells; smaller when a box would not stay well inside the periodic
+        // mesh (box_rel needs res > box width + 4)
         int brick = 16, lgb = 4;
-        while (brick > 2 && (brick > s->res / 2 || brick + s->W + 2 + 2 * s->R + 4 >= s->res ||
-                             gather_sx(brick, s->W, s->R) + 4 >= s->res)) {
+        brick_boxes(s, brick);
+        while (brick > 2 && (brick > s->res / 2 || s->gsx + 4 >= s->res)) {
             brick /= 2;
             --lgb;
+            brick_boxes(s, brick);
         }
-        s->gsx = gather_sx(brick, s->W, s->R);
-        s->ssx = gather_sx(brick, s->W, 0);
         const int nb = (s->res + brick - 1) / brick;
         const int hb = brick > 2 ? brick / 2 : 1;
         s->sg = djb::SortGeom{s->res, brick, lgb, nb, hb};
@@ -1380,12 +1417,10 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                       cembed[0] * cembed[1] * cembed[2], CUFFT_R2C, 1, &work));
         CUFFT_TRY(cufftSetStream(s->r2c_d, s->stream));
         s->bytes += int64_t(work);
-        const int S = s->sg.brick + s->W + 2 + 2 * s->R;
-        const int Ss = s->sg.brick + s->W + 2;
-        if (s->sorted && s->gsx <= res && S <= res) {
+        if (s->sorted && s->gsx <= res) {
             for (int m = 0; m < s->group; ++m) {
-                TRY(make_tmap(&s->tmap[m], s->phi[m], res, s->gsx, S));
-                TRY(make_tmap(&s->tmap_s[m], s->phi[m], res, s->ssx, Ss));
+                TRY(make_tmap(&s->tmap[m], s->phi[m], res, s->gsx, s->gS));
+                TRY(make_tmap(&s->tmap_s[m], s->phi[m], res, s->ssx, s->sS));
             }
             for (int m = s->group; m < kMaxGroup; ++m) {
                 s->tmap[m] = s->tmap[0];

@@ -26,17 +26,18 @@ struct SortGeom {
     int hb;      // sub-blocks of 2 cells per brick side (brick / 2, at least 1)
 };
 
-// Sort key of the cell floor(g) (the shift-0 cell; the brick kernels' boxes have one
-// node of margin for the interlacing shifts and odd-order rounding): the linear brick
-// index, then the 2^3-cell sub-block inside the brick, so that particles of one cell
-// are consecutive in the sorted order.
+// Sort key of the cell floor(g) (the shift-0 cell; the brick kernels' boxes cover the
+// base nodes of the interlacing shifts and odd-order rounding around it): the linear
+// brick index, then the 2^3-cell sub-block inside the brick, so that particles of one
+// cell are consecutive in the sorted order.
 __device__ __forceinline__ uint32_t brick_key(const float X[3], float L, float resf, const SortGeom& sg, int* err) {
     int bc[3], sc[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float g = grid_coord(X[a], L, resf, err);
+        // g lies in [0, res]: g == res (mod(X, L) rounded up to L) is the node 0 image
         int c = __float2int_rd(g);
-        c = c < 0 ? 0 : (c >= sg.res ? sg.res - 1 : c);
+        c = c >= sg.res ? c - sg.res : (c < 0 ? 0 : c);
         bc[a] = c >> sg.lgb;
         sc[a] = (sg.hb > 1) ? ((c & (sg.brick - 1)) >> 1) : 0;
     }
