@@ -24,10 +24,16 @@
 
 namespace djb {
 
+// Interpolation: particles kept per thread across the shifts, and the resident CTAs per
+// SM its registers are sized for (3 x 256 threads at <= 85 registers; the 26^3-node
+// PCS box of 76 KB lets 3 CTAs share an SM's shared memory).
 #ifndef DJB_BRICK_ROUNDS
-#define DJB_BRICK_ROUNDS 4
+#define DJB_BRICK_ROUNDS 1
 #endif
-constexpr int kBrickRounds = DJB_BRICK_ROUNDS;  // particles kept per thread across the shifts (interpolation)
+#ifndef DJB_BRICK_GATHER_BLOCKS
+#define DJB_BRICK_GATHER_BLOCKS 3
+#endif
+constexpr int kBrickRounds = DJB_BRICK_ROUNDS;
 
 struct BrickList {
     const unsigned* offset;  // block-local exclusive scan of the key counts
@@ -126,15 +132,26 @@ __device__ __forceinline__ void for_box_wrapped(const TileBox& box, int res, int
 }
 
 // ── mass assignment ───────────────────────────────────────────────────────────
-// Box: B + W + 2 nodes per axis (bl.ssx along x); one box per shift of the group, all
-// filled in one pass over the brick's particles. `tma` != 0: the meshes are dense
-// [res]^3 (pitch == res) described by tm0/tm1 with boxes of ssx x S x S; boxes that do
-// not wrap are then added to the mesh with one bulk tensor reduction each.
+// Box: the deposit box (BrickList::ssx, sSs, sos); kScatterBoxes shifts of the group
+// are filled per pass over the brick's particles, one box each. One box per pass (45 KB
+// for PCS) and registers sized for 4 resident CTAs per SM measured faster than both
+// shifts per pass at 2 CTAs per SM. `tma` != 0: the meshes are dense [res]^3
+// (pitch == res) described by tm0/tm1 with boxes of the deposit box's shape; boxes that
+// do not wrap are then added to the mesh with one bulk tensor reduction each.
+#ifndef DJB_SCATTER_BOXES
+#define DJB_SCATTER_BOXES 1
+#endif
+#ifndef DJB_BRICK_SCATTER_BLOCKS
+#define DJB_BRICK_SCATTER_BLOCKS 4
+#endif
+constexpr int kScatterBoxes = DJB_SCATTER_BOXES;
+
 template <int W, int NS>
-__global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
+__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scatter_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     GroupShifts sh, float* __restrict__ mesh0, float* __restrict__ mesh1, int* err, BrickList bl,
     const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1, int tma) {
+    constexpr int NB = kScatterBoxes < NS ? kScatterBoxes : NS;  // boxes per particle pass
     extern __shared__ __align__(128) unsigned int sacc[];
     const int b = blockIdx.x;
     unsigned start, cnt;
@@ -147,85 +164,90 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_scatter_brick(
     const float resf = float(res);
     const int cells = box.plane * box.S[2];  // a multiple of 4
     const int stride = box_stride(cells);    // boxes start on 128-byte boundaries (bulk tensor copies)
-    for (int t = 4 * tid; t < NS * stride; t += 4 * kTileThreads)
-        *reinterpret_cast<uint4*>(sacc + t) = make_uint4(0u, 0u, 0u, 0u);
     LatticeDiv ld;
     ld.init(n);
-    __syncthreads();
-    for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
-        // lanes 8 slots apart: particles of one cell land in different warps, which
-        // keeps same-address shared atomics out of a single instruction
-        const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
-        if (slot >= cnt) continue;
-        const int64_t p = bl.perm[start + slot];
-        int i, j, k;
-        ld.ijk(p, i, j, k);
-        const float X[3] = {psi[p] + q1[i], psi[p + np] + q1[j], psi[p + 2 * np] + q1[k]};
 #pragma unroll 1
-        for (int g = 0; g < NS; ++g) {
-            const Shift3 sg = (g == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
-            unsigned int* acc = sacc + g * stride;
-            float w[3][W];
-            int d[3];
+    for (int g0 = 0; g0 < NS; g0 += NB) {
+        for (int t = 4 * tid; t < NB * stride; t += 4 * kTileThreads)
+            *reinterpret_cast<uint4*>(sacc + t) = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
+            // lanes 8 slots apart: particles of one cell land in different warps, which
+            // keeps same-address shared atomics out of a single instruction
+            const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
+            if (slot >= cnt) continue;
+            const int64_t p = bl.perm[start + slot];
+            int i, j, k;
+            ld.ijk(p, i, j, k);
+            const float X[3] = {psi[p] + q1[i], psi[p + np] + q1[j], psi[p + 2 * np] + q1[k]};
+#pragma unroll 1
+            for (int gb = 0; gb < NB; ++gb) {
+                const int g = g0 + gb;
+                const Shift3 sg = (g == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
+                unsigned int* acc = sacc + gb * stride;
+                float w[3][W];
+                int d[3];
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const float s = (a == 0) ? sg.x : (a == 1) ? sg.y : sg.z;
-                const float gc = grid_coord(X[a] + s, L, resf, err);
-                const int bb = wbase<W>(gc);
+                for (int a = 0; a < 3; ++a) {
+                    const float s = (a == 0) ? sg.x : (a == 1) ? sg.y : sg.z;
+                    const float gc = grid_coord(X[a] + s, L, resf, err);
+                    const int bb = wbase<W>(gc);
 #pragma unroll
-                for (int o = 0; o < W; ++o) w[a][o] = wk<W>(fabsf(gc - float(bb + WLo<W>::v + o)));
-                d[a] = box_rel(bb + WLo<W>::v, box.o[a], res);
-                if (d[a] < 0 || d[a] > box.S[a] - W) {  // not binned consistently: report, stay in bounds
-                    atomicOr(err, 2);
-                    d[a] = d[a] < 0 ? 0 : box.S[a] - W;
+                    for (int o = 0; o < W; ++o) w[a][o] = wk<W>(fabsf(gc - float(bb + WLo<W>::v + o)));
+                    d[a] = box_rel(bb + WLo<W>::v, box.o[a], res);
+                    if (d[a] < 0 || d[a] > box.S[a] - W) {  // not binned consistently: report, stay in bounds
+                        atomicOr(err, 2);
+                        d[a] = d[a] < 0 ? 0 : box.S[a] - W;
+                    }
                 }
+#pragma unroll
+                for (int c = 0; c < W; ++c)
+#pragma unroll
+                    for (int bb = 0; bb < W; ++bb) {
+                        unsigned int* row = acc + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+                        const float wyz = w[1][bb];
+#pragma unroll
+                        for (int a = 0; a < W; ++a)
+                            atomicAdd(row + a, __float2uint_rn(w[0][a] * wyz * w[2][c] * FixScale<W>::up));
+                    }
             }
-#pragma unroll
-            for (int c = 0; c < W; ++c)
-#pragma unroll
-                for (int bb = 0; bb < W; ++bb) {
-                    unsigned int* row = acc + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
-                    const float wyz = w[1][bb];
-#pragma unroll
-                    for (int a = 0; a < W; ++a)
-                        atomicAdd(row + a, __float2uint_rn(w[0][a] * wyz * w[2][c] * FixScale<W>::up));
-                }
-        }
-    }
-    __syncthreads();
-    if (bulk) {
-        // fixed point -> float in place, then one bulk reduction per box
-        for (int t = 4 * tid; t < NS * stride; t += 4 * kTileThreads) {
-            const uint4 v = *reinterpret_cast<const uint4*>(sacc + t);
-            *reinterpret_cast<float4*>(sacc + t) =
-                make_float4(__uint2float_rn(v.x) * FixScale<W>::down, __uint2float_rn(v.y) * FixScale<W>::down,
-                            __uint2float_rn(v.z) * FixScale<W>::down, __uint2float_rn(v.w) * FixScale<W>::down);
-        }
-        fence_proxy_async_smem();  // the conversions are read by the bulk copies below
-        __syncthreads();
-        if (tid == 0) {
-            tma_reduce_add_3d(&tm0, box.o[0], box.o[1], box.o[2], sacc);
-            if (NS > 1) tma_reduce_add_3d(&tm1, box.o[0], box.o[1], box.o[2], sacc + stride);
-            bulk_commit_and_wait_read();  // shared memory stays allocated until read
         }
         __syncthreads();
-    } else {
+        if (bulk) {
+            // fixed point -> float in place, then one bulk reduction per box
+            for (int t = 4 * tid; t < NB * stride; t += 4 * kTileThreads) {
+                const uint4 v = *reinterpret_cast<const uint4*>(sacc + t);
+                *reinterpret_cast<float4*>(sacc + t) =
+                    make_float4(__uint2float_rn(v.x) * FixScale<W>::down, __uint2float_rn(v.y) * FixScale<W>::down,
+                                __uint2float_rn(v.z) * FixScale<W>::down, __uint2float_rn(v.w) * FixScale<W>::down);
+            }
+            fence_proxy_async_smem();  // the conversions are read by the bulk copies below
+            __syncthreads();
+            if (tid == 0) {
+                for (int gb = 0; gb < NB; ++gb)
+                    tma_reduce_add_3d((g0 + gb == 0) ? &tm0 : &tm1, box.o[0], box.o[1], box.o[2], sacc + gb * stride);
+                bulk_commit_and_wait_read();  // shared memory stays allocated until read
+            }
+            __syncthreads();
+        } else {
 #pragma unroll 1
-        for (int g = 0; g < NS; ++g) {
-            float* mesh = (g == 0) ? mesh0 : mesh1;
-            const unsigned int* acc = sacc + g * stride;
-            for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
-                if (vec) {
-                    const uint4 v = *reinterpret_cast<const uint4*>(acc + so);
-                    if ((v.x | v.y | v.z | v.w) == 0u) return;
-                    red_add_v4(mesh + go, __uint2float_rn(v.x) * FixScale<W>::down,
-                               __uint2float_rn(v.y) * FixScale<W>::down, __uint2float_rn(v.z) * FixScale<W>::down,
-                               __uint2float_rn(v.w) * FixScale<W>::down);
-                } else {
-                    const unsigned v = acc[so];
-                    if (v != 0u) atomicAdd(mesh + go, __uint2float_rn(v) * FixScale<W>::down);
-                }
-            });
+            for (int gb = 0; gb < NB; ++gb) {
+                float* mesh = (g0 + gb == 0) ? mesh0 : mesh1;
+                const unsigned int* acc = sacc + gb * stride;
+                for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
+                    if (vec) {
+                        const uint4 v = *reinterpret_cast<const uint4*>(acc + so);
+                        if ((v.x | v.y | v.z | v.w) == 0u) return;
+                        red_add_v4(mesh + go, __uint2float_rn(v.x) * FixScale<W>::down,
+                                   __uint2float_rn(v.y) * FixScale<W>::down, __uint2float_rn(v.z) * FixScale<W>::down,
+                                   __uint2float_rn(v.w) * FixScale<W>::down);
+                    } else {
+                        const unsigned v = acc[so];
+                        if (v != 0u) atomicAdd(mesh + go, __uint2float_rn(v) * FixScale<W>::down);
+                    }
+                });
+            }
+            __syncthreads();
         }
     }
 }
@@ -246,7 +268,7 @@ __device__ __forceinline__ void stage_box_wrapped(float* sbox, const float* __re
 // `tma` != 0: the potentials are dense [res]^3 meshes (pitch == res) described by tm0/tm1
 // (box sx x S x S); boxes that do not wrap are then fetched with one bulk tensor copy.
 template <int W, int R, int NS>
-__global__ void __launch_bounds__(kTileThreads, 2) k_gather_brick(GatherArgs A, BrickList bl,
+__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gather_brick(GatherArgs A, BrickList bl,
                                                                   const __grid_constant__ CUtensorMap tm0,
                                                                   const __grid_constant__ CUtensorMap tm1, int tma) {
     extern __shared__ __align__(128) float sbox[];

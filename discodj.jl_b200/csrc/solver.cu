@@ -939,7 +939,7 @@ void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShi
     if (s->tiled && s->cur_perm) {  // brick-owned: the drift was applied by the binning pass
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const int tma = (dense && s->tma) ? 1 : 0;
-        djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, NS * scatter_smem(s), s->stream>>>(
+        djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, std::min(NS, djb::kScatterBoxes) * scatter_smem(s), s->stream>>>(
             s->psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, m0, m1, s->err, brick_list(s), s->tmap_s[0],
             s->tmap_s[NS > 1 ? 1 : 0], tma);
         return;
