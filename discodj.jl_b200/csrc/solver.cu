@@ -619,6 +619,24 @@ __global__ void k_wrap_psi_lin(const float* __restrict__ psi, const float* __res
 }  // namespace djb
 
 #include "brick.cuh"
+#include "zpencil.cuh"
+
+namespace djb {
+// Kφ as a functor for the fused z pass.
+struct KPhiFn {
+    const double* T;
+    const double* M;
+    double s0;
+    __device__ __forceinline__ float operator()(int kx, int ky, int kz) const { return kphi(T, M, s0, kx, ky, kz); }
+    // float64 sums and products, one float division (within 1.5 ulp of the above)
+    __device__ __forceinline__ float fast(int kx, int ky, int kz) const {
+        if ((kx | ky | kz) == 0) return 0.0f;
+        double num = s0;
+        if (M) num *= M[kx] * M[ky] * M[kz];
+        return float(num) / float(T[kx] + T[ky] + T[kz]);
+    }
+};
+}  // namespace djb
 
 // ─────────────────────────────────────────────────────────────────────────────
 // solver object
@@ -727,6 +745,11 @@ struct djb_solver {
     CUtensorMap tmap[kMaxGroup];
     CUtensorMap tmap_s[kMaxGroup];
     bool tma = false;
+    // res == 1024: the dense transforms are batched 2-D transforms of the z planes and
+    // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
+    bool zpass = false;
+    float2* wN = nullptr;
+    int nsm = 148;  // SMs of the device (persistent grids)
     // brick boxes (brick.cuh): width along x, extent along y and z, first node relative
     // to the brick's first cell; g = interpolation, s = mass assignment
     int gsx = 0, gS = 0, gfirst = 0;
@@ -1163,7 +1186,17 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
             else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
             s->prof.end(s->stream, PH_R2C, 0);
-            if (!ik) {
+            if (s->zpass) {
+                s->prof.begin(s->stream, PH_KSPACE);
+                const int nh = s->res / 2 + 1;
+                djb::k_zpencil_kphi<<<dim3(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res)),
+                                      djb::kZThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh, s->wN,
+                                                                                djb::KPhiFn{s->lapT, s->makT, s->s0});
+                s->prof.end(s->stream, PH_KSPACE, 1);
+                s->prof.begin(s->stream, PH_C2R);
+                CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+                s->prof.end(s->stream, PH_C2R, 0);
+            } else if (!ik) {
                 s->prof.begin(s->stream, PH_KSPACE);
                 djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)),
                                     kThreads, 0, s->stream>>>(
@@ -1310,6 +1343,7 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         s->c3 = float(d3);
     }
     CUDA_TRY(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, cfg->device));
     s->stream = s->own_stream;
 
     // 1-D tables (float64): lap terms, deconvolution, ik gradient
@@ -1402,21 +1436,45 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         // dense potentials written by an out-of-place C2R from the (padded) spectrum
         for (int m = 0; m < s->group; ++m)
             TRY(dmalloc(s, (void**)&s->phi[m], sizeof(float) * size_t(res) * res * res));
-        CUFFT_TRY(cufftCreate(&s->c2r_d));
-        s->have_c2r_d = true;
+        {
+            const char* zp = std::getenv("DJB_ZPASS");
+            s->zpass = (res == djb::kZRes) && !(zp && std::strcmp(zp, "0") == 0);
+        }
+        // 3-D transforms, or with the fused z pass 2-D transforms batched over the z planes
+        const int rank = s->zpass ? 2 : 3;
+        const long long batch = s->zpass ? res : 1;
         long long dims[3] = {res, res, res};
         long long cembed[3] = {res, res, res / 2 + 1};
         long long dembed[3] = {res, res, res};
-        CUFFT_TRY(cufftMakePlanMany64(s->c2r_d, 3, dims, cembed, 1, cembed[0] * cembed[1] * cembed[2], dembed, 1,
-                                      dembed[0] * dembed[1] * dembed[2], CUFFT_C2R, 1, &work));
+        long long* cd = s->zpass ? cembed + 1 : cembed;
+        long long* dd = s->zpass ? dembed + 1 : dembed;
+        const long long cdist = s->zpass ? cembed[1] * cembed[2] : cembed[0] * cembed[1] * cembed[2];
+        const long long ddist = s->zpass ? dembed[1] * dembed[2] : dembed[0] * dembed[1] * dembed[2];
+        CUFFT_TRY(cufftCreate(&s->c2r_d));
+        s->have_c2r_d = true;
+        CUFFT_TRY(cufftMakePlanMany64(s->c2r_d, rank, s->zpass ? dims + 1 : dims, cd, 1, cdist, dd, 1, ddist,
+                                      CUFFT_C2R, batch, &work));
         CUFFT_TRY(cufftSetStream(s->c2r_d, s->stream));
         s->bytes += int64_t(work);
         CUFFT_TRY(cufftCreate(&s->r2c_d));
         s->have_r2c_d = true;
-        CUFFT_TRY(cufftMakePlanMany64(s->r2c_d, 3, dims, dembed, 1, dembed[0] * dembed[1] * dembed[2], cembed, 1,
-                                      cembed[0] * cembed[1] * cembed[2], CUFFT_R2C, 1, &work));
+        CUFFT_TRY(cufftMakePlanMany64(s->r2c_d, rank, s->zpass ? dims + 1 : dims, dd, 1, ddist, cd, 1, cdist,
+                                      CUFFT_R2C, batch, &work));
         CUFFT_TRY(cufftSetStream(s->r2c_d, s->stream));
         s->bytes += int64_t(work);
+        if (s->zpass) {
+            std::vector<float2> w(res);
+            for (int j = 0; j < res; ++j)
+                w[j] = make_float2(float(std::cos(2 * M_PI * j / res)), float(-std::sin(2 * M_PI * j / res)));
+            TRY(dmalloc(s, (void**)&s->wN, sizeof(float2) * res));
+            CUDA_TRY(cudaMemcpy(s->wN, w.data(), sizeof(float2) * res, cudaMemcpyHostToDevice));
+            float2 w32[16];
+            for (int j = 0; j < 16; ++j)
+                w32[j] = make_float2(float(std::cos(2 * M_PI * j / 32)), float(-std::sin(2 * M_PI * j / 32)));
+            CUDA_TRY(cudaMemcpyToSymbol(djb::c_w32, w32, sizeof(w32)));
+            CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_kphi<djb::KPhiFn>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
+        }
         if (s->sorted && s->gsx <= res) {
             for (int m = 0; m < s->group; ++m) {
                 TRY(make_tmap(&s->tmap[m], s->phi[m], res, s->gsx, s->gS));
