@@ -77,10 +77,12 @@ __device__ __forceinline__ TileBox brick_box(const BrickList& bl, int b, int fir
 
 // Offset of a node from the box origin, periodic differences taken in [-4, res - 4):
 // valid offsets lie in [0, sx - 1] and res > sx + 4 (the host sizes the bricks so).
+// node - origin lies in [-res - 4, 2 res - 4) (nodes in [-5, res + 2], origins in
+// [-5, res)), so one correction either way suffices.
 __device__ __forceinline__ int box_rel(int node, int origin, int res) {
-    int v = (node - origin) % res;
+    int v = node - origin;
     if (v < -4) v += res;
-    else if (v >= res - 4) v -= res;
+    if (v >= res - 4) v -= res;
     return v;
 }
 
@@ -134,15 +136,15 @@ __device__ __forceinline__ void for_box_wrapped(const TileBox& box, int res, int
 // ── mass assignment ───────────────────────────────────────────────────────────
 // Box: the deposit box (BrickList::ssx, sSs, sos); kScatterBoxes shifts of the group
 // are filled per pass over the brick's particles, one box each. One box per pass (45 KB
-// for PCS) and registers sized for 4 resident CTAs per SM measured faster than both
-// shifts per pass at 2 CTAs per SM. `tma` != 0: the meshes are dense [res]^3
+// for PCS) and registers sized for 5 resident CTAs per SM (48 registers, no spills)
+// measured faster than both shifts per pass at 2 CTAs per SM, and than 4 CTAs per SM. `tma` != 0: the meshes are dense [res]^3
 // (pitch == res) described by tm0/tm1 with boxes of the deposit box's shape; boxes that
 // do not wrap are then added to the mesh with one bulk tensor reduction each.
 #ifndef DJB_SCATTER_BOXES
 #define DJB_SCATTER_BOXES 1
 #endif
 #ifndef DJB_BRICK_SCATTER_BLOCKS
-#define DJB_BRICK_SCATTER_BLOCKS 4
+#define DJB_BRICK_SCATTER_BLOCKS 5
 #endif
 constexpr int kScatterBoxes = DJB_SCATTER_BOXES;
 

@@ -17,7 +17,13 @@
 namespace djb {
 
 // Julia `mod(x::Float32, y::Float32)` for y > 0 (rem, then add y when the sign differs).
+// Positions lie within one box length of [0, y), where the remainder is exact and
+// needs no fmodf: x itself, x - y (exact for y <= x < 2y), or x + y for -y <= x < 0
+// (the remainder x, then + y as below).
 __device__ __forceinline__ float jmodf(float x, float y) {
+    if (x >= 0.0f && x < y) return x;
+    if (x >= y && x < 2.0f * y) return x - y;
+    if (x < 0.0f && x >= -y) return x + y;
     float r = fmodf(x, y);
     if (r < 0.0f) r += y;
     return r;

@@ -35,7 +35,10 @@ namespace djb {
 #endif
 
 constexpr int kZRes = 1024;
-constexpr int kZPencils = 8;           // kx per CTA
+#ifndef DJB_ZPASS_PENCILS
+#define DJB_ZPASS_PENCILS 8
+#endif
+constexpr int kZPencils = DJB_ZPASS_PENCILS;  // kx per CTA
 constexpr int kZThreads = kZPencils * 32;
 constexpr int kZRow = 33;              // shared row pitch (float2), breaks bank alignment
 constexpr int kZPlane = 32 * kZRow + 2;  // per-pencil block (float2)
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(kZThreads, DJB_ZPASS_BLOCKS) k_zpencil_kphi(fl
                                                                              KPhi kphi) {
     extern __shared__ __align__(16) float2 s[];  // kZPencils transpose blocks (then Kφ rows)
     const int q = threadIdx.x & (kZPencils - 1);
-    const int t = threadIdx.x >> 3;  // n2 (steps A, B'), k1 (steps B, A')
+    const int t = threadIdx.x / kZPencils;  // n2 (steps A, B'), k1 (steps B, A')
     const int ky = blockIdx.y;
     const int kx = blockIdx.x * kZPencils + q;
     const bool active = kx < nh;
