@@ -56,6 +56,31 @@ __device__ __forceinline__ unsigned key_start(const BrickList& bl, int64_t key) 
     return key >= bl.nkeys ? bl.np : bl.offset[key] + bl.bsum[key / kScanBlock];
 }
 
+// Brick processed by CTA `blk`. DJB_BRICK_MORTON = 1 and a power-of-two number of bricks
+// per axis: Morton (Z-order) order, so that CTAs running at the same time own bricks
+// that are neighbours along all three axes and share their boxes' overlap in L2;
+// otherwise linear order (x fastest).
+#ifndef DJB_BRICK_MORTON
+#define DJB_BRICK_MORTON 1
+#endif
+__device__ __forceinline__ int compact3(unsigned v) {  // every third bit of v, from bit 0
+    v &= 0x09249249u;
+    v = (v ^ (v >> 2)) & 0x030c30c3u;
+    v = (v ^ (v >> 4)) & 0x0300f00fu;
+    v = (v ^ (v >> 8)) & 0xff0000ffu;
+    v = (v ^ (v >> 16)) & 0x000003ffu;
+    return int(v);
+}
+__device__ __forceinline__ int brick_of_block(const BrickList& bl, unsigned blk) {
+#if DJB_BRICK_MORTON
+    if ((bl.nb & (bl.nb - 1)) == 0 && bl.nb <= 1024) {
+        const int bx = compact3(blk), by = compact3(blk >> 1), bz = compact3(blk >> 2);
+        return (bz * bl.nb + by) * bl.nb + bx;
+    }
+#endif
+    return int(blk);
+}
+
 // Sorted range [start, start + cnt) of the particles of brick b.
 __device__ __forceinline__ void brick_range(const BrickList& bl, int b, unsigned& start, unsigned& cnt) {
     start = key_start(bl, int64_t(b) * bl.nsub);
@@ -155,7 +180,7 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
     const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1, int tma) {
     constexpr int NB = kScatterBoxes < NS ? kScatterBoxes : NS;  // boxes per particle pass
     extern __shared__ __align__(128) unsigned int sacc[];
-    const int b = blockIdx.x;
+    const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
     if (cnt == 0) return;
@@ -276,7 +301,7 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
     extern __shared__ __align__(128) float sbox[];
     __shared__ __align__(8) uint64_t s_bar;
     constexpr int E = W + 2 * R;
-    const int b = blockIdx.x;
+    const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
     if (cnt == 0) return;
