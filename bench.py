@@ -51,14 +51,16 @@ def algorithmic_bytes(n, res, nshift=2):
 
     step: n_shift·(24·N_m + 24·N_p) + 48·N_p (one compulsory pass per array).
     kernels, per launch (one launch covers the 2 interlacing meshes):
-      scatter: read Ψ, Mom (24 B/particle), write Ψ (12), write each mesh (4 B/cell)
+      scatter: read Ψ (12 B/particle) and the sort order (4), write each mesh (4 B/cell);
+               the first drift is applied by the binning pass
       gather:  read Ψ, Mom (24), write Ψ, Mom (24), read each potential mesh (4 B/cell)
-      kspace:  read + write the half spectrum of one mesh (16 B/complex mode)"""
+      kspace:  read + write the half spectrum of one mesh (16 B/complex mode); the same
+               for the fused z pass (forward z DFT, Kφ, inverse z DFT) at 1024³"""
     Np, Nm = n ** 3, res ** 3
     modes = res * res * (res // 2 + 1)
     return dict(
         step=nshift * (24 * Nm + 24 * Np) + 48 * Np,
-        scatter=36 * Np + 4 * Nm * nshift,
+        scatter=16 * Np + 4 * Nm * nshift,
         gather=48 * Np + 4 * Nm * nshift,
         kspace=16 * modes,
     )
