@@ -22,7 +22,10 @@ namespace djb {
 int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cudaStream_t* st);
 int64_t solver_np(const djb_solver* s);
 cufftHandle solver_r2c(const djb_solver* s);
+cufftHandle solver_c2r(const djb_solver* s);
 double solver_boxsize(const djb_solver* s);
+int solver_cic_gather_grad(djb_solver* s, const float* mesh, int pitch, float* psibar);
+int solver_check_err(djb_solver* s);
 }  // namespace djb
 
 namespace {
@@ -99,6 +102,40 @@ __global__ void __launch_bounds__(kThreads) k_shells(const float2* __restrict__ 
     }
 }
 
+// spec[k] *= coef[bin(k)] (0 outside every bin): the bins of k_shells.
+__global__ void __launch_bounds__(kThreads) k_shell_scale(float2* __restrict__ f, int res, double dk,
+                                                          const double* __restrict__ edges, int bins,
+                                                          const double* __restrict__ coef) {
+    const int nh = res / 2 + 1;
+    const int64_t total = int64_t(res) * res * nh;
+    const double kmin = edges[0], kmax = edges[bins];
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int kx = int(t % nh);
+        const int iy = int((t / nh) % res);
+        const int iz = int(t / (int64_t(nh) * res));
+        const double ky = double(iy <= res / 2 ? iy : iy - res) * dk;
+        const double kz = double(iz <= res / 2 ? iz : iz - res) * dk;
+        const double kh = double(kx) * dk;
+        const double k = sqrt((kz * kz + ky * ky) + kh * kh);
+        double c = 0.0;
+        if (k >= kmin && k < kmax) {
+            int lo = 0, hi = bins;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (edges[mid] <= k) lo = mid;
+                else hi = mid;
+            }
+            c = coef[lo];
+        }
+        const float cf = float(c);
+        float2 v = f[t];
+        v.x *= cf;
+        v.y *= cf;
+        f[t] = v;
+    }
+}
+
 // Julia LinRange element j of n (power_spectrum.jl:50-52).
 double linrange(double a, double b, int j, int n) {
     if (j == 0) return a;
@@ -120,7 +157,7 @@ std::vector<double> bin_edges(int res, double boxsize, int bins, bool logarithmi
 
 // Bins the spectrum `spec` (already transformed) and writes k, P, N on the host.
 int shells(const float2* spec, int res, double boxsize, double scale2, int bins, bool logarithmic,
-           double* k_out, double* pk_out, int64_t* n_out, cudaStream_t st) {
+           double* k_out, double* pk_out, int64_t* n_out, cudaStream_t st, double* wsum_out = nullptr) {
     std::vector<double> e = bin_edges(res, boxsize, bins, logarithmic);
     double* d_edges = nullptr;
     double* d_sums = nullptr;
@@ -170,6 +207,7 @@ int shells(const float2* spec, int res, double boxsize, double scale2, int bins,
     if (rc != DJB_OK) return rc;
     for (int b = 0; b < bins; ++b) {
         const unsigned long long n = counts[b];
+        if (wsum_out) wsum_out[b] = sums[4 * b + 1];
         if (n == 0) {
             k_out[b] = std::sqrt(e[b] * e[b + 1]);
             pk_out[b] = 0.0;
@@ -351,6 +389,79 @@ int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logarithmic, d
     const double f = double(res) * res * res / double(djb::solver_np(s));
     return shells(reinterpret_cast<const float2*>(mesh), res, djb::solver_boxsize(s), f * f, bins,
                   logarithmic != 0, k, pk, nmodes, st);
+}
+
+// Ψ̄ of Σ_b P̄_b·P_b for the solver's particle state, P as djb_state_power_spectrum.
+// P_b = (V/res⁶)·Σ_half w|δ̂|²/Σ_half w with δ = mesh·res³/n³ − 1, so
+// ∂/∂mesh(n) = Σ_b P̄_b·(V/res⁶)/(Σ_half w)_b·(res³/n³)²·Σ_{k∈b, full} f_k e^{ik·n}
+// with f the R2C of the CIC mesh: the spectrum is scaled per bin and brought back by the
+// unnormalised C2R, and the CIC weight derivatives gather it to the particles.
+int djb_state_power_spectrum_vjp(djb_solver* s, int32_t bins, int32_t logarithmic, const double* pk_bar,
+                                 float* psi_bar, int32_t mem) {
+    djb::clear_error();
+    if (!s || !pk_bar || !psi_bar) return fail(DJB_ERR_INVALID, "null argument");
+    if (bins < 1 || bins > kMaxBins) return fail(DJB_ERR_INVALID, "bins must be in 1..%d", kMaxBins);
+    float* mesh = nullptr;
+    int res = 0, pitch = 0;
+    cudaStream_t st = nullptr;
+    int rc = djb::solver_deposit_cic(s, &mesh, &res, &pitch, &st);
+    if (rc != DJB_OK) return rc;
+    CUFFT_TRY(cufftExecR2C(djb::solver_r2c(s), mesh, reinterpret_cast<cufftComplex*>(mesh)));
+    const double boxsize = djb::solver_boxsize(s);
+    const double f = double(res) * res * res / double(djb::solver_np(s));
+    std::vector<double> kk(bins), pk(bins), wsum(bins), coef(bins);
+    std::vector<int64_t> nm(bins);
+    rc = shells(reinterpret_cast<const float2*>(mesh), res, boxsize, f * f, bins, logarithmic != 0, kk.data(),
+                pk.data(), nm.data(), st, wsum.data());
+    if (rc != DJB_OK) return rc;
+    const double V = boxsize * boxsize * boxsize;
+    const double r3 = double(res) * res * res;
+    for (int b = 0; b < bins; ++b) coef[b] = (wsum[b] > 0.0) ? pk_bar[b] * (V / (r3 * r3)) / wsum[b] * f * f : 0.0;
+    const size_t count = size_t(3 * djb::solver_np(s));
+    std::vector<double> e = bin_edges(res, boxsize, bins, logarithmic != 0);
+    double* d_edges = nullptr;
+    double* d_coef = nullptr;
+    float* d_bar = nullptr;
+    auto cleanup = [&]() {
+        if (d_edges) cudaFreeAsync(d_edges, st);
+        if (d_coef) cudaFreeAsync(d_coef, st);
+        if (d_bar && mem == DJB_MEM_HOST) cudaFreeAsync(d_bar, st);
+    };
+    if (cudaMallocAsync((void**)&d_edges, sizeof(double) * (bins + 1), st) != cudaSuccess ||
+        cudaMallocAsync((void**)&d_coef, sizeof(double) * bins, st) != cudaSuccess ||
+        (mem == DJB_MEM_HOST && cudaMallocAsync((void**)&d_bar, sizeof(float) * count, st) != cudaSuccess)) {
+        cudaGetLastError();
+        cleanup();
+        return fail(DJB_ERR_ALLOC, "P(k) VJP work area allocation failed");
+    }
+    if (mem != DJB_MEM_HOST) d_bar = psi_bar;
+    do {
+        if (cudaMemcpyAsync(d_edges, e.data(), sizeof(double) * (bins + 1), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(d_coef, coef.data(), sizeof(double) * bins, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemsetAsync(d_bar, 0, sizeof(float) * count, st) != cudaSuccess) {
+            rc = fail(DJB_ERR_CUDA, "P(k) VJP set-up copy failed");
+            break;
+        }
+        const int64_t total = int64_t(res) * res * (res / 2 + 1);
+        const int grid = int(std::min<int64_t>((total + kThreads - 1) / kThreads, 148 * 16));
+        k_shell_scale<<<grid, kThreads, 0, st>>>(reinterpret_cast<float2*>(mesh), res, 2 * M_PI / boxsize, d_edges,
+                                                 bins, d_coef);
+        if (cufftExecC2R(djb::solver_c2r(s), reinterpret_cast<cufftComplex*>(mesh), mesh) != CUFFT_SUCCESS) {
+            rc = fail(DJB_ERR_CUFFT, "C2R of the P(k) cotangent failed");
+            break;
+        }
+        rc = djb::solver_cic_gather_grad(s, mesh, pitch, d_bar);
+        if (rc != DJB_OK) break;
+        if (mem == DJB_MEM_HOST &&
+            cudaMemcpyAsync(psi_bar, d_bar, sizeof(float) * count, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+            rc = fail(DJB_ERR_CUDA, "P(k) VJP read-back failed");
+            break;
+        }
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(DJB_ERR_CUDA, "P(k) VJP failed");
+    } while (false);
+    cleanup();
+    if (rc != DJB_OK) return rc;
+    return djb::solver_check_err(s);
 }
 
 }  // extern "C"

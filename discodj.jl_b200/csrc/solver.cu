@@ -620,6 +620,7 @@ __global__ void k_wrap_psi_lin(const float* __restrict__ psi, const float* __res
 
 #include "brick.cuh"
 #include "zpencil.cuh"
+#include "adjoint.cuh"
 
 namespace djb {
 // Kφ as a functor for the fused z pass.
@@ -749,6 +750,7 @@ struct djb_solver {
     // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
     bool zpass = false;
     float2* wN = nullptr;
+    float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
     int nsm = 148;  // SMs of the device (persistent grids)
     // brick boxes (brick.cuh): width along x, extent along y and z, first node relative
     // to the brick's first cell; g = interpolation, s = mass assignment
@@ -1257,6 +1259,91 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
     return DJB_OK;
 }
 
+// Potential of the density in rho_mesh(s, m), left in the same mesh: R2C, Kφ, C2R with the
+// force's transforms (finite-difference configurations).
+int poisson(djb_solver* s, int m) {
+    float* mesh = s->mesh[m];
+    cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
+    if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
+    else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
+    const int nh = s->res / 2 + 1;
+    if (s->zpass) {
+        djb::k_zpencil_kphi<<<dim3(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res)),
+                              djb::kZThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh, s->wN,
+                                                                        djb::KPhiFn{s->lapT, s->makT, s->s0});
+        CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+    } else {
+        djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)), kThreads,
+                            0, s->stream>>>(reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
+        if (s->phi[m]) CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+        else CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
+    }
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+template <int W>
+void launch_vjp_kernels(djb_solver* s, int stage, const float* psi, const float* abar, float* psibar,
+                        const Shift3& sh, float scale) {
+    float* rho = rho_mesh(s, 0);
+    const int pitch = rho_pitch(s);
+    const int b = blocks(s->np);
+    if (stage == 0)
+        djb::k_gather_grad<W><<<b, 256, 0, s->stream>>>(psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y,
+                                                         sh.z, s->adj[0], s->adj[1], s->adj[2], abar, scale, psibar,
+                                                         s->err);
+    else if (stage == 1)
+        djb::k_scatter_weighted<W><<<b, 256, 0, s->stream>>>(psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x,
+                                                              sh.y, sh.z, abar, scale, s->adj[0], s->adj[1],
+                                                              s->adj[2], s->err);
+    else
+        djb::k_gather_grad<W><<<b, 256, 0, s->stream>>>(psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y,
+                                                         sh.z, rho, nullptr, nullptr, nullptr, scale, psibar, s->err);
+}
+
+void vjp_kernels(djb_solver* s, int stage, const float* psi, const float* abar, float* psibar, const Shift3& sh,
+                 float scale) {
+    if (s->W == 2) launch_vjp_kernels<2>(s, stage, psi, abar, psibar, sh, scale);
+    else if (s->W == 3) launch_vjp_kernels<3>(s, stage, psi, abar, psibar, sh, scale);
+    else launch_vjp_kernels<4>(s, stage, psi, abar, psibar, sh, scale);
+}
+
+// psibar += (∂acc/∂Ψ)ᵀ abar at the displacements psi (device arrays, Lagrangian order).
+int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
+    if (s->cfg.grad_order == 0 || s->cfg.n_resample > 1)
+        return fail(DJB_ERR_INVALID, "the force VJP covers finite-difference gradients (2/4/6) without resampling");
+    const size_t rho_floats = s->phi[0] ? size_t(s->res) * s->res * s->res : size_t(s->mesh_floats);
+    for (int c = 0; c < 3; ++c)
+        if (!s->adj[c]) TRY(dmalloc(s, (void**)&s->adj[c], rho_floats * sizeof(float)));
+    float* rho = rho_mesh(s, 0);
+    const int pitch = rho_pitch(s);
+    const float inv_ns = 1.0f / float(s->nshift);
+    for (int si = 0; si < s->nshift; ++si) {
+        const GroupShifts g = group_shifts(s, si, 1);
+        const Shift3 sh = g.s[0];
+        CUDA_TRY(cudaMemsetAsync(rho, 0, rho_floats * sizeof(float), s->stream));
+        if (s->W == 2) djb::k_scatter<2, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+        if (s->W == 3) djb::k_scatter<3, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+        if (s->W == 4) djb::k_scatter<4, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+        TRY(poisson(s, 0));  // φ
+        const int cb = grid_for(int64_t(s->res) * s->res * s->res);
+        djb::k_fd_grad3<<<cb, 256, 0, s->stream>>>(rho, s->res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
+                                                    s->adj[2]);
+        vjp_kernels(s, 0, psi, abar, psibar, sh, inv_ns);  // interpolation weights
+        for (int c = 0; c < 3; ++c) CUDA_TRY(cudaMemsetAsync(s->adj[c], 0, rho_floats * sizeof(float), s->stream));
+        vjp_kernels(s, 1, psi, abar, psibar, sh, inv_ns);  // Ḡ
+        djb::k_fd_div3<<<cb, 256, 0, s->stream>>>(s->adj[0], s->adj[1], s->adj[2], s->res, pitch, s->c1, s->c2,
+                                                   s->c3, rho);  // φ̄
+        TRY(poisson(s, 0));                                    // ρ̄
+        vjp_kernels(s, 2, psi, abar, psibar, sh, 1.0f);        // deposit weights
+    }
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
 int check_err(djb_solver* s) {
     int h = 0;
     CUDA_TRY(cudaMemcpyAsync(&h, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
@@ -1569,6 +1656,94 @@ int djb_solver_device_bytes(const djb_solver* s, int64_t* bytes) {
     return DJB_OK;
 }
 
+// Device staging of `count` floats: the caller's device array itself, or a stream-ordered
+// copy of a host array (`copy` = 1) or zero-filled work area (`copy` = 0).
+struct Stage {
+    float* p = nullptr;
+    bool owned = false;
+};
+
+int stage_in(djb_solver* s, Stage& st, const float* src, size_t count, int mem, bool copy) {
+    if (mem == DJB_MEM_DEVICE && src) {
+        st.p = const_cast<float*>(src);
+        return DJB_OK;
+    }
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&st.p), count * sizeof(float), s->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DJB_ERR_ALLOC, "staging allocation failed: %s", cudaGetErrorString(e));
+    }
+    st.owned = true;
+    if (copy && src) return copy_in(s, st.p, src, count, mem);
+    CUDA_TRY(cudaMemsetAsync(st.p, 0, count * sizeof(float), s->stream));
+    return DJB_OK;
+}
+
+void stage_free(djb_solver* s, Stage& st) {
+    if (st.owned && st.p) cudaFreeAsync(st.p, s->stream);
+    st = Stage{};
+}
+
+int djb_pm_acceleration_vjp(djb_solver* s, const float* psi, const float* acc_bar, float* psi_bar, int32_t mem) {
+    djb::clear_error();
+    if (!s || !psi || !acc_bar || !psi_bar) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    Stage sp, sa, sb;
+    int rc = stage_in(s, sp, psi, count, mem, true);
+    if (rc == DJB_OK) rc = stage_in(s, sa, acc_bar, count, mem, true);
+    if (rc == DJB_OK) rc = stage_in(s, sb, mem == DJB_MEM_DEVICE ? nullptr : psi_bar, count, mem, false);
+    float* pb = (mem == DJB_MEM_DEVICE) ? psi_bar : sb.p;
+    if (rc == DJB_OK && mem == DJB_MEM_DEVICE) {
+        cudaError_t e = cudaMemsetAsync(pb, 0, count * sizeof(float), s->stream);
+        if (e != cudaSuccess) rc = fail(DJB_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    }
+    if (rc == DJB_OK) rc = force_vjp(s, sp.p, sa.p, pb);
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = copy_out(s, psi_bar, pb, count, DJB_MEM_HOST);
+    stage_free(s, sp);
+    stage_free(s, sa);
+    stage_free(s, sb);
+    if (rc != DJB_OK) return rc;
+    return check_err(s);
+}
+
+int djb_step_vjp(djb_solver* s, double dd1, double alpha, double beta, double dd2, const float* psi0,
+                 const float* mom0, float* psi_bar, float* mom_bar, int32_t mem) {
+    djb::clear_error();
+    if (!s || !psi0 || !mom0 || !psi_bar || !mom_bar) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    const int64_t m = int64_t(count);
+    Stage sp, sm, sb, smb, s1, sa;
+    int rc = stage_in(s, sp, psi0, count, mem, true);
+    if (rc == DJB_OK) rc = stage_in(s, sm, mom0, count, mem, true);
+    if (rc == DJB_OK) rc = stage_in(s, sb, psi_bar, count, mem, true);
+    if (rc == DJB_OK) rc = stage_in(s, smb, mom_bar, count, mem, true);
+    if (rc == DJB_OK) rc = stage_in(s, s1, nullptr, count, DJB_MEM_HOST, false);
+    if (rc == DJB_OK) rc = stage_in(s, sa, nullptr, count, DJB_MEM_HOST, false);
+    if (rc == DJB_OK) {
+        djb::k_drifted<<<grid_for(m), kThreads, 0, s->stream>>>(sp.p, sm.p, float(dd1), s1.p, m);
+        djb::k_step_vjp_pre<<<grid_for(m), kThreads, 0, s->stream>>>(sb.p, smb.p, float(dd2), float(beta), sa.p, m);
+        rc = force_vjp(s, s1.p, sa.p, sb.p);
+    }
+    if (rc == DJB_OK) {
+        djb::k_step_vjp_post<<<grid_for(m), kThreads, 0, s->stream>>>(sb.p, smb.p, float(alpha), float(dd1), m);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(DJB_ERR_CUDA, "step VJP kernel launch failed");
+    }
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) {
+        rc = copy_out(s, psi_bar, sb.p, count, DJB_MEM_HOST);
+        if (rc == DJB_OK) rc = copy_out(s, mom_bar, smb.p, count, DJB_MEM_HOST);
+    }
+    stage_free(s, sp);
+    stage_free(s, sm);
+    stage_free(s, sb);
+    stage_free(s, smb);
+    stage_free(s, s1);
+    stage_free(s, sa);
+    if (rc != DJB_OK) return rc;
+    return check_err(s);
+}
+
 int djb_pm_acceleration(djb_solver* s, const float* psi, float* acc, int32_t mem) {
     djb::clear_error();
     if (!s || !psi || !acc) return fail(DJB_ERR_INVALID, "null argument");
@@ -1725,6 +1900,16 @@ int djb_synchronize(djb_solver* s) {
 // Exposed to power.cu: the solver's CIC deposit of its state for P(k).
 namespace djb {
 cufftHandle solver_r2c(const djb_solver* s) { return s->r2c; }
+cufftHandle solver_c2r(const djb_solver* s) { return s->c2r; }
+// psibar += Σ_n ∂W_CIC(X − n)/∂X · mesh(n) for the resident state (shift 0); device arrays.
+int solver_cic_gather_grad(djb_solver* s, const float* mesh, int pitch, float* psibar) {
+    djb::k_gather_grad<2><<<blocks(s->np), 256, 0, s->stream>>>(s->psi, s->q1, s->n, s->np, s->Lf, s->res, pitch,
+                                                                 0.0f, 0.0f, 0.0f, mesh, nullptr, nullptr, nullptr,
+                                                                 1.0f, psibar, s->err);
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+int solver_check_err(djb_solver* s) { return check_err(s); }
 double solver_boxsize(const djb_solver* s) { return s->L; }
 int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cudaStream_t* st) {
     if (!s->have_state) return fail(DJB_ERR_STATE, "no particle state set");

@@ -85,6 +85,9 @@ SIGNATURES = {
     "djb_power_spectrum": [_P, _I, _D, _I, _I, _DP, _DP, _I64P, _I, _I],
     "djb_state_power_spectrum": [_P, _I, _I, _DP, _DP, _I64P],
     "djb_power_spectrum_shells_noalloc": [_P, _I, _D, _I, _I, _D, _DP, _DP, _I64P, _P, _I],
+    "djb_pm_acceleration_vjp": [_P, _P, _P, _P, _I],
+    "djb_step_vjp": [_P, _D, _D, _D, _D, _P, _P, _P, _P, _I],
+    "djb_state_power_spectrum_vjp": [_P, _I, _I, _DP, _P, _I],
 }
 _RESTYPES = {"djb_version": C.c_char_p, "djb_last_error": C.c_char_p}
 

@@ -77,6 +77,26 @@ def _ptr_mem(x, n: int):
     return C.c_void_p(h.ctypes.data), MEM_HOST, h
 
 
+def _empty_like_mem(x, n: int, mem: int):
+    if mem == MEM_DEVICE:
+        import torch
+        return torch.empty((3, n, n, n), dtype=torch.float32, device=x.device)
+    return np.empty((n, n, n, 3), dtype=np.float32, order="F")
+
+
+def _copy_mem(x, n: int, mem: int):
+    """A writable copy of a particle array in the C ABI's layout and memory kind."""
+    if mem == MEM_DEVICE:
+        if not _is_torch(x) or not x.is_cuda:
+            raise ValueError("all arrays must live in the same memory")
+        return x.contiguous().clone()
+    return np.array(native_host(x.numpy() if _is_torch(x) else x, n), order="F", copy=True)
+
+
+def _out_ptr(x):
+    return C.c_void_p(x.data_ptr()) if _is_torch(x) else C.c_void_p(x.ctypes.data)
+
+
 class PMSolver:
     """B200 PM workspace (`PMSolver` / `PMSolverLean`, pm.jl:371-414,547-585).
 
@@ -135,6 +155,49 @@ class PMSolver:
             raise ValueError("out must match psi's memory kind and layout")
         check(lib.djb_pm_acceleration(self._h, p, optr, mem))
         del keep
+        return out
+
+    def acceleration_vjp(self, psi, acc_bar):
+        """ψ̄ = (∂acc/∂ψ)ᵀ ā at displacements psi (no reference counterpart). Host arrays
+        give a host (n,n,n,3) array; device (3,n,n,n) tensors give a device tensor."""
+        n = self.n
+        p, mem, k1 = _ptr_mem(psi, n)
+        a, mem2, k2 = _ptr_mem(acc_bar, n)
+        if mem != mem2:
+            raise ValueError("psi and acc_bar must live in the same memory")
+        out = _empty_like_mem(psi, n, mem)
+        check(lib.djb_pm_acceleration_vjp(self._h, p, a, _out_ptr(out), mem))
+        del k1, k2
+        return out
+
+    def step_vjp(self, dd1, alpha, beta, dd2, psi0, mom0, psi_bar, mom_bar):
+        """Cotangents (ψ̄₀, M̄₀) of the state (psi0, mom0) a step started from, given those
+        after the step (psi_bar, mom_bar; not modified)."""
+        n = self.n
+        p, mem, k1 = _ptr_mem(psi0, n)
+        m, _, k2 = _ptr_mem(mom0, n)
+        pb = _copy_mem(psi_bar, n, mem)
+        mb = _copy_mem(mom_bar, n, mem)
+        check(lib.djb_step_vjp(self._h, float(dd1), float(alpha), float(beta), float(dd2), p, m, _out_ptr(pb),
+                               _out_ptr(mb), mem))
+        del k1, k2
+        return pb, mb
+
+    def state_power_spectrum_vjp(self, pk_bar, bins: int = 32, logarithmic: bool = True, device: bool = False):
+        """ψ̄ of Σ_b pk_bar[b]·P_b for P(k) of the resident state (state_power_spectrum)."""
+        n = self.n
+        pb = np.ascontiguousarray(pk_bar, dtype=np.float64)
+        if pb.shape != (bins,):
+            raise ValueError("pk_bar must have one entry per bin")
+        if device:
+            import torch
+            out = torch.empty((3, n, n, n), dtype=torch.float32, device=f"cuda:{self.device}")
+            check(lib.djb_state_power_spectrum_vjp(self._h, int(bins), int(bool(logarithmic)), _lib.dptr(pb),
+                                                   C.c_void_p(out.data_ptr()), MEM_DEVICE))
+            return out
+        out = np.empty((n, n, n, 3), dtype=np.float32, order="F")
+        check(lib.djb_state_power_spectrum_vjp(self._h, int(bins), int(bool(logarithmic)), _lib.dptr(pb),
+                                               C.c_void_p(out.ctypes.data), MEM_HOST))
         return out
 
     def set_state(self, psi, mom, mom_scale: float = 1.0):

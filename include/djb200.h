@@ -184,6 +184,31 @@ DJB_API int djb_power_spectrum(const float* field, int32_t res, double boxsize, 
 DJB_API int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logarithmic, double* k,
                              double* pk, int64_t* nmodes);
 
+/* ── adjoints (vector-Jacobian products) ────────────────────────────────────
+ * No counterpart in the reference, which has no adjoint; these are the transposes
+ * of the forward operators above, checked against finite differences of float64
+ * restatements. They cover finite-difference gradients (grad_order 2/4/6) without
+ * sheet resampling (DJB_ERR_INVALID otherwise). Arrays are (n,n,n,3) Float32 in
+ * the memory `mem` names; the calls wait for the GPU before returning.
+ *
+ * psi_bar = (d acc / d psi)^T acc_bar, acc = djb_pm_acceleration(psi): the
+ * transposes of the interpolation (weight derivatives, pm.jl:344-364), of the FD
+ * gradient (pm.jl:330-342; antisymmetric stencil), of Kphi (pm.jl:389-391; real and
+ * even) and of the mass assignment (pm.jl:57-74), averaged over the shifts like the
+ * force (pm.jl:513-519). */
+DJB_API int djb_pm_acceleration_vjp(djb_solver* s, const float* psi, const float* acc_bar, float* psi_bar,
+                                    int32_t mem);
+/* Adjoint of one djb_step from the state (psi0, mom0) it started from: on entry
+ * psi_bar, mom_bar hold the cotangents of the state after the step, on return
+ * those of (psi0, mom0). The step is Psi1 = Psi0 + dd1*Mom0, Mom1 = alpha*Mom0 +
+ * beta*acc(Psi1), Psi2 = Psi1 + dd2*Mom1 (run_nbody.jl:156-158). */
+DJB_API int djb_step_vjp(djb_solver* s, double ddrift1, double alpha, double beta, double ddrift2,
+                         const float* psi0, const float* mom0, float* psi_bar, float* mom_bar, int32_t mem);
+/* psi_bar = d(sum_b pk_bar[b] * P_b)/d psi for P(k) of the solver's particle state as
+ * djb_state_power_spectrum computes it (same bins); pk_bar: host double[bins]. */
+DJB_API int djb_state_power_spectrum_vjp(djb_solver* s, int32_t bins, int32_t logarithmic, const double* pk_bar,
+                                         float* psi_bar, int32_t mem);
+
 /* ── non-allocating shell sums ──────────────────────────────────────────────
  * No counterpart in the reference. For callers that cannot allocate device
  * memory at the point of the call: code running while a stream is being

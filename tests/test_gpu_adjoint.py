@@ -1,0 +1,140 @@
+"""GPU adjoints (no reference counterpart): the force VJP, the step VJP and the P(k)
+VJP through the C ABI against the float64 restatements of oracle/adjoint.py (which
+test_adjoint_oracle.py pins with finite differences), and the gradient of a P(k) loss
+through a checkpointed run against central finite differences of the float64 oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+COSMO = dict(Omega_c=0.31 - 0.049, Omega_b=0.049, h=0.677, n_s=0.965, sigma8=0.81)
+VJP_TOL = 2e-4  # float32 kernels against float64 sums of the same terms
+
+
+@pytest.fixture(scope="module")
+def djb(cuda_device):
+    import djb200
+    return djb200
+
+
+def _clustered(n, L, seed, amp=3.0):
+    return (amp * np.random.default_rng(seed).standard_normal((n, n, n, 3))).astype(np.float32)
+
+
+@pytest.mark.parametrize("W,g,aa,lap,dec", [(2, 2, 0, 0, False), (3, 4, 1, 4, False), (4, 6, 1, 0, True),
+                                            (4, 4, -1, 2, False), (3, 6, 2, 0, True)])
+def test_force_vjp_vs_oracle(djb, W, g, aa, lap, dec):
+    from oracle import adjoint as oad
+    from oracle import pm as opm
+    n, res, L = 16, 32, 100.0
+    psi = _clustered(n, L, 3 + W)
+    abar = np.random.default_rng(9 + g).standard_normal((n, n, n, 3)).astype(np.float32)
+    cfg = djb.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=W, grad_order=g, antialias=aa, lap_order=lap,
+                       deconvolve=dec)
+    with djb.PMSolver(cfg) as S:
+        gb = S.acceleration_vjp(psi, abar)
+    ocfg = opm.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=W, grad_order=g, antialias=aa, lap_order=lap,
+                        deconvolve=dec)
+    ref = oad.pm_acceleration_vjp(ocfg, psi.astype(np.float64), abar.astype(np.float64))
+    assert rel(gb, ref) < VJP_TOL
+
+
+def test_force_vjp_device_arrays_and_ik_rejected(djb):
+    import torch
+    n, res, L = 16, 32, 100.0
+    psi = _clustered(n, L, 4)
+    abar = np.random.default_rng(2).standard_normal((n, n, n, 3)).astype(np.float32)
+    cfg = djb.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=4, grad_order=4, antialias=1)
+    with djb.PMSolver(cfg) as S:
+        host = S.acceleration_vjp(psi, abar)
+        dev = S.acceleration_vjp(djb.native_view(torch.from_numpy(psi).cuda()),
+                                 djb.native_view(torch.from_numpy(abar).cuda()))
+    assert rel(djb.logical_view(dev).cpu().numpy(), host) < 1e-5  # float atomics reorder only
+    with djb.PMSolver(djb.PMConfig(res_pm=res, n_part=n, boxsize=L, grad_order=0)) as S:
+        with pytest.raises(djb.DJBInvalidOption):
+            S.acceleration_vjp(psi, abar)
+
+
+def test_step_vjp_vs_oracle(djb):
+    from oracle import adjoint as oad
+    from oracle import pm as opm
+    n, res, L = 16, 32, 100.0
+    rng = np.random.default_rng(21)
+    psi0 = _clustered(n, L, 6)
+    mom0 = rng.standard_normal((n, n, n, 3)).astype(np.float32)
+    pbar = rng.standard_normal((n, n, n, 3)).astype(np.float32)
+    mbar = rng.standard_normal((n, n, n, 3)).astype(np.float32)
+    dd1, alpha, beta, dd2 = 0.3, 0.9, 0.7, 0.25
+    cfg = djb.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=4, grad_order=6, antialias=1)
+    with djb.PMSolver(cfg) as S:
+        gp, gm = S.step_vjp(dd1, alpha, beta, dd2, psi0, mom0, pbar, mbar)
+    ocfg = opm.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=4, grad_order=6, antialias=1)
+    p1 = psi0.astype(np.float64) + np.float32(dd1) * mom0.astype(np.float64)
+    mb = mbar.astype(np.float64) + dd2 * pbar.astype(np.float64)
+    pb = pbar.astype(np.float64) + oad.pm_acceleration_vjp(ocfg, p1, beta * mb)
+    mb0 = alpha * mb + dd1 * pb
+    assert rel(gp, pb) < VJP_TOL
+    assert rel(gm, mb0) < VJP_TOL
+
+
+def test_power_spectrum_vjp_vs_oracle(djb):
+    from oracle import adjoint as oad
+    n, res, L, bins = 16, 32, 100.0, 12
+    psi = _clustered(n, L, 8)
+    mom = np.zeros_like(psi)
+    pk_bar = np.random.default_rng(4).standard_normal(bins)
+    with djb.PMSolver(djb.PMConfig(res_pm=res, n_part=n, boxsize=L)) as S:
+        S.set_state(psi, mom)
+        gb = S.state_power_spectrum_vjp(pk_bar, bins=bins)
+    ref = oad.power_spectrum_vjp(res, n, L, psi.astype(np.float64), pk_bar, bins=bins)
+    assert rel(gb, ref) < VJP_TOL
+
+
+def test_pk_loss_gradient_through_a_run_vs_finite_differences(djb):
+    """Adjoint stepper with checkpoints every 5 steps (BullFrog, 7 steps: two segments)
+    against central differences of the same loss through the float64 oracle run."""
+    from oracle import cosmology as cz
+    from oracle import nbody as onb
+    from oracle import pm as opm
+    from oracle import power as opw
+    from djb200 import adjoint as dad
+    from djb200 import ics
+    n, res, L, bins, steps = 16, 32, 200.0, 10, 7
+    cl = djb.Cosmology(**COSMO)
+    co = cz.compute_timetables(cz.Cosmology(**COSMO))
+    psi, pi = ics.lpt_ics(cl, n, L, 0.05, n_order=2, seed=13, device="cpu")
+    psi, pi = psi.numpy().astype(np.float64), pi.numpy().astype(np.float64)
+    kw = dict(boxsize=L, a_ini=0.05, a_end=1.0, n_steps=steps, res_pm=res, stepper="bullfrog", worder=4,
+              grad_kernel_order=4, antialias=1)
+
+    def pk_of(P):
+        mesh = opm.pm_scatter(np.zeros((res, res, res)), onb.add_q(P, L).reshape(-1, 3), res, L, 2)
+        return opw.evaluate_power_spectrum(opw.density_contrast(mesh, n), L, bins=bins)[1]
+
+    P_end, _, _ = onb.run_nbody(co, psi, pi, return_displacement=True, **kw)
+    target = pk_of(P_end) * 0.8
+
+    def loss(p, m):
+        P, _, _ = onb.run_nbody(co, p, m, return_displacement=True, **kw)
+        pk = pk_of(P)
+        ok = (pk > 0) & (target > 0)
+        return float(np.sum((np.log(pk[ok]) - np.log(target[ok])) ** 2))
+
+    lg, gpsi, gpi = dad.pk_loss_and_gradient(cl, psi.astype(np.float32), pi.astype(np.float32), target,
+                                             bins=bins, checkpoint_every=5, grad_kernel_order=4, **{
+                                                 k: v for k, v in kw.items() if k != "grad_kernel_order"})
+    assert abs(lg - loss(psi, pi)) < 1e-3 * abs(lg)
+    rng = np.random.default_rng(3)
+    for grad, which in ((gpsi, 0), (gpi, 1)):
+        v = rng.standard_normal(psi.shape)
+        eps = 1e-4 if which == 0 else 1e-4
+        if which == 0:
+            fd = (loss(psi + eps * v, pi) - loss(psi - eps * v, pi)) / (2 * eps)
+        else:
+            fd = (loss(psi, pi + eps * v) - loss(psi, pi - eps * v)) / (2 * eps)
+        an = float(np.sum(grad.astype(np.float64) * v))
+        assert abs(an - fd) < 2e-2 * abs(fd), (which, an, fd)
