@@ -255,6 +255,7 @@ def main():
     ap.add_argument("--size", default="c3", choices=sorted(SIZES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("warm-up must be >= 3 steps")
@@ -340,6 +341,32 @@ def main():
                    note=f"one run of {args.steps} steps through djb_set_state/djb_run/djb_get_output with "
                         f"pinned host buffers; bytes per step = state in + (X, P) out over the run")
 
+    # adjoint of a step (djb_step_vjp) on the resident final state, device arrays, CUDA
+    # events on the solver's stream: one untimed call, then two timed
+    adjoint = None
+    if not args.no_adjoint:
+        p_s, m_s = S.get_state(device=True)
+        gen = torch.Generator(device=dev).manual_seed(5)
+        pb = torch.randn(p_s.shape, generator=gen, device=dev)
+        mb = torch.randn(p_s.shape, generator=gen, device=dev)
+        k_last = nsteps - 1
+        cargs = (co["ddrift1"][k_last], co["alpha"][k_last], co["beta"][k_last], co["ddrift2"][k_last])
+        S.step_vjp(*cargs, p_s, m_s, pb, mb)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a0.record(stream)
+        for _ in range(2):
+            S.step_vjp(*cargs, p_s, m_s, pb, mb)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ms_vjp = allmax(world, a0.elapsed_time(a1) / 2)
+        adjoint = dict(ms_per_step_vjp=ms_vjp, value=world * Np / (ms_vjp / 1e3), unit=UNIT,
+                       note="djb_step_vjp at the last step's coefficients on the final state: drift, force VJP "
+                            "over both shifts (deposit, Poisson, FD gradient, weight-derivative gathers, "
+                            "cotangent deposit, transposed stencil, Poisson), kick and drift adjoints")
+        del p_s, m_s, pb, mb
+
     # roofline of the dominant kernel of this library (CUDA-event time per launch)
     ab = algorithmic_bytes(n, res)
     peak, peak_kind = measured_peaks()
@@ -370,7 +397,7 @@ def main():
                     ms_per_step=step_ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
                     data="synthetic (seeded white noise -> EH P(k) -> 3LPT)",
                     config=config_block(args.size, n, res, L, lpt, world), roofline=roof,
-                    step_roofline=step_roof, phases=phases, cpu_baseline=cpu, e2e=e2e, clocks=clk,
+                    step_roofline=step_roof, phases=phases, cpu_baseline=cpu, e2e=e2e, adjoint=adjoint, clocks=clk,
                     gpu_launches=int(sum(v[1] for v in prof.values())),
                     device_bytes=S.device_bytes)
         print(json.dumps(line), flush=True)
