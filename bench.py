@@ -126,12 +126,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def measured_peaks():
+def measured_peaks(key="hbm_gbs"):
+    """(peak, "measured" | "fallback") from MEASURED_PEAKS.json: HBM GB/s or bf16 TFLOP/s."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        if key in d:
+            return float(d[key]), "measured"
+    return (6650.0 if key == "hbm_gbs" else 1590.0), "fallback"
 
 
 def profile_traffic():
@@ -246,6 +248,65 @@ def config_block(size, n, res, L, lpt, world):
                 l2="inputs larger than L2 (each mesh exceeds 126 MB); no flush")
 
 
+def nn_flops_per_voxel(layers=4, cin=4, hidden=32, cout=3):
+    """GEMM FLOPs per voxel of one forward pass as executed (channels padded to 8)."""
+    pad = lambda c: (c + 7) // 8 * 8  # noqa: E731
+    f = 0
+    for l in range(layers):
+        ci = cin if l == 0 else hidden
+        co = cout if l == layers - 1 else hidden
+        f += 2 * 27 * pad(ci) * (co if l == layers - 1 else pad(co))
+    return f
+
+
+def nn_timing(dev, stream, world):
+    """Adam steps of the 4-layer, 32-channel network at 128³ and one forward at 512³."""
+    import torch
+
+    from djb200.nn import ForceNet
+    gen = torch.Generator(device=dev).manual_seed(11)
+    out = {}
+    with ForceNet(layers=4, cin=4, hidden=32, cout=3, seed=0) as net:
+        net.set_stream(stream.cuda_stream)
+        x = torch.randn((4, 128, 128, 128), generator=gen, device=dev)
+        t = torch.randn((3, 128, 128, 128), generator=gen, device=dev)
+        for _ in range(2):
+            net.train_step(x, t, lr=1e-4)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(5):
+            net.train_step(x, t, lr=1e-4)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_train = allmax(world, e0.elapsed_time(e1) / 5)
+        del x, t
+        x = torch.randn((4, 512, 512, 512), generator=gen, device=dev)
+        net.apply(x)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        net.apply(x)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_eval = allmax(world, e0.elapsed_time(e1))
+        del x
+    peak, kind = measured_peaks(key="bf16_tflops")
+    f = nn_flops_per_voxel()
+    v128, v512 = 128 ** 3, 512 ** 3
+    train_tflops = 3 * f * v128 / (ms_train / 1e3) / 1e12   # forward + two GEMMs per layer backward
+    eval_tflops = f * v512 / (ms_eval / 1e3) / 1e12
+    out.update(train_ms_per_step=ms_train, train_voxels_per_s=world * v128 / (ms_train / 1e3),
+               eval_ms_512=ms_eval, eval_voxels_per_s=world * v512 / (ms_eval / 1e3),
+               flops_per_voxel_forward=f,
+               roofline=dict(bound="tensor", unit="TFLOP/s", achieved_train=train_tflops,
+                             achieved_eval=eval_tflops, peak=peak, frac_train=train_tflops / peak,
+                             frac_eval=eval_tflops / peak, peak_source=f"{kind} bf16_tflops"),
+               note="4 layers 4->32->32->32->3, 3^3 kernels, periodic; bf16 GEMMs (im2col + cuBLAS), "
+                    "float32 accumulation; train = forward + backward + Adam at 128^3 (FLOPs counted as 3x "
+                    "forward); eval = one forward at 512^3 in 4 Mi-voxel chunks")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -256,6 +317,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-nn", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("warm-up must be >= 3 steps")
@@ -367,6 +429,12 @@ def main():
                             "cotangent deposit, transposed stencil, Poisson), kick and drift adjoints")
         del p_s, m_s, pb, mb
 
+    # force-correction network: Adam steps at 128³ and one application at 512³ (random
+    # inputs of the network's shape; the timing does not depend on the values)
+    nn = None
+    if not args.no_nn:
+        nn = nn_timing(dev, stream, world)
+
     # roofline of the dominant kernel of this library (CUDA-event time per launch)
     ab = algorithmic_bytes(n, res)
     peak, peak_kind = measured_peaks()
@@ -397,7 +465,8 @@ def main():
                     ms_per_step=step_ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
                     data="synthetic (seeded white noise -> EH P(k) -> 3LPT)",
                     config=config_block(args.size, n, res, L, lpt, world), roofline=roof,
-                    step_roofline=step_roof, phases=phases, cpu_baseline=cpu, e2e=e2e, adjoint=adjoint, clocks=clk,
+                    step_roofline=step_roof, phases=phases, cpu_baseline=cpu, e2e=e2e, adjoint=adjoint, nn=nn,
+                    clocks=clk,
                     gpu_launches=int(sum(v[1] for v in prof.values())),
                     device_bytes=S.device_bytes)
         print(json.dumps(line), flush=True)

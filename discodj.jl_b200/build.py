@@ -4,7 +4,7 @@
 
 Compiles `csrc/*.cu` and `csrc/*.cpp` with `-gencode arch=compute_100a,code=sm_100a
 -lineinfo -O3` into `discodj.jl_b200/lib/libdjb200.so`, linked against the
-CUDA toolkit's cuFFT (rpath to the toolkit's lib64). Rebuilds only when a source
+CUDA toolkit's cuFFT and cuBLAS (rpath to the toolkit's lib64). Rebuilds only when a source
 or header is newer than the library unless --force is given.
 """
 from __future__ import annotations
@@ -45,7 +45,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-Xptxas", "-warn-spills",
            f"-I{INCLUDE}", f"-I{CSRC}", *sources(), "-o", LIB + ".tmp",
-           f"-L{CUDA_HOME}/lib64", "-lcufft", f"-Xlinker", f"-rpath,{CUDA_HOME}/lib64"]
+           f"-L{CUDA_HOME}/lib64", "-lcufft", "-lcublas", f"-Xlinker", f"-rpath,{CUDA_HOME}/lib64"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -215,4 +215,16 @@ __global__ void k_step_vjp_post(const float* __restrict__ psibar, float* __restr
         mombar[t] = alpha * mombar[t] + dd1 * psibar[t];
 }
 
+// out = scale·in − offset on the res³ cells of a pitched mesh, written densely.
+__global__ void k_mesh_affine(const float* __restrict__ in, int res, int pitch, float scale, float offset,
+                              float* __restrict__ out) {
+    const int64_t total = int64_t(res) * res * res;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t row = t / res;
+        const int x = int(t - row * res);
+        out[t] = scale * in[row * pitch + x] - offset;
+    }
+}
+
 }  // namespace djb

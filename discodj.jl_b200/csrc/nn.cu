@@ -1,0 +1,591 @@
+// Force-correction network: a 3-D CNN on the PM mesh (no counterpart in the reference).
+//
+// Layers: L convolutions with 3³ kernels and periodic boundaries (the box is periodic),
+// cin → hidden → … → hidden → cout channels, ReLU after every layer but the last.
+// Inputs and outputs cross the C ABI as float32 meshes in the solver's layout,
+// [channel][z][y][x]; inside, activations are bf16 channels-last, [voxel][channel].
+//
+// Each convolution is an implicit GEMM made explicit per chunk of z planes:
+//   col[v][tap·C + c] = X[v + offset(tap)][c]        k_im2col (bf16, periodic wrap)
+//   Y = col · W  (M = voxels, K = 27·C, N = channels out; bf16 operands, float32
+//                 accumulation on the tensor cores through cuBLAS)
+//   X' = relu(Y + b) → bf16                           k_bias_act
+// Backward, per layer from the last: dY (ReLU mask applied), dW = colᵀ·dY and
+// dcol = dY·Wᵀ (cuBLAS), db = Σ_v dY, dX[v] = Σ_tap dcol[v − offset(tap)][tap]
+// (k_col2im, a gather: no atomics). Loss: mean squared error over all outputs.
+// Optimizer: Adam on float32 master weights, then the bf16 copies the GEMMs read.
+// Channel counts are padded to multiples of 8 (16-byte rows for the tensor cores);
+// the padding channels hold zeros and their weights stay zero.
+#include <cublas_v2.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <new>
+#include <random>
+#include <vector>
+
+#include "common.h"
+#include "djb200.h"
+
+using djb::fail;
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(DJB_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));      \
+    } while (0)
+
+#define CUBLAS_TRY(expr)                                                                        \
+    do {                                                                                        \
+        cublasStatus_t st_ = (expr);                                                            \
+        if (st_ != CUBLAS_STATUS_SUCCESS) return fail(DJB_ERR_CUDA, "%s failed (cuBLAS %d)", #expr, int(st_)); \
+    } while (0)
+
+namespace {
+
+constexpr int kMaxLayers = 8;
+constexpr int kNT = 256;
+
+__host__ __device__ inline int pad8(int c) { return (c + 7) & ~7; }
+
+// voxel index of (x, y, z) + (dx, dy, dz) on the periodic res³ mesh, v = (z·res + y)·res + x
+__device__ __forceinline__ int64_t nbr(int x, int y, int z, int dx, int dy, int dz, int res) {
+    x += dx;
+    y += dy;
+    z += dz;
+    x = x < 0 ? x + res : (x >= res ? x - res : x);
+    y = y < 0 ? y + res : (y >= res ? y - res : y);
+    z = z < 0 ? z + res : (z >= res ? z - res : z);
+    return (int64_t(z) * res + y) * res + x;
+}
+
+// float32 [c][z][y][x] (c < cin) → bf16 [v][cp] (zeros beyond cin), for voxels [v0, v0 + m).
+__global__ void k_pack(const float* __restrict__ in, int cin, int cp, int64_t nvox, int64_t v0, int64_t m,
+                       __nv_bfloat16* __restrict__ out) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m * cp; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / cp;
+        const int c = int(t - v * cp);
+        out[t] = __float2bfloat16_rn(c < cin ? in[int64_t(c) * nvox + v0 + v] : 0.0f);
+    }
+}
+
+// col[v][tap·C + c] for the m voxels starting at v0 (C a multiple of 8: 16-byte copies).
+__global__ void k_im2col(const __nv_bfloat16* __restrict__ X, int res, int C, int64_t v0, int64_t m,
+                         __nv_bfloat16* __restrict__ col) {
+    const int groups = C / 8;
+    const int64_t total = m * 27 * groups;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int g = int(t % groups);
+        const int64_t r = t / groups;
+        const int tap = int(r % 27);
+        const int64_t vl = r / 27;
+        const int64_t v = v0 + vl;
+        const int x = int(v % res), y = int((v / res) % res), z = int(v / (int64_t(res) * res));
+        const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+        const int64_t src = nbr(x, y, z, dx, dy, dz, res);
+        reinterpret_cast<uint4*>(col + (vl * 27 + tap) * C)[g] = reinterpret_cast<const uint4*>(X + src * C)[g];
+    }
+}
+
+// out[v][c] = act(Y[v][c] + b[c]) for c < n, zero for n <= c < np (bf16); `relu` or identity.
+__global__ void k_bias_act(const float* __restrict__ Y, int n, const float* __restrict__ b, int np, int relu,
+                           int64_t m, __nv_bfloat16* __restrict__ out) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m * np; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / np;
+        const int c = int(t - v * np);
+        float y = 0.0f;
+        if (c < n) {
+            y = Y[v * n + c] + b[c];
+            if (relu) y = fmaxf(y, 0.0f);
+        }
+        out[t] = __float2bfloat16_rn(y);
+    }
+}
+
+// last layer: out = Y + b (float32 [v][n]) for voxels [v0, v0 + m) → channel-major mesh
+__global__ void k_bias_out(const float* __restrict__ Y, int n, const float* __restrict__ b, int64_t nvox, int64_t v0,
+                           int64_t m, float* __restrict__ out) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m * n; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / n;
+        const int c = int(t - v * n);
+        out[int64_t(c) * nvox + v0 + v] = Y[t] + b[c];
+    }
+}
+
+// dY[v][c] = 2 (out − target) / count and Σ (out − target)² into *sum (double).
+__global__ void k_mse(const float* __restrict__ out, const float* __restrict__ target, int n, int64_t nvox,
+                      double inv_count, float* __restrict__ dY, double* __restrict__ sum) {
+    __shared__ double part[kNT];
+    double acc = 0.0;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nvox * n; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / n;
+        const int c = int(t - v * n);
+        const float d = out[int64_t(c) * nvox + v] - target[int64_t(c) * nvox + v];
+        acc += double(d) * d;
+        dY[t] = float(2.0 * inv_count) * d;
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(sum, part[0]);
+}
+
+// float32 [v][n] → bf16 [v][np] (zeros beyond n), optionally masked by A > 0 (ReLU backward).
+__global__ void k_grad_bf16(const float* __restrict__ dA, int n, int np, const __nv_bfloat16* __restrict__ A,
+                            int64_t m, __nv_bfloat16* __restrict__ dY) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m * np; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / np;
+        const int c = int(t - v * np);
+        float g = 0.0f;
+        if (c < n) {
+            g = dA[v * n + c];
+            if (A && !(__bfloat162float(A[t]) > 0.0f)) g = 0.0f;
+        }
+        dY[t] = __float2bfloat16_rn(g);
+    }
+}
+
+// db[c] += Σ_v dY[v][c] (bf16 [v][np], c < n)
+__global__ void k_bias_grad(const __nv_bfloat16* __restrict__ dY, int n, int np, int64_t m, float* __restrict__ db) {
+    for (int c = 0; c < n; ++c) {
+        float acc = 0.0f;
+        for (int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < m; v += int64_t(gridDim.x) * blockDim.x)
+            acc += __bfloat162float(dY[v * np + c]);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(db + c, acc);
+    }
+}
+
+// dX[v][c] = Σ_tap dcol[v − offset(tap)][tap][c] over all voxels (float32, C channels)
+__global__ void k_col2im(const float* __restrict__ dcol, int res, int C, int64_t nvox, float* __restrict__ dX) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nvox * C; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / C;
+        const int c = int(t - v * C);
+        const int x = int(v % res), y = int((v / res) % res), z = int(v / (int64_t(res) * res));
+        float acc = 0.0f;
+#pragma unroll
+        for (int tap = 0; tap < 27; ++tap) {
+            const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+            const int64_t src = nbr(x, y, z, -dx, -dy, -dz, res);
+            acc += dcol[(src * 27 + tap) * C + c];
+        }
+        dX[t] = acc;
+    }
+}
+
+// Adam (float32 master weights) and the bf16 copy of the weights.
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
+                       float* __restrict__ m2, int64_t count, float lr, float b1, float b2, float eps, float c1,
+                       float c2, const uint8_t* __restrict__ frozen, __nv_bfloat16* __restrict__ pb) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < count; t += int64_t(gridDim.x) * blockDim.x) {
+        if (frozen && frozen[t]) continue;
+        const float gi = g[t];
+        const float a = b1 * m1[t] + (1.0f - b1) * gi;
+        const float b = b2 * m2[t] + (1.0f - b2) * gi * gi;
+        m1[t] = a;
+        m2[t] = b;
+        const float mh = a / c1, vh = b / c2;
+        p[t] -= lr * mh / (sqrtf(vh) + eps);
+        if (pb) pb[t] = __float2bfloat16_rn(p[t]);
+    }
+}
+
+__global__ void k_to_bf16(const float* __restrict__ a, int64_t count, __nv_bfloat16* __restrict__ b) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < count; t += int64_t(gridDim.x) * blockDim.x)
+        b[t] = __float2bfloat16_rn(a[t]);
+}
+
+int grid_of(int64_t count) { return int(std::min<int64_t>((count + kNT - 1) / kNT, 148LL * 32)); }
+
+}  // namespace
+
+struct djb_nn {
+    int layers = 0;
+    int cin[kMaxLayers] = {}, cout[kMaxLayers] = {};   // real channel counts per layer
+    int cinp[kMaxLayers] = {}, coutp[kMaxLayers] = {};  // padded to 8
+    int64_t woff[kMaxLayers] = {}, boff[kMaxLayers] = {};
+    int64_t nparam = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr, own = nullptr;
+    cublasHandle_t blas = nullptr;
+    // parameters: float32 master, bf16 copy, Adam moments, gradients, frozen mask (padding)
+    float* p = nullptr;
+    __nv_bfloat16* pb = nullptr;
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    float* g = nullptr;
+    uint8_t* frozen = nullptr;
+    int64_t step = 0;
+    // work areas for a mesh of `res`³ voxels processed in chunks of `chunk` voxels
+    int res = 0;
+    int64_t chunk = 0;
+    __nv_bfloat16* act[kMaxLayers + 1] = {};  // [v][cinp] per layer input (act[L] unused)
+    __nv_bfloat16* col = nullptr;              // [chunk][27·Cmax]
+    float* Y = nullptr;                        // [chunk][Nmax] (also dA)
+    float* dcol = nullptr;                     // [nvox][27·Cmax] (training only)
+    float* dA = nullptr;                       // [nvox][Cmax]
+    __nv_bfloat16* dY = nullptr;               // [nvox][Cmax]
+    float* outm = nullptr;                     // [cout][nvox] float32
+    double* lsum = nullptr;
+    std::vector<void*> work;
+};
+
+namespace {
+
+int dalloc(djb_nn* h, void** p, size_t bytes, bool work) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DJB_ERR_ALLOC, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    if (work) h->work.push_back(*p);
+    return DJB_OK;
+}
+
+#define TRYN(expr)                  \
+    do {                            \
+        int rc_ = (expr);           \
+        if (rc_ != DJB_OK) return rc_; \
+    } while (0)
+
+void free_work(djb_nn* h) {
+    for (void* q : h->work) cudaFree(q);
+    h->work.clear();
+    for (auto& a : h->act) a = nullptr;
+    h->col = nullptr;
+    h->Y = nullptr;
+    h->dcol = nullptr;
+    h->dA = nullptr;
+    h->dY = nullptr;
+    h->outm = nullptr;
+    h->res = 0;
+}
+
+int cmax(const djb_nn* h) {
+    int c = 8;
+    for (int l = 0; l < h->layers; ++l) c = std::max({c, h->cinp[l], h->coutp[l]});
+    return c;
+}
+
+// Work areas for res³ voxels; training needs the whole mesh at once (chunk = nvox).
+int ensure_work(djb_nn* h, int res, bool train) {
+    const int64_t nvox = int64_t(res) * res * res;
+    const bool need_train = train && !h->dcol;
+    if (h->res == res && !need_train) return DJB_OK;
+    free_work(h);
+    const int C = cmax(h);
+    // chunks of whole z planes holding at most 4 Mi voxels (col: 27·C bf16 per voxel,
+    // 7 GB for C = 32)
+    int64_t planes = std::max<int64_t>(1, (int64_t(1) << 22) / (int64_t(res) * res));
+    planes = std::min<int64_t>(planes, res);
+    h->chunk = train ? nvox : planes * res * res;
+    for (int l = 0; l < h->layers; ++l)
+        TRYN(dalloc(h, (void**)&h->act[l], size_t(nvox) * h->cinp[l] * sizeof(__nv_bfloat16), true));
+    TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
+    TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
+    TRYN(dalloc(h, (void**)&h->outm, size_t(nvox) * h->cout[h->layers - 1] * sizeof(float), true));
+    TRYN(dalloc(h, (void**)&h->lsum, sizeof(double), true));
+    if (train) {
+        TRYN(dalloc(h, (void**)&h->dcol, size_t(nvox) * 27 * C * sizeof(float), true));
+        TRYN(dalloc(h, (void**)&h->dA, size_t(nvox) * C * sizeof(float), true));
+        TRYN(dalloc(h, (void**)&h->dY, size_t(nvox) * C * sizeof(__nv_bfloat16), true));
+    }
+    h->res = res;
+    return DJB_OK;
+}
+
+// Forward over all voxels: input (float32 mesh, device) → h->outm (float32 mesh).
+int forward(djb_nn* h, const float* in) {
+    const int res = h->res;
+    const int64_t nvox = int64_t(res) * res * res;
+    const float one = 1.0f, zero = 0.0f;
+    k_pack<<<grid_of(nvox * h->cinp[0]), kNT, 0, h->stream>>>(in, h->cin[0], h->cinp[0], nvox, 0, nvox, h->act[0]);
+    for (int l = 0; l < h->layers; ++l) {
+        const int C = h->cinp[l], K = 27 * C;
+        const bool last = (l == h->layers - 1);
+        const int N = last ? h->cout[l] : h->coutp[l];
+        for (int64_t v0 = 0; v0 < nvox; v0 += h->chunk) {
+            const int64_t m = std::min(h->chunk, nvox - v0);
+            k_im2col<<<grid_of(m * 27 * (C / 8)), kNT, 0, h->stream>>>(h->act[l], res, C, v0, m, h->col);
+            // Yᶜ (N×m) = Wᶜ (N×K) · colᶜ (K×m); W row-major [K][coutp]
+            CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, N, int(m), K, &one, h->pb + h->woff[l],
+                                    CUDA_R_16BF, h->coutp[l], h->col, CUDA_R_16BF, K, &zero, h->Y, CUDA_R_32F, N,
+                                    CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
+            if (last)
+                k_bias_out<<<grid_of(m * N), kNT, 0, h->stream>>>(h->Y, N, h->p + h->boff[l], nvox, v0, m, h->outm);
+            else
+                k_bias_act<<<grid_of(m * h->cinp[l + 1]), kNT, 0, h->stream>>>(
+                    h->Y, N, h->p + h->boff[l], h->cinp[l + 1], 1, m, h->act[l + 1] + v0 * h->cinp[l + 1]);
+        }
+    }
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+// Backward from the MSE loss against `target` (float32 mesh, device) into h->g; *loss.
+int backward(djb_nn* h, const float* target, double* loss) {
+    const int res = h->res;
+    const int64_t nvox = int64_t(res) * res * res;
+    const float one = 1.0f, zero = 0.0f;
+    const int L = h->layers;
+    const int nout = h->cout[L - 1];
+    CUDA_TRY(cudaMemsetAsync(h->g, 0, size_t(h->nparam) * sizeof(float), h->stream));
+    CUDA_TRY(cudaMemsetAsync(h->lsum, 0, sizeof(double), h->stream));
+    k_mse<<<grid_of(nvox * nout), kNT, 0, h->stream>>>(h->outm, target, nout, nvox, 1.0 / double(nvox * nout), h->dA,
+                                                      h->lsum);
+    for (int l = L - 1; l >= 0; --l) {
+        const int C = h->cinp[l], K = 27 * C;
+        const int N = h->coutp[l];
+        const int n = (l == L - 1) ? nout : h->cout[l];
+        // dY (bf16, [v][N]); the ReLU mask of this layer's output
+        const __nv_bfloat16* A = (l == L - 1) ? nullptr : h->act[l + 1];
+        k_grad_bf16<<<grid_of(nvox * N), kNT, 0, h->stream>>>(h->dA, (l == L - 1) ? nout : N, N, A, nvox, h->dY);
+        k_bias_grad<<<grid_of(nvox), kNT, 0, h->stream>>>(h->dY, n, N, nvox, h->g + h->boff[l]);
+        k_im2col<<<grid_of(nvox * 27 * (C / 8)), kNT, 0, h->stream>>>(h->act[l], res, C, 0, nvox, h->col);
+        // dWᶜ (N×K) = dYᶜ (N×M) · colᶜᵀ (M×K)
+        CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, N, K, int(nvox), &one, h->dY, CUDA_R_16BF, N,
+                                h->col, CUDA_R_16BF, K, &zero, h->g + h->woff[l], CUDA_R_32F, N, CUBLAS_COMPUTE_32F,
+                                CUBLAS_GEMM_DEFAULT));
+        if (l > 0) {
+            // dcolᶜ (K×M) = Wᶜᵀ (K×N) · dYᶜ (N×M)
+            CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, K, int(nvox), N, &one, h->pb + h->woff[l],
+                                    CUDA_R_16BF, N, h->dY, CUDA_R_16BF, N, &zero, h->dcol, CUDA_R_32F, K,
+                                    CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
+            k_col2im<<<grid_of(nvox * C), kNT, 0, h->stream>>>(h->dcol, res, C, nvox, h->dA);
+        }
+    }
+    if (loss) {
+        double s = 0.0;
+        CUDA_TRY(cudaMemcpyAsync(&s, h->lsum, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        *loss = s / double(nvox * nout);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+// Stages a float32 mesh of `count` floats to the device (host memory) or uses it in place.
+int stage(djb_nn* h, const float* src, size_t count, int mem, float** out, bool* owned) {
+    *owned = false;
+    if (mem == DJB_MEM_DEVICE) {
+        *out = const_cast<float*>(src);
+        return DJB_OK;
+    }
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(out), count * sizeof(float), h->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DJB_ERR_ALLOC, "staging allocation failed: %s", cudaGetErrorString(e));
+    }
+    *owned = true;
+    CUDA_TRY(cudaMemcpyAsync(*out, src, count * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    return DJB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int djb_nn_create(int32_t layers, int32_t cin, int32_t hidden, int32_t cout, uint64_t seed, int32_t device,
+                  djb_nn** out) {
+    djb::clear_error();
+    if (!out) return fail(DJB_ERR_INVALID, "null argument");
+    if (layers < 2 || layers > kMaxLayers || cin < 1 || hidden < 1 || cout < 1 || hidden > 256 || cin > 256 ||
+        cout > 256)
+        return fail(DJB_ERR_INVALID, "layers must be in 2..%d and channel counts in 1..256", kMaxLayers);
+    CUDA_TRY(cudaSetDevice(device));
+    djb_nn* h = new (std::nothrow) djb_nn();
+    if (!h) return fail(DJB_ERR_ALLOC, "host allocation failed");
+    *out = h;
+    h->layers = layers;
+    h->device = device;
+    int64_t off = 0;
+    for (int l = 0; l < layers; ++l) {
+        h->cin[l] = (l == 0) ? cin : hidden;
+        h->cout[l] = (l == layers - 1) ? cout : hidden;
+        h->cinp[l] = pad8(h->cin[l]);
+        h->coutp[l] = pad8(h->cout[l]);
+        h->woff[l] = off;
+        off += int64_t(27) * h->cinp[l] * h->coutp[l];
+        h->boff[l] = off;
+        off += h->coutp[l];
+    }
+    h->nparam = off;
+    // Kaiming-uniform weights (bound sqrt(6 / fan_in)), zero biases; padding frozen at 0
+    std::vector<float> p(size_t(off), 0.0f);
+    std::vector<uint8_t> fr(size_t(off), 1);
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l < layers; ++l) {
+        const double bound = std::sqrt(6.0 / (27.0 * h->cin[l]));
+        std::uniform_real_distribution<double> U(-bound, bound);
+        for (int tap = 0; tap < 27; ++tap)
+            for (int c = 0; c < h->cin[l]; ++c)
+                for (int o = 0; o < h->cout[l]; ++o) {
+                    const int64_t i = h->woff[l] + (int64_t(tap) * h->cinp[l] + c) * h->coutp[l] + o;
+                    p[size_t(i)] = float(U(rng));
+                    fr[size_t(i)] = 0;
+                }
+        for (int o = 0; o < h->cout[l]; ++o) fr[size_t(h->boff[l] + o)] = 0;
+    }
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+    h->stream = h->own;
+    CUBLAS_TRY(cublasCreate(&h->blas));
+    CUBLAS_TRY(cublasSetStream(h->blas, h->stream));
+    CUBLAS_TRY(cublasSetMathMode(h->blas, CUBLAS_DEFAULT_MATH));
+    TRYN(dalloc(h, (void**)&h->p, size_t(off) * sizeof(float), false));
+    TRYN(dalloc(h, (void**)&h->pb, size_t(off) * sizeof(__nv_bfloat16), false));
+    TRYN(dalloc(h, (void**)&h->m1, size_t(off) * sizeof(float), false));
+    TRYN(dalloc(h, (void**)&h->m2, size_t(off) * sizeof(float), false));
+    TRYN(dalloc(h, (void**)&h->g, size_t(off) * sizeof(float), false));
+    TRYN(dalloc(h, (void**)&h->frozen, size_t(off), false));
+    CUDA_TRY(cudaMemcpy(h->p, p.data(), size_t(off) * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->frozen, fr.data(), size_t(off), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(h->m1, 0, size_t(off) * sizeof(float)));
+    CUDA_TRY(cudaMemset(h->m2, 0, size_t(off) * sizeof(float)));
+    k_to_bf16<<<grid_of(off), kNT>>>(h->p, off, h->pb);
+    CUDA_TRY(cudaDeviceSynchronize());
+    return DJB_OK;
+}
+
+int djb_nn_destroy(djb_nn* h) {
+    if (!h) return DJB_OK;
+    cudaSetDevice(h->device);
+    free_work(h);
+    for (void* q : {(void*)h->p, (void*)h->pb, (void*)h->m1, (void*)h->m2, (void*)h->g, (void*)h->frozen})
+        if (q) cudaFree(q);
+    if (h->blas) cublasDestroy(h->blas);
+    if (h->own) cudaStreamDestroy(h->own);
+    delete h;
+    return DJB_OK;
+}
+
+int djb_nn_param_count(const djb_nn* h, int64_t* count) {
+    djb::clear_error();
+    if (!h || !count) return fail(DJB_ERR_INVALID, "null argument");
+    *count = h->nparam;
+    return DJB_OK;
+}
+
+int djb_nn_get_params(djb_nn* h, float* params) {
+    djb::clear_error();
+    if (!h || !params) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaMemcpyAsync(params, h->p, size_t(h->nparam) * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DJB_OK;
+}
+
+int djb_nn_load(djb_nn* h, const float* params) {
+    djb::clear_error();
+    if (!h || !params) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaMemcpyAsync(h->p, params, size_t(h->nparam) * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemsetAsync(h->m1, 0, size_t(h->nparam) * sizeof(float), h->stream));
+    CUDA_TRY(cudaMemsetAsync(h->m2, 0, size_t(h->nparam) * sizeof(float), h->stream));
+    k_to_bf16<<<grid_of(h->nparam), kNT, 0, h->stream>>>(h->p, h->nparam, h->pb);
+    h->step = 0;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DJB_OK;
+}
+
+int djb_nn_set_stream(djb_nn* h, void* stream) {
+    djb::clear_error();
+    if (!h) return fail(DJB_ERR_INVALID, "null argument");
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own;
+    CUBLAS_TRY(cublasSetStream(h->blas, h->stream));
+    return DJB_OK;
+}
+
+int djb_nn_apply(djb_nn* h, const float* in, int32_t res, float* out, int32_t mem) {
+    djb::clear_error();
+    if (!h || !in || !out) return fail(DJB_ERR_INVALID, "null argument");
+    if (res < 3) return fail(DJB_ERR_INVALID, "res must be >= 3");
+    CUDA_TRY(cudaSetDevice(h->device));
+    TRYN(ensure_work(h, res, false));
+    const int64_t nvox = int64_t(res) * res * res;
+    float* din = nullptr;
+    bool own_in = false;
+    TRYN(stage(h, in, size_t(nvox) * h->cin[0], mem, &din, &own_in));
+    int rc = forward(h, din);
+    const size_t nout = size_t(nvox) * h->cout[h->layers - 1];
+    if (rc == DJB_OK && cudaMemcpyAsync(out, h->outm, nout * sizeof(float),
+                                        mem == DJB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                        h->stream) != cudaSuccess)
+        rc = fail(DJB_ERR_CUDA, "output copy failed");
+    if (own_in) cudaFreeAsync(din, h->stream);
+    if (rc != DJB_OK) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DJB_OK;
+}
+
+// Gradients of the mean squared error of net(in) against target, into the network's
+// gradient buffer (read with djb_nn_grads, replaced with djb_nn_set_grads).
+int djb_nn_backward(djb_nn* h, const float* in, const float* target, int32_t res, double* loss, int32_t mem) {
+    djb::clear_error();
+    if (!h || !in || !target) return fail(DJB_ERR_INVALID, "null argument");
+    if (res < 3) return fail(DJB_ERR_INVALID, "res must be >= 3");
+    CUDA_TRY(cudaSetDevice(h->device));
+    TRYN(ensure_work(h, res, true));
+    const int64_t nvox = int64_t(res) * res * res;
+    float *din = nullptr, *dt = nullptr;
+    bool own_in = false, own_t = false;
+    TRYN(stage(h, in, size_t(nvox) * h->cin[0], mem, &din, &own_in));
+    int rc = stage(h, target, size_t(nvox) * h->cout[h->layers - 1], mem, &dt, &own_t);
+    if (rc == DJB_OK) rc = forward(h, din);
+    if (rc == DJB_OK) rc = backward(h, dt, loss);
+    if (own_in) cudaFreeAsync(din, h->stream);
+    if (own_t) cudaFreeAsync(dt, h->stream);
+    if (rc != DJB_OK) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DJB_OK;
+}
+
+int djb_nn_grads(djb_nn* h, float* grads, int32_t mem) {
+    djb::clear_error();
+    if (!h || !grads) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaMemcpyAsync(grads, h->g, size_t(h->nparam) * sizeof(float),
+                             mem == DJB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DJB_OK;
+}
+
+int djb_nn_set_grads(djb_nn* h, const float* grads, int32_t mem) {
+    djb::clear_error();
+    if (!h || !grads) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaMemcpyAsync(h->g, grads, size_t(h->nparam) * sizeof(float),
+                             mem == DJB_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DJB_OK;
+}
+
+// One Adam step (beta 0.9/0.999, eps 1e-8) with the gradients in the gradient buffer.
+int djb_nn_adam_step(djb_nn* h, double lr) {
+    djb::clear_error();
+    if (!h) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    ++h->step;
+    const float c1 = float(1.0 - std::pow(0.9, double(h->step)));
+    const float c2 = float(1.0 - std::pow(0.999, double(h->step)));
+    k_adam<<<grid_of(h->nparam), kNT, 0, h->stream>>>(h->p, h->g, h->m1, h->m2, h->nparam, float(lr), 0.9f, 0.999f,
+                                                       1e-8f, c1, c2, h->frozen, h->pb);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DJB_OK;
+}
+
+int djb_nn_train_step(djb_nn* h, const float* in, const float* target, int32_t res, double lr, double* loss,
+                      int32_t mem) {
+    TRYN(djb_nn_backward(h, in, target, res, loss, mem));
+    return djb_nn_adam_step(h, lr);
+}
+
+}  // extern "C"

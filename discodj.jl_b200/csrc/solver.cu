@@ -1744,6 +1744,52 @@ int djb_step_vjp(djb_solver* s, double dd1, double alpha, double beta, double dd
     return check_err(s);
 }
 
+int djb_mesh_fields(djb_solver* s, const float* psi, float* out, int32_t mem) {
+    djb::clear_error();
+    if (!s || !psi || !out) return fail(DJB_ERR_INVALID, "null argument");
+    if (s->cfg.grad_order == 0 || s->cfg.n_resample > 1)
+        return fail(DJB_ERR_INVALID, "mesh fields need a finite-difference gradient (2/4/6) without resampling");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    const int res = s->res;
+    const int64_t cells = int64_t(res) * res * res;
+    const size_t rho_floats = s->phi[0] ? size_t(cells) : size_t(s->mesh_floats);
+    for (int c = 0; c < 3; ++c)
+        if (!s->adj[c]) TRY(dmalloc(s, (void**)&s->adj[c], rho_floats * sizeof(float)));
+    Stage sp, so;
+    int rc = stage_in(s, sp, psi, count, mem, true);
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = stage_in(s, so, nullptr, size_t(4 * cells), DJB_MEM_HOST, false);
+    float* o = (mem == DJB_MEM_HOST) ? so.p : out;
+    if (rc == DJB_OK) {
+        float* rho = rho_mesh(s, 0);
+        const int pitch = rho_pitch(s);
+        GroupShifts g{};
+        CUDA_TRY(cudaMemsetAsync(rho, 0, rho_floats * sizeof(float), s->stream));
+        if (s->W == 2) djb::k_scatter<2, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+            sp.p, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, res, pitch, g, rho, nullptr, s->err);
+        if (s->W == 3) djb::k_scatter<3, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+            sp.p, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, res, pitch, g, rho, nullptr, s->err);
+        if (s->W == 4) djb::k_scatter<4, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+            sp.p, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, res, pitch, g, rho, nullptr, s->err);
+        const int cb = grid_for(cells);
+        const float f = float(double(cells) / double(s->np));
+        djb::k_mesh_affine<<<cb, 256, 0, s->stream>>>(rho, res, pitch, f, 1.0f, o);  // δ
+        rc = poisson(s, 0);
+        if (rc == DJB_OK) {
+            djb::k_fd_grad3<<<cb, 256, 0, s->stream>>>(rho, res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
+                                                        s->adj[2]);
+            for (int c = 0; c < 3; ++c)
+                djb::k_mesh_affine<<<cb, 256, 0, s->stream>>>(s->adj[c], res, pitch, 1.0f, 0.0f, o + (c + 1) * cells);
+            if (cudaGetLastError() != cudaSuccess) rc = fail(DJB_ERR_CUDA, "mesh field kernels failed");
+        }
+    }
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = copy_out(s, out, o, size_t(4 * cells), DJB_MEM_HOST);
+    stage_free(s, sp);
+    stage_free(s, so);
+    if (rc != DJB_OK) return rc;
+    return check_err(s);
+}
+
 int djb_pm_acceleration(djb_solver* s, const float* psi, float* acc, int32_t mem) {
     djb::clear_error();
     if (!s || !psi || !acc) return fail(DJB_ERR_INVALID, "null argument");

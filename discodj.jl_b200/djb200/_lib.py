@@ -88,6 +88,19 @@ SIGNATURES = {
     "djb_pm_acceleration_vjp": [_P, _P, _P, _P, _I],
     "djb_step_vjp": [_P, _D, _D, _D, _D, _P, _P, _P, _P, _I],
     "djb_state_power_spectrum_vjp": [_P, _I, _I, _DP, _P, _I],
+    "djb_mesh_fields": [_P, _P, _P, _I],
+    "djb_nn_create": [_I, _I, _I, _I, C.c_uint64, _I, C.POINTER(_P)],
+    "djb_nn_destroy": [_P],
+    "djb_nn_param_count": [_P, _I64P],
+    "djb_nn_get_params": [_P, _P],
+    "djb_nn_load": [_P, _P],
+    "djb_nn_set_stream": [_P, _P],
+    "djb_nn_apply": [_P, _P, _I, _P, _I],
+    "djb_nn_train_step": [_P, _P, _P, _I, _D, _DP, _I],
+    "djb_nn_backward": [_P, _P, _P, _I, _DP, _I],
+    "djb_nn_grads": [_P, _P, _I],
+    "djb_nn_set_grads": [_P, _P, _I],
+    "djb_nn_adam_step": [_P, _D],
 }
 _RESTYPES = {"djb_version": C.c_char_p, "djb_last_error": C.c_char_p}
 

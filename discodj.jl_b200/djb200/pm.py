@@ -200,6 +200,20 @@ class PMSolver:
                                                C.c_void_p(out.ctypes.data), MEM_HOST))
         return out
 
+    def mesh_fields(self, psi):
+        """[δ, F_x, F_y, F_z] on the mesh for displacements psi: (4, res, res, res) float32
+        [c][z][y][x] (host numpy for host psi, a device tensor for a device psi)."""
+        n, res = self.n, int(self.cfg.res_pm)
+        p, mem, keep = _ptr_mem(psi, n)
+        if mem == MEM_DEVICE:
+            import torch
+            out = torch.empty((4, res, res, res), dtype=torch.float32, device=psi.device)
+        else:
+            out = np.empty((4, res, res, res), dtype=np.float32)
+        check(lib.djb_mesh_fields(self._h, p, _out_ptr(out), mem))
+        del keep
+        return out
+
     def set_state(self, psi, mom, mom_scale: float = 1.0):
         n = self.n
         p, mem, k1 = _ptr_mem(psi, n)

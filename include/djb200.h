@@ -209,6 +209,48 @@ DJB_API int djb_step_vjp(djb_solver* s, double ddrift1, double alpha, double bet
 DJB_API int djb_state_power_spectrum_vjp(djb_solver* s, int32_t bins, int32_t logarithmic, const double* pk_bar,
                                          float* psi_bar, int32_t mem);
 
+/* The PM fields on the solver's mesh for displacements psi: out = [delta, F_x, F_y,
+ * F_z], four float32 res^3 meshes [z][y][x] (delta = mesh*res^3/n^3 - 1 of the W-order
+ * deposit without shift; F_c = -D_c phi, the FD gradient of the potential the force
+ * interpolates, pm.jl:330-342). No counterpart in the reference: the inputs of the
+ * force-correction network. FD gradients (2/4/6) without resampling. */
+DJB_API int djb_mesh_fields(djb_solver* s, const float* psi, float* out, int32_t mem);
+
+/* ── force-correction network ──────────────────────────────────────────────────
+ * No counterpart in the reference. A 3-D CNN on the PM mesh: `layers` convolutions
+ * with 3^3 kernels and periodic boundaries, cin -> hidden -> ... -> cout channels, ReLU
+ * between layers (for the force correction: in = delta and the three force
+ * components, out = the three components of a force correction). bf16 operands with
+ * float32 accumulation on the tensor cores (im2col + cuBLAS GEMMs), float32 master
+ * weights and Adam. Meshes cross the ABI as float32 [channel][z][y][x] of res^3
+ * voxels in the memory `mem` names. Parameters: per layer the weights
+ * [27 taps (dz, dy, dx) x cin_pad x cout_pad] then cout_pad biases, channel counts
+ * padded to multiples of 8 (padding entries are zero and stay zero). */
+typedef struct djb_nn djb_nn;
+DJB_API int djb_nn_create(int32_t layers, int32_t cin, int32_t hidden, int32_t cout, uint64_t seed,
+                          int32_t device, djb_nn** out);
+DJB_API int djb_nn_destroy(djb_nn* h);
+DJB_API int djb_nn_param_count(const djb_nn* h, int64_t* count);
+/* Host float32 arrays of djb_nn_param_count entries; load also resets the optimizer. */
+DJB_API int djb_nn_get_params(djb_nn* h, float* params);
+DJB_API int djb_nn_load(djb_nn* h, const float* params);
+DJB_API int djb_nn_set_stream(djb_nn* h, void* stream);
+/* out = net(in); large meshes are processed in chunks of z planes. */
+DJB_API int djb_nn_apply(djb_nn* h, const float* in, int32_t res, float* out, int32_t mem);
+/* Gradients of the mean squared error of net(in) against target into the network's
+ * gradient buffer; *loss (may be null) receives the loss. For data-parallel training
+ * the buffer is read (djb_nn_grads), summed across replicas and written back
+ * (djb_nn_set_grads) before djb_nn_adam_step. */
+DJB_API int djb_nn_backward(djb_nn* h, const float* in, const float* target, int32_t res, double* loss,
+                            int32_t mem);
+DJB_API int djb_nn_grads(djb_nn* h, float* grads, int32_t mem);
+DJB_API int djb_nn_set_grads(djb_nn* h, const float* grads, int32_t mem);
+/* One Adam step (beta 0.9/0.999, eps 1e-8, learning rate lr) with the buffered gradients. */
+DJB_API int djb_nn_adam_step(djb_nn* h, double lr);
+/* djb_nn_backward then djb_nn_adam_step; *loss is the loss before the step. */
+DJB_API int djb_nn_train_step(djb_nn* h, const float* in, const float* target, int32_t res, double lr,
+                              double* loss, int32_t mem);
+
 /* ── non-allocating shell sums ──────────────────────────────────────────────
  * No counterpart in the reference. For callers that cannot allocate device
  * memory at the point of the call: code running while a stream is being
