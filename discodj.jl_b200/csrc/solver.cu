@@ -1139,6 +1139,18 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
 
 // Force evaluation for all shifts; if `step`, fused with the drift/kick/drift.
 // Reads s->psi (and s->mom). Output: s->acc (step == 0) or updated psi/mom.
+// The fused z pass of the 1024³ Poisson solve on the half spectrum in `mesh`.
+void launch_zpass(djb_solver* s, float* mesh, int nh) {
+    const dim3 grid(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res));
+    const djb::KPhiFn kp{s->lapT, s->makT, s->s0};
+    if (DJB_ZPASS_PAIR)
+        djb::k_zpencil_pair<<<grid, djb::kZPairThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh,
+                                                                                  s->wN, kp);
+    else
+        djb::k_zpencil_kphi<<<grid, djb::kZThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh,
+                                                                              s->wN, kp);
+}
+
 // Brick sort of the particles at X = q + Ψ (+ dd1·Mom when `mom`): perm (sort.cuh).
 int sort_particles(djb_solver* s, const float* mom, float dd1) {
     s->prof.begin(s->stream, PH_SORT);
@@ -1191,9 +1203,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             if (s->zpass) {
                 s->prof.begin(s->stream, PH_KSPACE);
                 const int nh = s->res / 2 + 1;
-                djb::k_zpencil_kphi<<<dim3(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res)),
-                                      djb::kZThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh, s->wN,
-                                                                                djb::KPhiFn{s->lapT, s->makT, s->s0});
+                launch_zpass(s, mesh, nh);
                 s->prof.end(s->stream, PH_KSPACE, 1);
                 s->prof.begin(s->stream, PH_C2R);
                 CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
@@ -1268,9 +1278,7 @@ int poisson(djb_solver* s, int m) {
     else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
     const int nh = s->res / 2 + 1;
     if (s->zpass) {
-        djb::k_zpencil_kphi<<<dim3(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res)),
-                              djb::kZThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh, s->wN,
-                                                                        djb::KPhiFn{s->lapT, s->makT, s->s0});
+        launch_zpass(s, mesh, nh);
         CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
     } else {
         djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)), kThreads,
@@ -1560,6 +1568,8 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                 w32[j] = make_float2(float(std::cos(2 * M_PI * j / 32)), float(-std::sin(2 * M_PI * j / 32)));
             CUDA_TRY(cudaMemcpyToSymbol(djb::c_w32, w32, sizeof(w32)));
             CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_kphi<djb::KPhiFn>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
+            CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
         }
         if (s->sorted && s->gsx <= res) {

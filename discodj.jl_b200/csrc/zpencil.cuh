@@ -176,4 +176,138 @@ __global__ void __launch_bounds__(kZThreads, DJB_ZPASS_BLOCKS) k_zpencil_kphi(fl
     }
 }
 
+// ── pencil transforms on thread pairs ───────────────────────────────────────
+// The same transform with each 32-point DFT split over two threads (lanes 8 apart):
+// thread h of the pair holds points 16h .. 16h + 15. The radix-2 stage of length 32
+// pairs point j with j + 16, i.e. the two threads, and exchanges them with one
+// shuffle per point; the stages of length 16 .. 2 stay inside each thread. Half the
+// registers per thread (16 points) let twice as many warps share an SM, which the pass
+// needs to keep enough loads in flight (it is bound by load latency).
+#ifndef DJB_ZPASS_PAIR
+#define DJB_ZPASS_PAIR 1
+#endif
+constexpr int kZPairThreads = kZPencils * 64;
+
+template <int LEN>
+__device__ __forceinline__ void dif_stage16(float2 (&b)[16]) {
+    constexpr int half = LEN / 2;
+#pragma unroll
+    for (int s = 0; s < 16; s += LEN) {
+#pragma unroll
+        for (int j = 0; j < half; ++j) {
+            const float2 u = b[s + j], v = b[s + j + half];
+            b[s + j] = make_float2(u.x + v.x, u.y + v.y);
+            const float2 d = make_float2(u.x - v.x, u.y - v.y);
+            b[s + j + half] = (j == 0) ? d : cmul(d, c_w32[j * (32 / LEN)]);
+        }
+    }
+}
+
+template <int LEN>
+__device__ __forceinline__ void dit_stage16(float2 (&b)[16]) {
+    constexpr int half = LEN / 2;
+#pragma unroll
+    for (int s = 0; s < 16; s += LEN) {
+#pragma unroll
+        for (int j = 0; j < half; ++j) {
+            const float2 u = b[s + j];
+            const float2 v = (j == 0) ? b[s + j + half] : cmul(b[s + j + half], c_w32[j * (32 / LEN)]);
+            b[s + j] = make_float2(u.x + v.x, u.y + v.y);
+            b[s + j + half] = make_float2(u.x - v.x, u.y - v.y);
+        }
+    }
+}
+
+__device__ __forceinline__ float2 shfl_pair(float2 v) {
+    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, 8), __shfl_xor_sync(0xffffffffu, v.y, 8));
+}
+
+// Forward DIF over the pair: natural order in, bit-reversed order out (position 16h + i).
+__device__ __forceinline__ void dft32_dif_pair(float2 (&b)[16], int h) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const float2 o = shfl_pair(b[j]);
+        if (h == 0) {
+            b[j] = make_float2(b[j].x + o.x, b[j].y + o.y);
+        } else {
+            const float2 d = make_float2(o.x - b[j].x, o.y - b[j].y);
+            b[j] = (j == 0) ? d : cmul(d, c_w32[j]);
+        }
+    }
+    dif_stage16<16>(b);
+    dif_stage16<8>(b);
+    dif_stage16<4>(b);
+    dif_stage16<2>(b);
+}
+
+// Forward DIT over the pair: bit-reversed order in, natural order out.
+__device__ __forceinline__ void dft32_dit_pair(float2 (&b)[16], int h) {
+    dit_stage16<2>(b);
+    dit_stage16<4>(b);
+    dit_stage16<8>(b);
+    dit_stage16<16>(b);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const float2 m = (h == 1 && j > 0) ? cmul(b[j], c_w32[j]) : b[j];
+        const float2 o = shfl_pair(m);
+        b[j] = (h == 0) ? make_float2(m.x + o.x, m.y + o.y) : make_float2(o.x - m.x, o.y - m.y);
+    }
+}
+
+// Thread (q, h, t) at threadIdx.x = q + 8 h + 16 t: pencil q, half h, and t = n2 (steps
+// A, B') or k1 (steps B, A'); a warp reads 4 kz rows of 8 consecutive kx per load.
+template <class KPhi>
+__global__ void __launch_bounds__(kZPairThreads, 2) k_zpencil_pair(float2* __restrict__ f, int nh,
+                                                                   const float2* __restrict__ wN, KPhi kphi) {
+    extern __shared__ __align__(16) float2 s[];  // kZPencils transpose blocks
+    const int q = threadIdx.x & 7;
+    const int h = (threadIdx.x >> 3) & 1;
+    const int t = threadIdx.x >> 4;
+    const int ky = blockIdx.y;
+    const int kx = blockIdx.x * kZPencils + q;
+    const bool active = kx < nh;
+    const int64_t zstride = int64_t(kZRes) * nh;
+    float2* __restrict__ col = f + int64_t(ky) * nh + (active ? kx : 0);
+    float2* const sq = s + q * kZPlane;
+    float2 b[16];
+    // A: x[t + 32 n1], n1 = 16 h + i
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        b[i] = active ? __ldcs(col + int64_t(t + 32 * (16 * h + i)) * zstride) : make_float2(0.f, 0.f);
+    dft32_dif_pair(b, h);  // b[i] = Y[k1 = brev(16h + i)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int k1 = brev5(16 * h + i);
+        sq[k1 * kZRow + t] = (k1 == 0) ? b[i] : cmul(b[i], __ldg(wN + ((t * k1) & (kZRes - 1))));
+    }
+    __syncthreads();
+    // B: thread pair k1 = t: DFT over n2 (this thread: n2 = 16 h + i)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) b[i] = sq[t * kZRow + 16 * h + i];
+    dft32_dif_pair(b, h);  // b[i] = X[t + 32 brev(16h + i)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const float K = kphi.fast(kx, ky, t + 32 * brev5(16 * h + i));
+        b[i] = make_float2(b[i].x * K, -(b[i].y * K));  // conjugated for the inverse below
+    }
+    // A': inverse DFT over k2 -> Z[k1 = t][n2 = 16 h + i]; this thread reads and writes
+    // only its half of row t
+    dft32_dit_pair(b, h);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int n2 = 16 * h + i;
+        const float2 z = conjf2(b[i]);
+        sq[t * kZRow + n2] = (t == 0 || n2 == 0) ? z : cmul(z, conjf2(__ldg(wN + ((n2 * t) & (kZRes - 1)))));
+    }
+    __syncthreads();
+    // B': thread pair n2 = t: inverse DFT over k1 (this thread: k1 = 16 h + i)
+#pragma unroll
+    for (int i = 0; i < 16; ++i) b[i] = conjf2(sq[(16 * h + i) * kZRow + t]);
+    dft32_dif_pair(b, h);  // b[i] = conj(x[t + 32 brev(16h + i)])
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) __stcs(col + int64_t(t + 32 * brev5(16 * h + i)) * zstride, conjf2(b[i]));
+    }
+}
+
 }  // namespace djb
