@@ -249,13 +249,13 @@ def config_block(size, n, res, L, lpt, world):
 
 
 def nn_flops_per_voxel(layers=4, cin=4, hidden=32, cout=3):
-    """GEMM FLOPs per voxel of one forward pass as executed (channels padded to 8)."""
-    pad = lambda c: (c + 7) // 8 * 8  # noqa: E731
+    """Algorithmic FLOPs per voxel of one forward pass: 2·27·cin·cout per layer with the
+    real channel counts (the kernels pad K and N; the padding is not counted)."""
     f = 0
     for l in range(layers):
         ci = cin if l == 0 else hidden
         co = cout if l == layers - 1 else hidden
-        f += 2 * 27 * pad(ci) * (co if l == layers - 1 else pad(co))
+        f += 2 * 27 * ci * co
     return f
 
 
@@ -301,9 +301,10 @@ def nn_timing(dev, stream, world):
                roofline=dict(bound="tensor", unit="TFLOP/s", achieved_train=train_tflops,
                              achieved_eval=eval_tflops, peak=peak, frac_train=train_tflops / peak,
                              frac_eval=eval_tflops / peak, peak_source=f"{kind} bf16_tflops"),
-               note="4 layers 4->32->32->32->3, 3^3 kernels, periodic; bf16 GEMMs (im2col + cuBLAS), "
-                    "float32 accumulation; train = forward + backward + Adam at 128^3 (FLOPs counted as 3x "
-                    "forward); eval = one forward at 512^3 in 4 Mi-voxel chunks")
+               note="4 layers 4->32->32->32->3, 3^3 kernels, periodic; forward convolutions as implicit "
+                    "GEMMs on the tcgen05 tensor cores (bf16 operands, float32 accumulation in tensor memory), "
+                    "backward as im2col + cuBLAS GEMMs; train = forward + backward + Adam at 128^3 (FLOPs "
+                    "counted as 3x forward); eval = one forward at 512^3; FLOPs with the real channel counts")
     return out
 
 

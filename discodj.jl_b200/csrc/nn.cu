@@ -5,7 +5,11 @@
 // Inputs and outputs cross the C ABI as float32 meshes in the solver's layout,
 // [channel][z][y][x]; inside, activations are bf16 channels-last, [voxel][channel].
 //
-// Each convolution is an implicit GEMM made explicit per chunk of z planes:
+// Each convolution whose padded channel counts are at most 32 runs as an implicit GEMM
+// on the tensor cores (tcgen05.mma, `conv_tc.cuh`): input planes staged in shared memory
+// once, the 27 taps read as shifted operand views, the accumulator in tensor memory,
+// bias + ReLU fused into the epilogue. Wider layers, the backward pass, and every layer
+// after djb_nn_set_conv(h, 1), make the implicit GEMM explicit per chunk of z planes:
 //   col[v][tap·C + c] = X[v + offset(tap)][c]        k_im2col (bf16, periodic wrap)
 //   Y = col · W  (M = voxels, K = 27·C, N = channels out; bf16 operands, float32
 //                 accumulation on the tensor cores through cuBLAS)
@@ -28,6 +32,7 @@
 #include <vector>
 
 #include "common.h"
+#include "conv_tc.cuh"
 #include "djb200.h"
 
 using djb::fail;
@@ -235,6 +240,9 @@ struct djb_nn {
     __nv_bfloat16* dY = nullptr;               // [nvox][Cmax]
     float* outm = nullptr;                     // [cout][nvox] float32
     double* lsum = nullptr;
+    int* derr = nullptr;                       // set by a tensor-core convolution whose wait ran out
+    int conv_mode = 0;                         // 0: tensor-core convolutions where possible; 1: im2col
+    bool have_col = false;                     // col and Y allocated
     std::vector<void*> work;
 };
 
@@ -262,6 +270,7 @@ void free_work(djb_nn* h) {
     for (auto& a : h->act) a = nullptr;
     h->col = nullptr;
     h->Y = nullptr;
+    h->have_col = false;
     h->dcol = nullptr;
     h->dA = nullptr;
     h->dY = nullptr;
@@ -275,11 +284,92 @@ int cmax(const djb_nn* h) {
     return c;
 }
 
+// Layer l runs on the tensor-core implicit GEMM (padded channel counts up to 32).
+bool use_tc(const djb_nn* h, int l) { return h->conv_mode == 0 && h->cinp[l] <= 32 && h->coutp[l] <= 32; }
+
+bool any_im2col(const djb_nn* h) {
+    for (int l = 0; l < h->layers; ++l)
+        if (!use_tc(h, l)) return true;
+    return false;
+}
+
+template <int CC, int N, bool LAST>
+int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
+    using namespace djb::conv;
+    constexpr int KC = (CC + 1) / 2 * 2;
+    constexpr int bytes = smem_bytes<KC, N>();
+    auto kern = k_conv3_tc<CC, N, LAST>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    int occ = 0, sms = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, bytes));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    if (occ < 1) return fail(DJB_ERR_CUDA, "tensor-core convolution does not fit on an SM (%d bytes)", bytes);
+    Args a = a0;
+    a.ntx = (a.res + kTX - 1) / kTX;
+    a.nty = (a.res + kTY - 1) / kTY;
+    // z segments: whole columns when there are enough of them for every CTA slot four
+    // times over, else shorter segments (each costs two extra planes)
+    const int64_t slots = int64_t(occ) * sms;
+    a.zlen = a.res;
+    while (a.zlen > 4 && int64_t(a.ntx) * a.nty * ((a.res + a.zlen - 1) / a.zlen) < 4 * slots)
+        a.zlen = (a.zlen + 1) / 2;
+    a.nzs = (a.res + a.zlen - 1) / a.zlen;
+    const int64_t items = int64_t(a.ntx) * a.nty * a.nzs;
+    const int grid = int(std::min<int64_t>(items, slots));
+    kern<<<grid, kThreads, bytes, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+template <int N, bool LAST>
+int launch_tc_cc(djb_nn* h, int cc, const djb::conv::Args& a, cudaStream_t st) {
+    switch (cc) {
+        case 1: return launch_tc_inst<1, N, LAST>(h, a, st);
+        case 2: return launch_tc_inst<2, N, LAST>(h, a, st);
+        case 3: return launch_tc_inst<3, N, LAST>(h, a, st);
+        case 4: return launch_tc_inst<4, N, LAST>(h, a, st);
+        default: return fail(DJB_ERR_INVALID, "tensor-core convolution: %d input channels", cc * 8);
+    }
+}
+
+// Layer l on the tensor cores: act[l] → act[l + 1] (hidden) or outm (last).
+int conv_tc(djb_nn* h, int l) {
+    const bool last = (l == h->layers - 1);
+    djb::conv::Args a{};
+    a.X = h->act[l];
+    a.W = h->pb + h->woff[l];
+    a.bias = h->p + h->boff[l];
+    a.Y = last ? nullptr : h->act[l + 1];
+    a.Yf = last ? h->outm : nullptr;
+    a.res = h->res;
+    a.cin = h->cinp[l];
+    a.cout = h->coutp[l];
+    a.nout = h->cout[l];
+    a.err = h->derr;
+    const int cc = h->cinp[l] / 8;
+    const bool n16 = h->coutp[l] <= 16;
+    if (last) return n16 ? launch_tc_cc<16, true>(h, cc, a, h->stream) : launch_tc_cc<32, true>(h, cc, a, h->stream);
+    return n16 ? launch_tc_cc<16, false>(h, cc, a, h->stream) : launch_tc_cc<32, false>(h, cc, a, h->stream);
+}
+
+// Reads the device error word of the tensor-core convolutions (after a stream sync).
+int check_derr(djb_nn* h) {
+    int e = 0;
+    CUDA_TRY(cudaMemcpyAsync(&e, h->derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (e) {
+        cudaMemsetAsync(h->derr, 0, sizeof(int), h->stream);
+        return fail(DJB_ERR_CUDA, "tensor-core convolution: a wait for the tensor cores ran out");
+    }
+    return DJB_OK;
+}
+
 // Work areas for res³ voxels; training needs the whole mesh at once (chunk = nvox).
 int ensure_work(djb_nn* h, int res, bool train) {
     const int64_t nvox = int64_t(res) * res * res;
     const bool need_train = train && !h->dcol;
-    if (h->res == res && !need_train) return DJB_OK;
+    const bool need_col = (train || any_im2col(h)) && !h->have_col;
+    if (h->res == res && !need_train && !need_col) return DJB_OK;
     free_work(h);
     const int C = cmax(h);
     // chunks of whole z planes holding at most 4 Mi voxels (col: 27·C bf16 per voxel,
@@ -289,8 +379,11 @@ int ensure_work(djb_nn* h, int res, bool train) {
     h->chunk = train ? nvox : planes * res * res;
     for (int l = 0; l < h->layers; ++l)
         TRYN(dalloc(h, (void**)&h->act[l], size_t(nvox) * h->cinp[l] * sizeof(__nv_bfloat16), true));
-    TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
-    TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
+    if (train || any_im2col(h)) {
+        TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
+        TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
+        h->have_col = true;
+    }
     TRYN(dalloc(h, (void**)&h->outm, size_t(nvox) * h->cout[h->layers - 1] * sizeof(float), true));
     TRYN(dalloc(h, (void**)&h->lsum, sizeof(double), true));
     if (train) {
@@ -309,6 +402,10 @@ int forward(djb_nn* h, const float* in) {
     const float one = 1.0f, zero = 0.0f;
     k_pack<<<grid_of(nvox * h->cinp[0]), kNT, 0, h->stream>>>(in, h->cin[0], h->cinp[0], nvox, 0, nvox, h->act[0]);
     for (int l = 0; l < h->layers; ++l) {
+        if (use_tc(h, l)) {
+            TRYN(conv_tc(h, l));
+            continue;
+        }
         const int C = h->cinp[l], K = 27 * C;
         const bool last = (l == h->layers - 1);
         const int N = last ? h->cout[l] : h->coutp[l];
@@ -445,6 +542,8 @@ int djb_nn_create(int32_t layers, int32_t cin, int32_t hidden, int32_t cout, uin
     TRYN(dalloc(h, (void**)&h->m2, size_t(off) * sizeof(float), false));
     TRYN(dalloc(h, (void**)&h->g, size_t(off) * sizeof(float), false));
     TRYN(dalloc(h, (void**)&h->frozen, size_t(off), false));
+    TRYN(dalloc(h, (void**)&h->derr, sizeof(int), false));
+    CUDA_TRY(cudaMemset(h->derr, 0, sizeof(int)));
     CUDA_TRY(cudaMemcpy(h->p, p.data(), size_t(off) * sizeof(float), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->frozen, fr.data(), size_t(off), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemset(h->m1, 0, size_t(off) * sizeof(float)));
@@ -458,7 +557,8 @@ int djb_nn_destroy(djb_nn* h) {
     if (!h) return DJB_OK;
     cudaSetDevice(h->device);
     free_work(h);
-    for (void* q : {(void*)h->p, (void*)h->pb, (void*)h->m1, (void*)h->m2, (void*)h->g, (void*)h->frozen})
+    for (void* q : {(void*)h->p, (void*)h->pb, (void*)h->m1, (void*)h->m2, (void*)h->g, (void*)h->frozen,
+                    (void*)h->derr})
         if (q) cudaFree(q);
     if (h->blas) cublasDestroy(h->blas);
     if (h->own) cudaStreamDestroy(h->own);
@@ -503,6 +603,14 @@ int djb_nn_set_stream(djb_nn* h, void* stream) {
     return DJB_OK;
 }
 
+int djb_nn_set_conv(djb_nn* h, int32_t mode) {
+    djb::clear_error();
+    if (!h) return fail(DJB_ERR_INVALID, "null argument");
+    if (mode != 0 && mode != 1) return fail(DJB_ERR_INVALID, "conv mode must be 0 (tensor-core) or 1 (im2col)");
+    h->conv_mode = mode;
+    return DJB_OK;
+}
+
 int djb_nn_apply(djb_nn* h, const float* in, int32_t res, float* out, int32_t mem) {
     djb::clear_error();
     if (!h || !in || !out) return fail(DJB_ERR_INVALID, "null argument");
@@ -521,8 +629,7 @@ int djb_nn_apply(djb_nn* h, const float* in, int32_t res, float* out, int32_t me
         rc = fail(DJB_ERR_CUDA, "output copy failed");
     if (own_in) cudaFreeAsync(din, h->stream);
     if (rc != DJB_OK) return rc;
-    CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return DJB_OK;
+    return check_derr(h);
 }
 
 // Gradients of the mean squared error of net(in) against target, into the network's
@@ -543,8 +650,7 @@ int djb_nn_backward(djb_nn* h, const float* in, const float* target, int32_t res
     if (own_in) cudaFreeAsync(din, h->stream);
     if (own_t) cudaFreeAsync(dt, h->stream);
     if (rc != DJB_OK) return rc;
-    CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return DJB_OK;
+    return check_derr(h);
 }
 
 int djb_nn_grads(djb_nn* h, float* grads, int32_t mem) {

@@ -95,6 +95,7 @@ SIGNATURES = {
     "djb_nn_get_params": [_P, _P],
     "djb_nn_load": [_P, _P],
     "djb_nn_set_stream": [_P, _P],
+    "djb_nn_set_conv": [_P, _I],
     "djb_nn_apply": [_P, _P, _I, _P, _I],
     "djb_nn_train_step": [_P, _P, _P, _I, _D, _DP, _I],
     "djb_nn_backward": [_P, _P, _P, _I, _DP, _I],

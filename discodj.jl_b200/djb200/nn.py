@@ -60,6 +60,15 @@ class ForceNet:
     def set_stream(self, stream_ptr: int | None):
         check(lib.djb_nn_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
 
+    def set_conv(self, mode: str):
+        """"tensor" (default): forward convolutions as implicit GEMMs on the tcgen05
+        tensor cores where the padded channel counts are at most 32; "im2col": im2col +
+        cuBLAS GEMMs for every layer."""
+        modes = {"tensor": 0, "im2col": 1}
+        if mode not in modes:
+            raise ValueError(f"conv mode must be one of {sorted(modes)}")
+        check(lib.djb_nn_set_conv(self._h, modes[mode]))
+
     def get_params(self) -> np.ndarray:
         p = np.empty(self.n_params, dtype=np.float32)
         check(lib.djb_nn_get_params(self._h, C.c_void_p(p.ctypes.data)))

@@ -221,7 +221,7 @@ DJB_API int djb_mesh_fields(djb_solver* s, const float* psi, float* out, int32_t
  * with 3^3 kernels and periodic boundaries, cin -> hidden -> ... -> cout channels, ReLU
  * between layers (for the force correction: in = delta and the three force
  * components, out = the three components of a force correction). bf16 operands with
- * float32 accumulation on the tensor cores (im2col + cuBLAS GEMMs), float32 master
+ * float32 accumulation on the tensor cores, float32 master
  * weights and Adam. Meshes cross the ABI as float32 [channel][z][y][x] of res^3
  * voxels in the memory `mem` names. Parameters: per layer the weights
  * [27 taps (dz, dy, dx) x cin_pad x cout_pad] then cout_pad biases, channel counts
@@ -235,6 +235,10 @@ DJB_API int djb_nn_param_count(const djb_nn* h, int64_t* count);
 DJB_API int djb_nn_get_params(djb_nn* h, float* params);
 DJB_API int djb_nn_load(djb_nn* h, const float* params);
 DJB_API int djb_nn_set_stream(djb_nn* h, void* stream);
+/* Convolution path: 0 (default) = implicit GEMM on the tcgen05 tensor cores for the
+ * forward convolutions whose padded channel counts are at most 32 (others, and the
+ * backward pass, use im2col + cuBLAS GEMMs); 1 = im2col + cuBLAS for every layer. */
+DJB_API int djb_nn_set_conv(djb_nn* h, int32_t mode);
 /* out = net(in); large meshes are processed in chunks of z planes. */
 DJB_API int djb_nn_apply(djb_nn* h, const float* in, int32_t res, float* out, int32_t mem);
 /* Gradients of the mean squared error of net(in) against target into the network's

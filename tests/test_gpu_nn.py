@@ -114,3 +114,26 @@ def test_training_reduces_loss_on_mesh_fields(djb):
         for _ in range(40):
             l1 = net.train_step(x, t, lr=1e-3)
     assert l1 < 0.7 * l0
+
+
+@pytest.mark.parametrize("res", [20, 35])
+def test_tensor_core_convolution_matches_im2col_and_torch(djb, res):
+    """The tcgen05 implicit-GEMM forward (partial 8 × 16 tiles when res is not a
+    multiple of the tile, several z segments) against the im2col + cuBLAS path and the
+    PyTorch restatement, for the 4-layer, 32-channel network."""
+    from djb200.nn import ForceNet
+    rng = np.random.default_rng(res)
+    x = rng.standard_normal((4, res, res, res)).astype(np.float32)
+    with ForceNet(layers=4, cin=4, hidden=32, cout=3, seed=5) as net:
+        p = net.get_params()
+        out_tc = net.apply(x)
+        net.set_conv("im2col")
+        out_gemm = net.apply(x)
+        net.set_conv("tensor")
+        again = net.apply(x)
+    assert np.array_equal(out_tc, again)
+    scale = np.max(np.abs(out_gemm))
+    assert np.max(np.abs(out_tc - out_gemm)) < 1e-2 * scale
+    ws, bs = _torch_net(net, p)
+    r = _torch_forward(ws, bs, x).detach().numpy()
+    assert np.max(np.abs(out_tc - r)) < NN_TOL * np.max(np.abs(r))
