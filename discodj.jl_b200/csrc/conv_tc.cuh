@@ -2,23 +2,34 @@
 // (tcgen05.mma, accumulator in tensor memory), for the force-correction network.
 //
 // Output tile: 8 (x) × 16 (y) voxels of one z plane = the 128 rows of one M = 128 MMA.
-// A CTA walks a column of such tiles along z. Its input planes are staged in shared
+// A CTA walks columns of such tiles along z. Its input planes are staged in shared
 // memory with a one-voxel halo (10 × 18 positions per plane, periodic wrap), as
 // [plane slot][8-channel chunk][position][8 channels]: in every chunk the 16-byte rows
 // of consecutive positions are contiguous. That is the no-swizzle K-major operand
 // layout with 8-row groups 160 bytes apart (one staged y row), so the A operand of a
 // tap (dx, dy, dz) is the same staged block read from a start address shifted by
 // (dy·10 + dx) rows: the 27 taps need no copies (no im2col).
-// Per tile: 27 taps × (K / 16) MMAs of 128 × N × 16 (bf16 operands, float32
-// accumulation), committed to an mbarrier. Two accumulators in tensor memory let the
-// epilogue of one tile (tcgen05.ld → bias, ReLU → bf16 rows) run while the MMAs of the
-// next are in flight; the next plane is copied in (cp.async) at the same time.
+// Warp roles (persistent CTAs, producer/consumer mbarriers, no CTA-wide barrier in the
+// loop):
+//   loader (warp 4): planes into a ring of kRing slots, one bulk tensor copy per plane
+//     (5-D map over [z][chunk][y][x][8 channels]) where the halo does not wrap, else
+//     16-byte cp.async with the periodic wrap; completion on the slot's `full` barrier.
+//   MMA (warp 5, one thread): per tile 27 taps × (K / 16) tcgen05.mma of 128 × N × 16
+//     (bf16 operands, float32 accumulation) into one of kAcc tensor-memory
+//     accumulators; commits to the accumulator's `accf` barrier and to the `empty`
+//     barrier of the plane the tile was the last reader of.
+//   epilogue (warps 0-3, tensor-memory lanes 0-127): tcgen05.ld of the accumulator,
+//     `acce` arrive, then bias + ReLU → bf16 rows (hidden layers), bias → float32
+//     channel-major mesh (last layer), or the ReLU mask of the layer below → bf16
+//     (data gradient: the convolution with the flipped, transposed weights).
 // The weights of the layer, [tap][chunk][n][8] (K-major B operand), stay in shared
 // memory for the CTA's whole run.
-// Waits are bounded: a wait that runs out sets the error word, and the CTA drains its
-// copies, frees its tensor memory and returns.
+// Waits are bounded: a wait that runs out sets the error word and the CTA's abort
+// flag; every role then stops, the MMAs and copies in flight are waited for (bounded),
+// and the tensor memory is freed.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -30,23 +41,29 @@ namespace conv {
 constexpr int kTX = 8, kTY = 16;                       // tile: 8 × 16 voxels = 128 MMA rows
 constexpr int kBX = kTX + 2, kBY = kTY + 2;            // staged plane with its halo
 constexpr int kPlane = kBX * kBY;                      // 180 positions
-constexpr int kRing = 4;                               // planes z−1, z, z+1 and the next
-constexpr int kThreads = 128;                          // four warps: tensor-memory lanes 0-127
+constexpr int kRing = 8;                               // staged planes
+constexpr int kAcc = 4;                                // accumulators in tensor memory
+constexpr int kLoaderWarp = 4, kMmaWarp = 5;
+constexpr int kThreads = 192;
+
+enum Mode { kHidden = 0, kLast = 1, kBackData = 2 };
 
 struct Args {
-    const __nv_bfloat16* X;   // [nvox][cin] input activations (cin = 8·CC)
-    const __nv_bfloat16* W;   // [27][cin][cout] weights (tap = kz·9 + ky·3 + kx)
-    const float* bias;        // [cout]
-    __nv_bfloat16* Y;         // hidden layers: [nvox][cout] bf16, relu(acc + bias)
-    float* Yf;                // last layer: [nout][nvox] float32, acc + bias
-    int res, cin, cout, nout;
+    const __nv_bfloat16* X;   // [nvox][cin] input (cin = 8·CC)
+    const __nv_bfloat16* W;   // flip = 0: [27][cin][cout]; flip = 1: [27][cout][cin] of the forward layer
+    const float* bias;        // [cout] (kHidden, kLast)
+    const __nv_bfloat16* M;   // kBackData: [nvox][cout], output kept where M > 0
+    __nv_bfloat16* Y;         // kHidden, kBackData: [nvox][cout] bf16
+    float* Yf;                // kLast: [nout][nvox] float32
+    int res, cin, cout, nout, flip;
     int ntx, nty, nzs, zlen;  // tiles along x, y; z segments of zlen planes
+    int use_tma;              // the map covers X: interior planes by bulk tensor copy
     int* err;                 // set to 1 when a wait runs out
 };
 
 template <int KC, int N>
 constexpr int smem_bytes() {
-    return 27 * KC * N * 16 + kRing * KC * kPlane * 16 + 32;
+    return 27 * KC * N * 16 + kRing * KC * kPlane * 16 + (2 * kRing + 2 * kAcc + 1) * 8 + 16;
 }
 
 // Shared-memory matrix descriptor, no swizzle: start, leading (K-chunk) and stride
@@ -70,6 +87,7 @@ __device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t a, uint64_t b,
         : "memory");
 }
 
+// Arrives on `bar` once every MMA this thread issued before has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
@@ -78,25 +96,38 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 16 consecutive float32 columns of this thread's tensor-memory lane.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* f) {
-    uint32_t r[16];
+// 16 consecutive float32 columns of this thread's tensor-memory lane (no wait).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) f[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Arrives on `bar` when this thread's earlier cp.async copies have landed (the barrier's
+// expected count includes this arrival).
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            int c4, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
 
 __device__ __forceinline__ int wrap(int v, int res) {
     v %= res;
@@ -108,29 +139,46 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// Copies input plane z (any integer, wrapped) of the tile column at (x0, y0) into `slot`.
-template <int CC, int KC>
-__device__ __forceinline__ void stage_plane(const Args& a, uint32_t ring, int slot, int z, int x0, int y0) {
-    const int gz = wrap(z, a.res);
-    for (int e = threadIdx.x; e < CC * kPlane; e += kThreads) {
-        const int pos = e / CC, kc = e - pos * CC;
-        const int by = pos / kBX, bx = pos - by * kBX;
-        const int gy = wrap(y0 - 1 + by, a.res), gx = wrap(x0 - 1 + bx, a.res);
-        const __nv_bfloat16* src = a.X + ((int64_t(gz) * a.res + gy) * a.res + gx) * (CC * 8) + kc * 8;
-        cp_async16(ring + uint32_t(((slot * KC + kc) * kPlane + pos) * 16), src);
-    }
+// Bounded barrier wait of one role; false (and the CTA's abort flag set) when it ran
+// out or another role has aborted.
+__device__ __forceinline__ bool role_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+    if (*abort_flag) return false;
+    if (mbar_wait(bar, parity)) return true;
+    *abort_flag = 1;
+    return false;
 }
 
-template <int CC, int N, bool LAST>
-__global__ void __launch_bounds__(kThreads, 2) k_conv3_tc(Args a) {
+struct Item {
+    int x0, y0, z0, nt;
+};
+
+__device__ __forceinline__ Item item_of(const Args& a, int item) {
+    const int tx = item % a.ntx, rr = item / a.ntx, ty = rr % a.nty, zs = rr / a.nty;
+    Item it;
+    it.x0 = tx * kTX;
+    it.y0 = ty * kTY;
+    it.z0 = zs * a.zlen;
+    it.nt = min(a.zlen, a.res - it.z0);
+    return it;
+}
+
+template <int CC, int N, int MODE>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_conv3_tc(const __grid_constant__ Args a, const __grid_constant__ CUtensorMap tmap) {
     constexpr int KC = (CC + 1) / 2 * 2;          // K chunks staged (K a multiple of 16)
-    constexpr uint32_t kCols = N * 2 < 32 ? 32 : N * 2;
+    constexpr uint32_t kCols = kAcc * N < 32 ? 32 : kAcc * N;
+    constexpr uint32_t kSlot = KC * kPlane * 16;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* ws = smem;
     uint8_t* ringp = smem + 27 * KC * N * 16;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(ringp + kRing * KC * kPlane * 16);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    uint64_t* full = reinterpret_cast<uint64_t*>(ringp + kRing * kSlot);
+    uint64_t* empty = full + kRing;
+    uint64_t* accf = empty + kRing;
+    uint64_t* acce = accf + kAcc;
+    uint64_t* fin = acce + kAcc;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t ws_u = smem_u32(ws), ring = smem_u32(ringp);
 
     // weights → [tap][chunk][n][8 k], zeros beyond cin and cout
@@ -143,7 +191,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_conv3_tc(Args a) {
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
                 const int k = kc * 8 + 2 * j + u;
-                f[u] = (k < a.cin && n < a.cout) ? __bfloat162float(a.W[(int64_t(tap) * a.cin + k) * a.cout + n]) : 0.0f;
+                float v = 0.0f;
+                if (k < a.cin && n < a.cout)
+                    v = __bfloat162float(a.flip ? a.W[(int64_t(26 - tap) * a.cout + n) * a.cin + k]
+                                                : a.W[(int64_t(tap) * a.cin + k) * a.cout + n]);
+                f[u] = v;
             }
             w[j] = pack_bf16(f[0], f[1]);
         }
@@ -157,8 +209,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_conv3_tc(Args a) {
         }
     }
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int i = 0; i < kRing; ++i) {
+            mbar_init(&full[i], 32);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < kAcc; ++i) {
+            mbar_init(&accf[i], 1);
+            mbar_init(&acce[i], 4);
+        }
+        mbar_init(fin, 1);
+        *abort_flag = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -171,117 +231,164 @@ __global__ void __launch_bounds__(kThreads, 2) k_conv3_tc(Args a) {
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = *tslot;
-    const uint32_t lane_base = uint32_t(warp * 32) << 16;
-    const uint32_t id = idesc<N>();
-    const int64_t nvox = int64_t(a.res) * a.res * a.res;
+    const int items = a.ntx * a.nty * a.nzs;
 
-    uint32_t ph[2] = {0u, 0u};
-    int t = 0;        // tiles committed by this CTA; accumulator t & 1
-    bool ok = true;
-
-    auto epilogue = [&](int x0, int y0, int z, int buf) {
-        float f[N];
-#pragma unroll
-        for (int q = 0; q < N / 16; ++q) tmem_ld16(tmem + lane_base + uint32_t(buf * N + q * 16), f + q * 16);
-        const int x = x0 + (tid & 7), y = y0 + (tid >> 3);
-        if (x >= a.res || y >= a.res) return;
-        const int64_t v = (int64_t(z) * a.res + y) * a.res + x;
-        if constexpr (LAST) {
-#pragma unroll
-            for (int c = 0; c < N; ++c)
-                if (c < a.nout) a.Yf[int64_t(c) * nvox + v] = f[c] + __ldg(a.bias + c);
-        } else {
-            uint4* dst = reinterpret_cast<uint4*>(a.Y + v * a.cout);
-#pragma unroll
-            for (int c8 = 0; c8 < N / 8; ++c8) {
-                if (c8 * 8 >= a.cout) break;
-                uint32_t w[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int c = c8 * 8 + 2 * j;
-                    w[j] = pack_bf16(fmaxf(f[c] + __ldg(a.bias + c), 0.0f), fmaxf(f[c + 1] + __ldg(a.bias + c + 1), 0.0f));
+    if (warp == kLoaderWarp) {
+        // ── loader ──────────────────────────────────────────────────────────────
+        uint32_t k = 0;   // planes issued by this CTA; plane k in slot k % kRing
+        bool ok = true;
+        for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+            const Item it = item_of(a, item);
+            const bool interior = a.use_tma && it.x0 >= 1 && it.x0 - 1 + kBX <= a.res && it.y0 >= 1 &&
+                                  it.y0 - 1 + kBY <= a.res;
+            for (int j = 0; j < it.nt + 2; ++j, ++k) {
+                const int slot = int(k % kRing);
+                if (!role_wait(&empty[slot], ((k / kRing) & 1u) ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
                 }
-                dst[c8] = make_uint4(w[0], w[1], w[2], w[3]);
+                const int gz = wrap(it.z0 - 1 + j, a.res);
+                const uint32_t dst = ring + uint32_t(slot) * kSlot;
+                if (interior) {
+                    if (lane == 0) {
+                        mbar_arrive_expect_tx(&full[slot], uint32_t(CC * kPlane * 16));
+                        tma_load_5d(dst, &tmap, 0, it.x0 - 1, it.y0 - 1, 0, gz, &full[slot]);
+                    } else {
+                        mbar_arrive(&full[slot]);
+                    }
+                } else {
+                    for (int e = lane; e < CC * kPlane; e += 32) {
+                        const int pos = e / CC, kc = e - pos * CC;
+                        const int by = pos / kBX, bx = pos - by * kBX;
+                        const int gy = wrap(it.y0 - 1 + by, a.res), gx = wrap(it.x0 - 1 + bx, a.res);
+                        const __nv_bfloat16* src =
+                            a.X + ((int64_t(gz) * a.res + gy) * a.res + gx) * (CC * 8) + kc * 8;
+                        cp_async16(dst + uint32_t((kc * kPlane + pos) * 16), src);
+                    }
+                    cp_async_arrive(&full[slot]);
+                }
             }
         }
-    };
-
-    const int items = a.ntx * a.nty * a.nzs;
-    for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
-        const int tx = item % a.ntx, rr = item / a.ntx, ty = rr % a.nty, zs = rr / a.nty;
-        const int x0 = tx * kTX, y0 = ty * kTY, z0 = zs * a.zlen;
-        const int nt = min(a.zlen, a.res - z0);
-        // planes z0 − 1 + j live in slot j % kRing; tile i reads j = i, i + 1, i + 2
-        stage_plane<CC, KC>(a, ring, 0, z0 - 1, x0, y0);
-        stage_plane<CC, KC>(a, ring, 1, z0, x0, y0);
-        stage_plane<CC, KC>(a, ring, 2, z0 + 1, x0, y0);
-        cp_async_commit();
-        for (int i = 0; i < nt; ++i) {
-            cp_async_wait_all();       // plane i + 2 (the newest group)
-            fence_proxy_async_smem();  // the copies are read by the tensor cores
-            tc_before_sync();
-            __syncthreads();
-            tc_after_sync();
-            const int buf = t & 1;
-            if (tid == 0) {
-                const uint32_t d = tmem + uint32_t(buf * N);
+        cp_async_wait_all();
+        if (!ok) {
+            // bulk copies still in flight land before the CTA ends
+            const uint32_t n = k < uint32_t(kRing) ? k : uint32_t(kRing);
+            for (uint32_t q = k - n; q < k; ++q) mbar_wait(&full[q % kRing], (q / kRing) & 1u);
+        }
+    } else if (warp == kMmaWarp) {
+        // ── MMA issue (one thread) ──────────────────────────────────────────────
+        if (lane == 0) {
+            const uint32_t id = idesc<N>();
+            const uint64_t adesc0 = sdesc(ring, kPlane * 16, kBX * 16);
+            const uint64_t bdesc0 = sdesc(ws_u, N * 16, 128);
+            uint32_t kp = 0, t = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+                const Item it = item_of(a, item);
+                const uint32_t base = kp;
+                for (int i = 0; i < it.nt; ++i, ++t) {
+                    const uint32_t b = t % kAcc;
+                    ok = role_wait(&acce[b], ((t / kAcc) & 1u) ^ 1u, abort_flag);
+                    for (int j = (i == 0 ? 0 : i + 2); ok && j <= i + 2; ++j) {
+                        const uint32_t p = base + uint32_t(j);
+                        ok = role_wait(&full[p % kRing], (p / kRing) & 1u, abort_flag);
+                    }
+                    if (!ok) break;
+                    tc_after_sync();
+                    const uint32_t d = tmem + b * N;
 #pragma unroll 1
-                for (int dz = 0; dz < 3; ++dz) {
-                    const uint32_t plane = ring + uint32_t(((i + dz) % kRing) * KC * kPlane * 16);
+                    for (int dz = 0; dz < 3; ++dz) {
+                        const uint64_t ad = adesc0 + (((base + i + dz) % kRing) * kSlot >> 4);
 #pragma unroll
-                    for (int dy = 0; dy < 3; ++dy)
+                        for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-                        for (int dx = 0; dx < 3; ++dx) {
-                            const int tap = dz * 9 + dy * 3 + dx;
-                            const uint32_t a0 = plane + uint32_t((dy * kBX + dx) * 16);
-                            const uint32_t b0 = ws_u + uint32_t(tap * KC * N * 16);
+                            for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-                            for (int s = 0; s < KC / 2; ++s)
-                                mma_bf16(d, sdesc(a0 + uint32_t(2 * s * kPlane * 16), kPlane * 16, kBX * 16),
-                                         sdesc(b0 + uint32_t(2 * s * N * 16), N * 16, 128), id,
-                                         (tap | s) != 0 ? 1u : 0u);
-                        }
+                                for (int s = 0; s < KC / 2; ++s) {
+                                    const int tap = dz * 9 + dy * 3 + dx;
+                                    mma_bf16(d, ad + uint64_t(((2 * s * kPlane + dy * kBX + dx) * 16) >> 4),
+                                             bdesc0 + uint64_t(((tap * KC + 2 * s) * N * 16) >> 4), id,
+                                             (dz | dy | dx | s) != 0 ? 1u : 0u);
+                                }
+                    }
+                    mma_commit(&accf[b]);
+                    mma_commit(&empty[(base + i) % kRing]);   // tile i is the last reader of plane i
                 }
-                mma_commit(&bar[buf]);
+                if (!ok) break;
+                mma_commit(&empty[(base + it.nt) % kRing]);
+                mma_commit(&empty[(base + it.nt + 1) % kRing]);
+                kp = base + it.nt + 2;
             }
-            if (i > 0) {
-                const bool w = mbar_wait(&bar[buf ^ 1], ph[buf ^ 1]);
-                ph[buf ^ 1] ^= 1u;
-                if (!__syncthreads_and(w)) {
+            // every MMA has completed before the tensor memory is released
+            mma_commit(fin);
+            mbar_wait(fin, 0);
+        }
+    } else {
+        // ── epilogue (warps 0-3: tensor-memory lanes 32·warp .. +31) ───────────────
+        const uint32_t lane_base = uint32_t(warp * 32) << 16;
+        const int64_t nvox = int64_t(a.res) * a.res * a.res;
+        uint32_t t = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+            const Item it = item_of(a, item);
+            const int x = it.x0 + (tid & 7), y = it.y0 + (tid >> 3);
+            const bool valid = x < a.res && y < a.res;
+            for (int i = 0; i < it.nt; ++i, ++t) {
+                const uint32_t b = t % kAcc;
+                if (!role_wait(&accf[b], (t / kAcc) & 1u, abort_flag)) {
                     ok = false;
-                    ++t;
                     break;
                 }
                 tc_after_sync();
+                uint32_t r[N];
+#pragma unroll
+                for (int q = 0; q < N / 16; ++q) tmem_ld16(tmem + lane_base + b * N + uint32_t(q * 16), r + q * 16);
+                tmem_wait_ld();
+                tc_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce[b]);
+                if (!valid) continue;
+                const int64_t v = (int64_t(it.z0 + i) * a.res + y) * a.res + x;
+                if constexpr (MODE == kLast) {
+#pragma unroll
+                    for (int c = 0; c < N; ++c)
+                        if (c < a.nout) a.Yf[int64_t(c) * nvox + v] = __uint_as_float(r[c]) + __ldg(a.bias + c);
+                } else {
+                    uint4* dst = reinterpret_cast<uint4*>(a.Y + v * a.cout);
+                    const uint4* msk = nullptr;
+                    if constexpr (MODE == kBackData) msk = reinterpret_cast<const uint4*>(a.M + v * a.cout);
+#pragma unroll
+                    for (int c8 = 0; c8 < N / 8; ++c8) {
+                        if (c8 * 8 >= a.cout) break;
+                        uint32_t w[4];
+                        if constexpr (MODE == kBackData) {
+                            const uint4 m4 = __ldg(msk + c8);
+                            const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const __nv_bfloat162 m2 = *reinterpret_cast<const __nv_bfloat162*>(&mw[j]);
+                                const float g0 = __bfloat162float(m2.x) > 0.0f ? __uint_as_float(r[c8 * 8 + 2 * j]) : 0.0f;
+                                const float g1 =
+                                    __bfloat162float(m2.y) > 0.0f ? __uint_as_float(r[c8 * 8 + 2 * j + 1]) : 0.0f;
+                                w[j] = pack_bf16(g0, g1);
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const int c = c8 * 8 + 2 * j;
+                                w[j] = pack_bf16(fmaxf(__uint_as_float(r[c]) + __ldg(a.bias + c), 0.0f),
+                                                 fmaxf(__uint_as_float(r[c + 1]) + __ldg(a.bias + c + 1), 0.0f));
+                            }
+                        }
+                        dst[c8] = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                }
             }
-            // plane i + 3 into the slot of plane i − 1 (its last reader, tile i − 1, is done)
-            if (i + 3 <= nt + 1) stage_plane<CC, KC>(a, ring, (i + 3) % kRing, z0 + i + 2, x0, y0);
-            cp_async_commit();
-            if (i > 0) epilogue(x0, y0, z0 + i - 1, buf ^ 1);
-            ++t;
         }
-        if (!ok) break;
-        // the column's last tile
-        const int lb = (t - 1) & 1;
-        const bool w = mbar_wait(&bar[lb], ph[lb]);
-        ph[lb] ^= 1u;
-        if (!__syncthreads_and(w)) {
-            ok = false;
-            break;
-        }
-        tc_after_sync();
-        epilogue(x0, y0, z0 + nt - 1, lb);
-        tc_before_sync();
-        __syncthreads();   // slots and accumulators are free for the next column
-    }
-    cp_async_wait_all();
-    if (!ok) {
-        if (tid == 0) atomicExch(a.err, 1);
-        // let the MMAs this CTA committed finish before the tensor memory is released
-        for (int b = 0; b < 2; ++b) mbar_wait(&bar[b], ph[b]);
     }
     tc_before_sync();
     __syncthreads();
+    if (tid == 0 && *abort_flag) atomicExch(a.err, 1);
     if (warp == 0) {
         tc_after_sync();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");

@@ -21,6 +21,8 @@
 // Channel counts are padded to multiples of 8 (16-byte rows for the tensor cores);
 // the padding channels hold zeros and their weights stay zero.
 #include <cublas_v2.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -238,11 +240,15 @@ struct djb_nn {
     float* dcol = nullptr;                     // [nvox][27·Cmax] (training only)
     float* dA = nullptr;                       // [nvox][Cmax]
     __nv_bfloat16* dY = nullptr;               // [nvox][Cmax]
+    __nv_bfloat16* dY2 = nullptr;              // [nvox][Cmax] (the next layer's, ping-pong)
     float* outm = nullptr;                     // [cout][nvox] float32
     double* lsum = nullptr;
     int* derr = nullptr;                       // set by a tensor-core convolution whose wait ran out
     int conv_mode = 0;                         // 0: tensor-core convolutions where possible; 1: im2col
-    bool have_col = false;                     // col and Y allocated
+    bool tma = true;                           // interior planes by bulk tensor copy
+    bool tma_used = false;                     // a plane map was accepted by the driver
+    bool work_train = false;                   // work areas sized for training
+    bool work_im2col = false;                  // work areas hold the im2col buffers
     std::vector<void*> work;
 };
 
@@ -270,10 +276,12 @@ void free_work(djb_nn* h) {
     for (auto& a : h->act) a = nullptr;
     h->col = nullptr;
     h->Y = nullptr;
-    h->have_col = false;
+    h->work_train = false;
+    h->work_im2col = false;
     h->dcol = nullptr;
     h->dA = nullptr;
     h->dY = nullptr;
+    h->dY2 = nullptr;
     h->outm = nullptr;
     h->res = 0;
 }
@@ -293,12 +301,40 @@ bool any_im2col(const djb_nn* h) {
     return false;
 }
 
-template <int CC, int N, bool LAST>
+// Tensor map of a bf16 [res]^3 × (8·cc) channels-last activation as the 5-D tensor
+// [z][chunk][y][x][8] with boxes of one staged plane (10 × 18 positions, all chunks).
+// false when the driver does not accept it (the kernel then copies every plane with
+// cp.async).
+bool plane_map(CUtensorMap* m, const __nv_bfloat16* X, int res, int cc) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && fn)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        cudaGetLastError();
+    }
+    if (!encode) return false;
+    using namespace djb::conv;
+    const cuuint64_t r = cuuint64_t(res), row = cuuint64_t(cc) * 16;
+    const cuuint64_t dims[5] = {8, r, r, cuuint64_t(cc), r};
+    const cuuint64_t strides[4] = {row, r * row, 16, r * r * row};
+    const cuuint32_t box[5] = {8, cuuint32_t(kBX), cuuint32_t(kBY), cuuint32_t(cc), 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(X), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int CC, int N, int MODE>
 int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
     using namespace djb::conv;
     constexpr int KC = (CC + 1) / 2 * 2;
     constexpr int bytes = smem_bytes<KC, N>();
-    auto kern = k_conv3_tc<CC, N, LAST>;
+    auto kern = k_conv3_tc<CC, N, MODE>;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int occ = 0, sms = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, bytes));
@@ -314,28 +350,38 @@ int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
     while (a.zlen > 4 && int64_t(a.ntx) * a.nty * ((a.res + a.zlen - 1) / a.zlen) < 4 * slots)
         a.zlen = (a.zlen + 1) / 2;
     a.nzs = (a.res + a.zlen - 1) / a.zlen;
+    CUtensorMap map{};
+    a.use_tma = h->tma && a.res >= kBY && plane_map(&map, a.X, a.res, CC) ? 1 : 0;
+    h->tma_used = h->tma_used || a.use_tma;
     const int64_t items = int64_t(a.ntx) * a.nty * a.nzs;
     const int grid = int(std::min<int64_t>(items, slots));
-    kern<<<grid, kThreads, bytes, st>>>(a);
+    kern<<<grid, kThreads, bytes, st>>>(a, map);
     CUDA_TRY(cudaGetLastError());
     return DJB_OK;
 }
 
-template <int N, bool LAST>
+template <int N, int MODE>
 int launch_tc_cc(djb_nn* h, int cc, const djb::conv::Args& a, cudaStream_t st) {
     switch (cc) {
-        case 1: return launch_tc_inst<1, N, LAST>(h, a, st);
-        case 2: return launch_tc_inst<2, N, LAST>(h, a, st);
-        case 3: return launch_tc_inst<3, N, LAST>(h, a, st);
-        case 4: return launch_tc_inst<4, N, LAST>(h, a, st);
+        case 1: return launch_tc_inst<1, N, MODE>(h, a, st);
+        case 2: return launch_tc_inst<2, N, MODE>(h, a, st);
+        case 3: return launch_tc_inst<3, N, MODE>(h, a, st);
+        case 4: return launch_tc_inst<4, N, MODE>(h, a, st);
         default: return fail(DJB_ERR_INVALID, "tensor-core convolution: %d input channels", cc * 8);
     }
 }
 
+template <int MODE>
+int launch_tc(djb_nn* h, const djb::conv::Args& a) {
+    const int cc = a.cin / 8;
+    return a.cout <= 16 ? launch_tc_cc<16, MODE>(h, cc, a, h->stream) : launch_tc_cc<32, MODE>(h, cc, a, h->stream);
+}
+
 // Layer l on the tensor cores: act[l] → act[l + 1] (hidden) or outm (last).
 int conv_tc(djb_nn* h, int l) {
+    using namespace djb::conv;
     const bool last = (l == h->layers - 1);
-    djb::conv::Args a{};
+    Args a{};
     a.X = h->act[l];
     a.W = h->pb + h->woff[l];
     a.bias = h->p + h->boff[l];
@@ -346,10 +392,25 @@ int conv_tc(djb_nn* h, int l) {
     a.cout = h->coutp[l];
     a.nout = h->cout[l];
     a.err = h->derr;
-    const int cc = h->cinp[l] / 8;
-    const bool n16 = h->coutp[l] <= 16;
-    if (last) return n16 ? launch_tc_cc<16, true>(h, cc, a, h->stream) : launch_tc_cc<32, true>(h, cc, a, h->stream);
-    return n16 ? launch_tc_cc<16, false>(h, cc, a, h->stream) : launch_tc_cc<32, false>(h, cc, a, h->stream);
+    return last ? launch_tc<kLast>(h, a) : launch_tc<kHidden>(h, a);
+}
+
+// Data gradient of layer l > 0 on the tensor cores: dY (bf16 [v][coutp]) → the next
+// dY down, (act[l] > 0) · Σ_tap Σ_o dY[v − offset(tap)][o] W[tap][c][o] (bf16 [v][cinp]).
+int conv_tc_back(djb_nn* h, int l, const __nv_bfloat16* dy, __nv_bfloat16* dy_next) {
+    using namespace djb::conv;
+    Args a{};
+    a.X = dy;
+    a.W = h->pb + h->woff[l];
+    a.M = h->act[l];
+    a.Y = dy_next;
+    a.res = h->res;
+    a.cin = h->coutp[l];
+    a.cout = h->cinp[l];
+    a.nout = h->cinp[l];
+    a.flip = 1;
+    a.err = h->derr;
+    return launch_tc<kBackData>(h, a);
 }
 
 // Reads the device error word of the tensor-core convolutions (after a stream sync).
@@ -365,11 +426,12 @@ int check_derr(djb_nn* h) {
 }
 
 // Work areas for res³ voxels; training needs the whole mesh at once (chunk = nvox).
+// The im2col buffers exist only for what runs on that path: the weight gradients (col),
+// and layers that do not fit the tensor-core kernel (col, Y, and dcol when training).
 int ensure_work(djb_nn* h, int res, bool train) {
     const int64_t nvox = int64_t(res) * res * res;
-    const bool need_train = train && !h->dcol;
-    const bool need_col = (train || any_im2col(h)) && !h->have_col;
-    if (h->res == res && !need_train && !need_col) return DJB_OK;
+    const bool im2col = any_im2col(h);
+    if (h->res == res && (h->work_train || !train) && (h->work_im2col || !im2col)) return DJB_OK;
     free_work(h);
     const int C = cmax(h);
     // chunks of whole z planes holding at most 4 Mi voxels (col: 27·C bf16 per voxel,
@@ -379,18 +441,19 @@ int ensure_work(djb_nn* h, int res, bool train) {
     h->chunk = train ? nvox : planes * res * res;
     for (int l = 0; l < h->layers; ++l)
         TRYN(dalloc(h, (void**)&h->act[l], size_t(nvox) * h->cinp[l] * sizeof(__nv_bfloat16), true));
-    if (train || any_im2col(h)) {
+    if (train || im2col)
         TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
-        TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
-        h->have_col = true;
-    }
+    if (im2col) TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
     TRYN(dalloc(h, (void**)&h->outm, size_t(nvox) * h->cout[h->layers - 1] * sizeof(float), true));
     TRYN(dalloc(h, (void**)&h->lsum, sizeof(double), true));
     if (train) {
-        TRYN(dalloc(h, (void**)&h->dcol, size_t(nvox) * 27 * C * sizeof(float), true));
+        if (im2col) TRYN(dalloc(h, (void**)&h->dcol, size_t(nvox) * 27 * C * sizeof(float), true));
         TRYN(dalloc(h, (void**)&h->dA, size_t(nvox) * C * sizeof(float), true));
         TRYN(dalloc(h, (void**)&h->dY, size_t(nvox) * C * sizeof(__nv_bfloat16), true));
+        TRYN(dalloc(h, (void**)&h->dY2, size_t(nvox) * C * sizeof(__nv_bfloat16), true));
     }
+    h->work_train = train;
+    h->work_im2col = im2col;
     h->res = res;
     return DJB_OK;
 }
@@ -402,7 +465,7 @@ int forward(djb_nn* h, const float* in) {
     const float one = 1.0f, zero = 0.0f;
     k_pack<<<grid_of(nvox * h->cinp[0]), kNT, 0, h->stream>>>(in, h->cin[0], h->cinp[0], nvox, 0, nvox, h->act[0]);
     for (int l = 0; l < h->layers; ++l) {
-        if (use_tc(h, l)) {
+            if (use_tc(h, l)) {
             TRYN(conv_tc(h, l));
             continue;
         }
@@ -438,26 +501,34 @@ int backward(djb_nn* h, const float* target, double* loss) {
     CUDA_TRY(cudaMemsetAsync(h->lsum, 0, sizeof(double), h->stream));
     k_mse<<<grid_of(nvox * nout), kNT, 0, h->stream>>>(h->outm, target, nout, nvox, 1.0 / double(nvox * nout), h->dA,
                                                       h->lsum);
+    // dY of the last layer (bf16, [v][coutp], no activation)
+    __nv_bfloat16* dy = h->dY;
+    __nv_bfloat16* dy_next = h->dY2;
+    k_grad_bf16<<<grid_of(nvox * h->coutp[L - 1]), kNT, 0, h->stream>>>(h->dA, nout, h->coutp[L - 1], nullptr, nvox,
+                                                                       dy);
     for (int l = L - 1; l >= 0; --l) {
         const int C = h->cinp[l], K = 27 * C;
         const int N = h->coutp[l];
         const int n = (l == L - 1) ? nout : h->cout[l];
-        // dY (bf16, [v][N]); the ReLU mask of this layer's output
-        const __nv_bfloat16* A = (l == L - 1) ? nullptr : h->act[l + 1];
-        k_grad_bf16<<<grid_of(nvox * N), kNT, 0, h->stream>>>(h->dA, (l == L - 1) ? nout : N, N, A, nvox, h->dY);
-        k_bias_grad<<<grid_of(nvox), kNT, 0, h->stream>>>(h->dY, n, N, nvox, h->g + h->boff[l]);
+        k_bias_grad<<<grid_of(nvox), kNT, 0, h->stream>>>(dy, n, N, nvox, h->g + h->boff[l]);
         k_im2col<<<grid_of(nvox * 27 * (C / 8)), kNT, 0, h->stream>>>(h->act[l], res, C, 0, nvox, h->col);
         // dWᶜ (N×K) = dYᶜ (N×M) · colᶜᵀ (M×K)
-        CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, N, K, int(nvox), &one, h->dY, CUDA_R_16BF, N,
+        CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, N, K, int(nvox), &one, dy, CUDA_R_16BF, N,
                                 h->col, CUDA_R_16BF, K, &zero, h->g + h->woff[l], CUDA_R_32F, N, CUBLAS_COMPUTE_32F,
                                 CUBLAS_GEMM_DEFAULT));
-        if (l > 0) {
+        if (l == 0) break;
+        // dY of layer l − 1: the data gradient of this layer, masked by ReLU'(act[l])
+        if (use_tc(h, l)) {
+            TRYN(conv_tc_back(h, l, dy, dy_next));
+        } else {
             // dcolᶜ (K×M) = Wᶜᵀ (K×N) · dYᶜ (N×M)
             CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, K, int(nvox), N, &one, h->pb + h->woff[l],
-                                    CUDA_R_16BF, N, h->dY, CUDA_R_16BF, N, &zero, h->dcol, CUDA_R_32F, K,
+                                    CUDA_R_16BF, N, dy, CUDA_R_16BF, N, &zero, h->dcol, CUDA_R_32F, K,
                                     CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
             k_col2im<<<grid_of(nvox * C), kNT, 0, h->stream>>>(h->dcol, res, C, nvox, h->dA);
+            k_grad_bf16<<<grid_of(nvox * C), kNT, 0, h->stream>>>(h->dA, C, C, h->act[l], nvox, dy_next);
         }
+        std::swap(dy, dy_next);
     }
     if (loss) {
         double s = 0.0;

@@ -137,3 +137,26 @@ def test_tensor_core_convolution_matches_im2col_and_torch(djb, res):
     ws, bs = _torch_net(net, p)
     r = _torch_forward(ws, bs, x).detach().numpy()
     assert np.max(np.abs(out_tc - r)) < NN_TOL * np.max(np.abs(r))
+
+
+def test_tensor_core_backward_matches_im2col(djb):
+    """Weight and bias gradients with the data gradients on the tensor cores (flipped,
+    transposed weights, ReLU mask fused) against the im2col + cuBLAS backward."""
+    from djb200.nn import ForceNet
+    rng = np.random.default_rng(3)
+    res = 20
+    x = rng.standard_normal((4, res, res, res)).astype(np.float32)
+    t = rng.standard_normal((3, res, res, res)).astype(np.float32)
+    with ForceNet(layers=4, cin=4, hidden=32, cout=3, seed=9) as net:
+        l_tc = net.backward(x, t)
+        g_tc = net.grads()
+        net.set_conv("im2col")
+        l_ref = net.backward(x, t)
+        g_ref = net.grads()
+    assert abs(l_tc - l_ref) < 1e-3 * l_ref
+    for (woff, wshape, boff, op, ci, co) in net.layout():
+        n = int(np.prod(wshape))
+        gw, gw_ref = g_tc[woff:woff + n], g_ref[woff:woff + n]
+        assert np.max(np.abs(gw - gw_ref)) < 2e-2 * np.max(np.abs(gw_ref))
+        gb, gb_ref = g_tc[boff:boff + op], g_ref[boff:boff + op]
+        assert np.max(np.abs(gb - gb_ref)) < 2e-2 * np.max(np.abs(gb_ref))
