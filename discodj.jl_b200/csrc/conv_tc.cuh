@@ -41,7 +41,13 @@ namespace conv {
 constexpr int kTX = 8, kTY = 16;                       // tile: 8 × 16 voxels = 128 MMA rows
 constexpr int kBX = kTX + 2, kBY = kTY + 2;            // staged plane with its halo
 constexpr int kPlane = kBX * kBY;                      // 180 positions
-constexpr int kRing = 8;                               // staged planes
+#ifndef DJB_CONV_RING
+#define DJB_CONV_RING 8
+#endif
+#ifndef DJB_CONV_CTAS
+#define DJB_CONV_CTAS 1
+#endif
+constexpr int kRing = DJB_CONV_RING;                   // staged planes
 constexpr int kAcc = 4;                                // accumulators in tensor memory
 constexpr int kLoaderWarp = 4, kMmaWarp = 5;
 constexpr int kThreads = 192;
@@ -85,6 +91,25 @@ __device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t a, uint64_t b,
         " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(dtmem),
         "l"(a), "l"(b), "r"(id), "r"(acc)
         : "memory");
+}
+
+// The same with the descriptors as (low, high) words: the start address lives in the
+// low word, so per-tap offsets are 32-bit adds.
+__device__ __forceinline__ void mma_bf16_w(uint32_t dtmem, uint32_t alo, uint32_t ahi, uint32_t blo, uint32_t bhi,
+                                           uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n .reg .b64 da, db;\n setp.ne.b32 p, %6, 0;\n"
+        " mov.b64 da, {%1, %2};\n mov.b64 db, {%3, %4};\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], da, db, %5, p;\n}" ::"r"(dtmem),
+        "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(id), "r"(acc)
+        : "memory");
+}
+
+// One lane of the (converged) warp.
+__device__ __forceinline__ bool elect_one() {
+    uint32_t e;
+    asm volatile("{\n .reg .pred p;\n elect.sync _|p, 0xffffffff;\n selp.u32 %0, 1, 0, p;\n}" : "=r"(e));
+    return e != 0;
 }
 
 // Arrives on `bar` once every MMA this thread issued before has completed.
@@ -163,7 +188,7 @@ __device__ __forceinline__ Item item_of(const Args& a, int item) {
 }
 
 template <int CC, int N, int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
     k_conv3_tc(const __grid_constant__ Args a, const __grid_constant__ CUtensorMap tmap) {
     constexpr int KC = (CC + 1) / 2 * 2;          // K chunks staged (K a multiple of 16)
     constexpr uint32_t kCols = kAcc * N < 32 ? 32 : kAcc * N;
@@ -276,29 +301,32 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (uint32_t q = k - n; q < k; ++q) mbar_wait(&full[q % kRing], (q / kRing) & 1u);
         }
     } else if (warp == kMmaWarp) {
-        // ── MMA issue (one thread) ──────────────────────────────────────────────
-        if (lane == 0) {
-            const uint32_t id = idesc<N>();
-            const uint64_t adesc0 = sdesc(ring, kPlane * 16, kBX * 16);
-            const uint64_t bdesc0 = sdesc(ws_u, N * 16, 128);
-            uint32_t kp = 0, t = 0;
-            bool ok = true;
-            for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
-                const Item it = item_of(a, item);
-                const uint32_t base = kp;
-                for (int i = 0; i < it.nt; ++i, ++t) {
-                    const uint32_t b = t % kAcc;
-                    ok = role_wait(&acce[b], ((t / kAcc) & 1u) ^ 1u, abort_flag);
-                    for (int j = (i == 0 ? 0 : i + 2); ok && j <= i + 2; ++j) {
-                        const uint32_t p = base + uint32_t(j);
-                        ok = role_wait(&full[p % kRing], (p / kRing) & 1u, abort_flag);
-                    }
-                    if (!ok) break;
-                    tc_after_sync();
-                    const uint32_t d = tmem + b * N;
+        // ── MMA issue: the warp runs the loop (uniform), one elected lane issues ──
+        const uint32_t id = idesc<N>();
+        const uint64_t adesc0 = sdesc(ring, kPlane * 16, kBX * 16);
+        const uint64_t bdesc0 = sdesc(ws_u, N * 16, 128);
+        const uint32_t alo0 = uint32_t(adesc0), ahi = uint32_t(adesc0 >> 32);
+        const uint32_t blo0 = uint32_t(bdesc0), bhi = uint32_t(bdesc0 >> 32);
+        uint32_t kp = 0, t = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+            const Item it = item_of(a, item);
+            const uint32_t base = kp;
+            for (int i = 0; i < it.nt; ++i, ++t) {
+                const uint32_t b = t % kAcc;
+                ok = role_wait(&acce[b], ((t / kAcc) & 1u) ^ 1u, abort_flag);
+                for (int j = (i == 0 ? 0 : i + 2); ok && j <= i + 2; ++j) {
+                    const uint32_t p = base + uint32_t(j);
+                    ok = role_wait(&full[p % kRing], (p / kRing) & 1u, abort_flag);
+                }
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+                tc_after_sync();
+                const uint32_t d = tmem + b * N;
+                if (elect_one()) {
 #pragma unroll 1
                     for (int dz = 0; dz < 3; ++dz) {
-                        const uint64_t ad = adesc0 + (((base + i + dz) % kRing) * kSlot >> 4);
+                        const uint32_t alo = alo0 + ((((base + i + dz) % kRing) * kSlot) >> 4);
 #pragma unroll
                         for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
@@ -306,23 +334,28 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                                 for (int s = 0; s < KC / 2; ++s) {
                                     const int tap = dz * 9 + dy * 3 + dx;
-                                    mma_bf16(d, ad + uint64_t(((2 * s * kPlane + dy * kBX + dx) * 16) >> 4),
-                                             bdesc0 + uint64_t(((tap * KC + 2 * s) * N * 16) >> 4), id,
-                                             (dz | dy | dx | s) != 0 ? 1u : 0u);
+                                    mma_bf16_w(d, alo + uint32_t(((2 * s * kPlane + dy * kBX + dx) * 16) >> 4), ahi,
+                                               blo0 + uint32_t(((tap * KC + 2 * s) * N * 16) >> 4), bhi, id,
+                                               (dz | dy | dx | s) != 0 ? 1u : 0u);
                                 }
                     }
                     mma_commit(&accf[b]);
                     mma_commit(&empty[(base + i) % kRing]);   // tile i is the last reader of plane i
                 }
-                if (!ok) break;
+                __syncwarp();
+            }
+            if (!ok) break;
+            if (elect_one()) {
                 mma_commit(&empty[(base + it.nt) % kRing]);
                 mma_commit(&empty[(base + it.nt + 1) % kRing]);
-                kp = base + it.nt + 2;
             }
-            // every MMA has completed before the tensor memory is released
-            mma_commit(fin);
-            mbar_wait(fin, 0);
+            __syncwarp();
+            kp = base + it.nt + 2;
         }
+        // every MMA has completed before the tensor memory is released
+        if (elect_one()) mma_commit(fin);
+        __syncwarp();
+        mbar_wait(fin, 0);
     } else {
         // ── epilogue (warps 0-3: tensor-memory lanes 32·warp .. +31) ───────────────
         const uint32_t lane_base = uint32_t(warp * 32) << 16;

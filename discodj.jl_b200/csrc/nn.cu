@@ -160,14 +160,36 @@ __global__ void k_grad_bf16(const float* __restrict__ dA, int n, int np, const _
     }
 }
 
-// db[c] += Σ_v dY[v][c] (bf16 [v][np], c < n)
+// db[c] += Σ_v dY[v][c] (bf16 [v][np], c < n, np a multiple of 8): thread t of a block
+// sums the 8-channel chunk t % (np/8) of every (blockDim / (np/8))-th voxel of a
+// grid-stride run; the block's partial sums meet in shared memory and leave with one
+// atomic per channel.
 __global__ void k_bias_grad(const __nv_bfloat16* __restrict__ dY, int n, int np, int64_t m, float* __restrict__ db) {
-    for (int c = 0; c < n; ++c) {
-        float acc = 0.0f;
-        for (int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < m; v += int64_t(gridDim.x) * blockDim.x)
-            acc += __bfloat162float(dY[v * np + c]);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(db + c, acc);
+    __shared__ float part[kNT][8];
+    const int chunks = np / 8;
+    const int vpb = kNT / chunks;                       // voxels per block and pass
+    const int c8 = threadIdx.x % chunks, r = threadIdx.x / chunks;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (r < vpb) {
+        for (int64_t v = int64_t(blockIdx.x) * vpb + r; v < m; v += int64_t(gridDim.x) * vpb) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(dY + v * np) + c8);
+            const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&w[j]);
+                acc[2 * j] += __bfloat162float(h.x);
+                acc[2 * j + 1] += __bfloat162float(h.y);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) part[threadIdx.x][j] = acc[j];
+    __syncthreads();
+    if (int(threadIdx.x) < n) {
+        const int c = threadIdx.x, ch = c / 8, j = c % 8;
+        float s = 0.0f;
+        for (int q = 0; q < vpb; ++q) s += part[q * chunks + ch][j];
+        atomicAdd(db + c, s);
     }
 }
 
@@ -510,7 +532,8 @@ int backward(djb_nn* h, const float* target, double* loss) {
         const int C = h->cinp[l], K = 27 * C;
         const int N = h->coutp[l];
         const int n = (l == L - 1) ? nout : h->cout[l];
-        k_bias_grad<<<grid_of(nvox), kNT, 0, h->stream>>>(dy, n, N, nvox, h->g + h->boff[l]);
+        k_bias_grad<<<int(std::min<int64_t>((nvox + 255) / 256, 148 * 4)), kNT, 0, h->stream>>>(dy, n, N, nvox,
+                                                                                              h->g + h->boff[l]);
         k_im2col<<<grid_of(nvox * 27 * (C / 8)), kNT, 0, h->stream>>>(h->act[l], res, C, 0, nvox, h->col);
         // dWᶜ (N×K) = dYᶜ (N×M) · colᶜᵀ (M×K)
         CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, N, K, int(nvox), &one, dy, CUDA_R_16BF, N,
@@ -679,6 +702,14 @@ int djb_nn_set_conv(djb_nn* h, int32_t mode) {
     if (!h) return fail(DJB_ERR_INVALID, "null argument");
     if (mode != 0 && mode != 1) return fail(DJB_ERR_INVALID, "conv mode must be 0 (tensor-core) or 1 (im2col)");
     h->conv_mode = mode;
+    return DJB_OK;
+}
+
+int djb_nn_get_conv(const djb_nn* h, int32_t* mode, int32_t* tma_used) {
+    djb::clear_error();
+    if (!h || !mode || !tma_used) return fail(DJB_ERR_INVALID, "null argument");
+    *mode = h->conv_mode;
+    *tma_used = h->tma_used ? 1 : 0;
     return DJB_OK;
 }
 

@@ -53,6 +53,7 @@ class PMConfigC(C.Structure):
 _P = C.c_void_p
 _D = C.c_double
 _I = C.c_int32
+_IP = C.POINTER(C.c_int32)
 _DP = C.POINTER(C.c_double)
 _I64P = C.POINTER(C.c_int64)
 
@@ -96,6 +97,7 @@ SIGNATURES = {
     "djb_nn_load": [_P, _P],
     "djb_nn_set_stream": [_P, _P],
     "djb_nn_set_conv": [_P, _I],
+    "djb_nn_get_conv": [_P, _IP, _IP],
     "djb_nn_apply": [_P, _P, _I, _P, _I],
     "djb_nn_train_step": [_P, _P, _P, _I, _D, _DP, _I],
     "djb_nn_backward": [_P, _P, _P, _I, _DP, _I],

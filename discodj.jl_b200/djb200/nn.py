@@ -69,6 +69,13 @@ class ForceNet:
             raise ValueError(f"conv mode must be one of {sorted(modes)}")
         check(lib.djb_nn_set_conv(self._h, modes[mode]))
 
+    def conv_info(self) -> dict:
+        """{"mode": "tensor" | "im2col", "tma": bool}: the convolution path and whether
+        the tensor-core kernel has staged planes by bulk tensor copies."""
+        mode, tma = C.c_int32(), C.c_int32()
+        check(lib.djb_nn_get_conv(self._h, C.byref(mode), C.byref(tma)))
+        return {"mode": "im2col" if mode.value else "tensor", "tma": bool(tma.value)}
+
     def get_params(self) -> np.ndarray:
         p = np.empty(self.n_params, dtype=np.float32)
         check(lib.djb_nn_get_params(self._h, C.c_void_p(p.ctypes.data)))
@@ -157,3 +164,34 @@ def force_correction_pair(cosmo, *, n=64, boxsize=250.0, res=128, a=1.0, seed=0,
                   device=device) as hi:
         fh = hi.mesh_fields(psi)[1:, ::2, ::2, ::2].contiguous()
     return x, (fh - x[1:]).contiguous()
+
+
+def _main(argv=None):
+    """Forward passes (and optionally Adam steps) of the 4-layer, 32-channel network on
+    a seeded random res³ input, for profiling: python -m djb200.nn --res 256."""
+    import argparse
+
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--res", type=int, default=256)
+    ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--conv", default="tensor", choices=["tensor", "im2col"])
+    ap.add_argument("--train", action="store_true", help="Adam steps instead of forward passes")
+    args = ap.parse_args(argv)
+    gen = torch.Generator(device="cuda:0").manual_seed(11)
+    r = args.res
+    with ForceNet(layers=4, cin=4, hidden=32, cout=3, seed=0) as net:
+        net.set_conv(args.conv)
+        x = torch.randn((4, r, r, r), generator=gen, device="cuda:0")
+        t = torch.randn((3, r, r, r), generator=gen, device="cuda:0") if args.train else None
+        for _ in range(args.repeat):
+            if args.train:
+                net.train_step(x, t, lr=1e-4)
+            else:
+                net.apply(x)
+        torch.cuda.synchronize()
+        print(net.conv_info())
+
+
+if __name__ == "__main__":
+    _main()

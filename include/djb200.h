@@ -239,6 +239,9 @@ DJB_API int djb_nn_set_stream(djb_nn* h, void* stream);
  * forward convolutions whose padded channel counts are at most 32 (others, and the
  * backward pass, use im2col + cuBLAS GEMMs); 1 = im2col + cuBLAS for every layer. */
 DJB_API int djb_nn_set_conv(djb_nn* h, int32_t mode);
+/* The convolution path in use; *tma_used = 1 once a tensor-core convolution has staged
+ * planes by bulk tensor copies (the driver accepted the plane tensor map). */
+DJB_API int djb_nn_get_conv(const djb_nn* h, int32_t* mode, int32_t* tma_used);
 /* out = net(in); large meshes are processed in chunks of z planes. */
 DJB_API int djb_nn_apply(djb_nn* h, const float* in, int32_t res, float* out, int32_t mem);
 /* Gradients of the mean squared error of net(in) against target into the network's
