@@ -177,7 +177,8 @@ struct Item {
     int x0, y0, z0, nt;
 };
 
-__device__ __forceinline__ Item item_of(const Args& a, int item) {
+template <class A>
+__device__ __forceinline__ Item item_of(const A& a, int item) {
     const int tx = item % a.ntx, rr = item / a.ntx, ty = rr % a.nty, zs = rr / a.nty;
     Item it;
     it.x0 = tx * kTX;
@@ -417,6 +418,307 @@ __global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
                     }
                 }
             }
+        }
+    }
+    tc_before_sync();
+    __syncthreads();
+    if (tid == 0 && *abort_flag) atomicExch(a.err, 1);
+    if (warp == 0) {
+        tc_after_sync();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+    }
+}
+
+
+// ── weight gradient ─────────────────────────────────────────────────────────────
+// dW[tap][c][o] = Σ_v X[v + offset(tap)][c] · dY[v][o] for 32 input channels.
+// The operand trick: four consecutive staged planes, [slot][chunk][position][8], have
+// their 8-channel groups evenly spaced (slot stride = 4 × chunk stride), so one
+// MN-major A operand of 128 rows = (slot, channel) covers them all, with K = the 16
+// voxels of two tile rows read at a (dy, dx) position shift. B = the dY tile,
+// [chunk][voxel][8] (MN-major). A tile whose planes z − 1, z, z + 1 sit in slots
+// r, r + 1, r + 2 (mod 4) accumulates, in rows of slot r + dz, the tap dz (the fourth
+// slot's rows are discarded, and may be refilled while they are read). One
+// accumulator per (dx, r): 12 × N columns of tensor memory, so the three dy are three
+// passes over the mesh. After each pass the rows are reduced in shared memory and
+// added to dW with one float atomic per entry and CTA.
+
+constexpr int kWRing = 4;                  // exactly four slots: the A operand spans them
+constexpr int kWgSmemMin = 116 * 1024;     // one CTA per SM (its tensor memory is 512 columns)
+
+struct WArgs {
+    const __nv_bfloat16* X;   // [nvox][32]
+    const __nv_bfloat16* dY;  // [nvox][cout] (cout = 8·CCO)
+    float* dW;                // [27][32][cout], accumulated with atomics
+    int res, cout;
+    int ntx, nty, nzs, zlen;
+    int use_tma;              // plane map (X) and tile map (dY) accepted
+    int* err;
+};
+
+template <int N>
+constexpr int wg_smem_bytes() {
+    const int b = kWRing * 4 * kPlane * 16 + 2 * N * 128 * 2 + 9 * 32 * N * 4 + (2 * kWRing + 2 * 2 + 3) * 8 + 16;
+    return b < kWgSmemMin ? kWgSmemMin : b;
+}
+
+template <int N>
+__device__ __forceinline__ uint32_t idesc_mn() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | (uint32_t(N >> 3) << 17) |
+           (uint32_t(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void bar_epi() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// Barrier of the four epilogue warps that returns whether any of them passed true.
+__device__ __forceinline__ bool bar_epi_or(bool v) {
+    uint32_t r;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, 128, q;\n"
+                 " selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(r)
+                 : "r"(v ? 1u : 0u)
+                 : "memory");
+    return r != 0;
+}
+
+template <int CCO, int N>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_conv3_wgrad(const __grid_constant__ WArgs a, const __grid_constant__ CUtensorMap xmap,
+                  const __grid_constant__ CUtensorMap ymap) {
+    constexpr int CC = 4;
+    constexpr uint32_t kSlot = CC * kPlane * 16;            // 11520 = 4 × the chunk stride
+    constexpr uint32_t kYBuf = N * 128 * 2;                 // [N/8][128 voxels][8]
+    constexpr uint32_t kCols = 12 * N <= 256 ? 256 : 512;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* ringp = smem;
+    uint8_t* ybufp = ringp + kWRing * kSlot;
+    float* dws = reinterpret_cast<float*>(ybufp + 2 * kYBuf);   // [9 (dz, dx)][32][N]
+    uint64_t* fullx = reinterpret_cast<uint64_t*>(dws + 9 * 32 * N);
+    uint64_t* emptyx = fullx + kWRing;
+    uint64_t* fully = emptyx + kWRing;
+    uint64_t* emptyy = fully + 2;
+    uint64_t* accf = emptyy + 2;
+    uint64_t* acce = accf + 1;
+    uint64_t* fin = acce + 1;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t ring = smem_u32(ringp), ybuf = smem_u32(ybufp);
+
+    // dY channel padding (chunks CCO .. N/8 − 1) is zero for good
+    if constexpr (N / 8 > CCO) {
+        for (int i = tid; i < 2 * (N / 8 - CCO) * 128; i += kThreads) {
+            const int v = i % 128, r = i / 128, kc = CCO + r % (N / 8 - CCO), b = r / (N / 8 - CCO);
+            *reinterpret_cast<uint4*>(ybufp + size_t(b) * kYBuf + size_t(kc * 128 + v) * 16) = make_uint4(0, 0, 0, 0);
+        }
+    }
+    if (tid == 0) {
+        for (int i = 0; i < kWRing; ++i) {
+            mbar_init(&fullx[i], 32);
+            mbar_init(&emptyx[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&fully[i], 32);
+            mbar_init(&emptyy[i], 1);
+        }
+        mbar_init(accf, 1);
+        mbar_init(acce, 4);
+        mbar_init(fin, 1);
+        *abort_flag = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_proxy_async_smem();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *tslot;
+    const int items = a.ntx * a.nty * a.nzs;
+
+    if (warp == kLoaderWarp) {
+        uint32_t kx = 0, ky = 0;
+        bool ok = true;
+        auto load_plane = [&](const Item& it, int j, bool interior) -> bool {
+            const int slot = int(kx % kWRing);
+            if (!role_wait(&emptyx[slot], ((kx / kWRing) & 1u) ^ 1u, abort_flag)) return false;
+            const int gz = wrap(it.z0 - 1 + j, a.res);
+            const uint32_t dst = ring + uint32_t(slot) * kSlot;
+            if (interior) {
+                if (lane == 0) {
+                    mbar_arrive_expect_tx(&fullx[slot], kSlot);
+                    tma_load_5d(dst, &xmap, 0, it.x0 - 1, it.y0 - 1, 0, gz, &fullx[slot]);
+                } else {
+                    mbar_arrive(&fullx[slot]);
+                }
+            } else {
+                for (int e = lane; e < CC * kPlane; e += 32) {
+                    const int pos = e / CC, kc = e - pos * CC;
+                    const int by = pos / kBX, bx = pos - by * kBX;
+                    const int gy = wrap(it.y0 - 1 + by, a.res), gx = wrap(it.x0 - 1 + bx, a.res);
+                    cp_async16(dst + uint32_t((kc * kPlane + pos) * 16),
+                               a.X + ((int64_t(gz) * a.res + gy) * a.res + gx) * (CC * 8) + kc * 8);
+                }
+                cp_async_arrive(&fullx[slot]);
+            }
+            ++kx;
+            return true;
+        };
+        auto load_dy = [&](const Item& it, int i) -> bool {
+            const int b = int(ky % 2);
+            if (!role_wait(&emptyy[b], ((ky / 2) & 1u) ^ 1u, abort_flag)) return false;
+            const uint32_t dst = ybuf + uint32_t(b) * kYBuf;
+            const int z = it.z0 + i;
+            if (a.use_tma) {
+                if (lane == 0) {
+                    mbar_arrive_expect_tx(&fully[b], uint32_t(CCO * 128 * 16));
+                    tma_load_5d(dst, &ymap, 0, it.x0, it.y0, 0, z, &fully[b]);
+                } else {
+                    mbar_arrive(&fully[b]);
+                }
+            } else {
+                // voxels outside the mesh contribute nothing: zero rows
+                for (int e = lane; e < CCO * 128; e += 32) {
+                    const int v = e / CCO, kc = e - v * CCO;
+                    const int x = it.x0 + (v & 7), y = it.y0 + (v >> 3);
+                    const uint32_t d = dst + uint32_t((kc * 128 + v) * 16);
+                    if (x < a.res && y < a.res)
+                        cp_async16(d, a.dY + ((int64_t(z) * a.res + y) * a.res + x) * (CCO * 8) + kc * 8);
+                    else
+                        asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(d), "r"(0) : "memory");
+                }
+                fence_proxy_async_smem();
+                cp_async_arrive(&fully[b]);
+            }
+            ++ky;
+            return true;
+        };
+        for (int pass = 0; pass < 3 && ok; ++pass)
+            for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+                const Item it = item_of(a, item);
+                const bool interior = a.use_tma && it.x0 >= 1 && it.x0 - 1 + kBX <= a.res && it.y0 >= 1 &&
+                                      it.y0 - 1 + kBY <= a.res;
+                for (int i = 0; i < it.nt && ok; ++i) {
+                    if (i == 0) ok = load_plane(it, 0, interior) && load_plane(it, 1, interior);
+                    ok = ok && load_plane(it, i + 2, interior) && load_dy(it, i);
+                }
+            }
+        cp_async_wait_all();
+        if (!ok) {
+            for (uint32_t q = kx > kWRing ? kx - kWRing : 0; q < kx; ++q) mbar_wait(&fullx[q % kWRing], (q / kWRing) & 1u);
+            for (uint32_t q = ky > 2 ? ky - 2 : 0; q < ky; ++q) mbar_wait(&fully[q % 2], (q / 2) & 1u);
+        }
+    } else if (warp == kMmaWarp) {
+        const uint32_t id = idesc_mn<N>();
+        // A: M groups (slot, chunk) every 2880 bytes, K groups (tile rows) every 160
+        const uint64_t ad0 = sdesc(ring, kBX * 16, kPlane * 16);
+        // B: N groups every 128 voxels, K groups every 8 voxels
+        const uint64_t bd0 = sdesc(ybuf, 128, 128 * 16);
+        const uint32_t alo0 = uint32_t(ad0), ahi = uint32_t(ad0 >> 32);
+        const uint32_t blo0 = uint32_t(bd0), bhi = uint32_t(bd0 >> 32);
+        uint32_t kx = 0, ky = 0;
+        bool ok = true;
+        for (int pass = 0; pass < 3 && ok; ++pass) {
+            const int dy = pass;
+            bool used[4] = {false, false, false, false};
+            if (pass > 0) {
+                ok = __all_sync(0xffffffffu, role_wait(acce, (pass - 1) & 1, abort_flag));
+                if (!ok) break;
+                tc_after_sync();
+            }
+            for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+                const Item it = item_of(a, item);
+                const uint32_t base = kx;
+                for (int i = 0; i < it.nt; ++i, ++ky) {
+                    bool w = role_wait(&fully[ky % 2], (ky / 2) & 1u, abort_flag);
+                    for (int j = (i == 0 ? 0 : i + 2); w && j <= i + 2; ++j) {
+                        const uint32_t p = base + uint32_t(j);
+                        w = role_wait(&fullx[p % kWRing], (p / kWRing) & 1u, abort_flag);
+                    }
+                    ok = __all_sync(0xffffffffu, w);
+                    if (!ok) break;
+                    tc_after_sync();
+                    const int r = int((base + i) % kWRing);
+                    const uint32_t yb = blo0 + (((ky % 2) * kYBuf) >> 4);
+                    if (elect_one()) {
+#pragma unroll
+                        for (int dx = 0; dx < 3; ++dx) {
+                            const uint32_t d = tmem + uint32_t((dx * 4 + r) * N);
+#pragma unroll
+                            for (int s = 0; s < 8; ++s)
+                                mma_bf16_w(d, alo0 + uint32_t((((dy + 2 * s) * kBX + dx) * 16) >> 4), ahi,
+                                           yb + uint32_t((s * 256) >> 4), bhi, id, (used[r] || s > 0) ? 1u : 0u);
+                        }
+                        mma_commit(&emptyx[(base + i) % kWRing]);   // tile i is the last reader of plane i
+                        mma_commit(&emptyy[ky % 2]);
+                    }
+                    __syncwarp();
+                    used[r] = true;
+                }
+                if (!ok) break;
+                if (elect_one()) {
+                    mma_commit(&emptyx[(base + it.nt) % kWRing]);
+                    mma_commit(&emptyx[(base + it.nt + 1) % kWRing]);
+                }
+                __syncwarp();
+                kx = base + it.nt + 2;
+            }
+            if (!ok) break;
+            if (elect_one()) mma_commit(accf);
+            __syncwarp();
+        }
+        if (elect_one()) mma_commit(fin);
+        __syncwarp();
+        mbar_wait(fin, 0);
+    } else {
+        // ── epilogue: warps 0-3, row tid = (slot, channel) ─────────────────────────
+        const uint32_t lane_base = uint32_t(warp * 32) << 16;
+        const int slot = tid >> 5, c = tid & 31;
+        // planes per pass: the MMA role's plane counter runs on across passes
+        uint32_t per_pass = 0;
+        for (int item = blockIdx.x; item < items; item += gridDim.x) per_pass += uint32_t(item_of(a, item).nt + 2);
+        for (int pass = 0; pass < 3; ++pass) {
+            // the accumulator sets (slot of plane z − 1) this CTA touched in the pass
+            bool used[4] = {false, false, false, false};
+            uint32_t kx = uint32_t(pass) * per_pass;
+            for (int item = blockIdx.x; item < items; item += gridDim.x) {
+                const Item it = item_of(a, item);
+                for (int i = 0; i < it.nt; ++i) used[(kx + i) % kWRing] = true;
+                kx += it.nt + 2;
+            }
+            const bool w = role_wait(accf, pass & 1, abort_flag);
+            if (bar_epi_or(!w || *abort_flag)) break;
+            tc_after_sync();
+            for (int e = tid; e < 9 * 32 * N; e += 128) dws[e] = 0.0f;
+            bar_epi();
+            for (int dx = 0; dx < 3; ++dx)
+                for (int r = 0; r < 4; ++r) {
+                    if (!used[r]) continue;
+                    uint32_t v[N];
+#pragma unroll
+                    for (int q = 0; q < N / 16; ++q)
+                        tmem_ld16(tmem + lane_base + uint32_t((dx * 4 + r) * N + q * 16), v + q * 16);
+                    tmem_wait_ld();
+                    const int dz = (slot - r + 4) & 3;
+                    if (dz < 3) {
+                        float* row = dws + size_t((dz * 3 + dx) * 32 + c) * N;
+#pragma unroll
+                        for (int o = 0; o < N; ++o) row[o] += __uint_as_float(v[o]);
+                    }
+                    bar_epi();   // another slot's rows meet the same (dz, c) at the next r
+                }
+            tc_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acce);
+            for (int e = tid; e < 9 * 32 * N; e += 128) {
+                const int o = e % N, rest = e / N, cc = rest % 32, tz = rest / 32;   // tz = dz·3 + dx
+                if (o >= a.cout) continue;
+                const int tap = (tz / 3) * 9 + pass * 3 + tz % 3;
+                atomicAdd(a.dW + (size_t(tap) * 32 + cc) * a.cout + o, dws[e]);
+            }
+            bar_epi();
         }
     }
     tc_before_sync();

@@ -324,10 +324,10 @@ bool any_im2col(const djb_nn* h) {
 }
 
 // Tensor map of a bf16 [res]^3 × (8·cc) channels-last activation as the 5-D tensor
-// [z][chunk][y][x][8] with boxes of one staged plane (10 × 18 positions, all chunks).
-// false when the driver does not accept it (the kernel then copies every plane with
-// cp.async).
-bool plane_map(CUtensorMap* m, const __nv_bfloat16* X, int res, int cc) {
+// [z][chunk][y][x][8] with boxes of bx × by positions of one plane, all chunks (a
+// staged plane with its halo: 10 × 18; a dY tile: 8 × 16). false when the driver does
+// not accept it (the kernels then copy with cp.async).
+bool act_map(CUtensorMap* m, const __nv_bfloat16* X, int res, int cc, int bx, int by) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static bool tried = false;
     if (!tried) {
@@ -344,7 +344,7 @@ bool plane_map(CUtensorMap* m, const __nv_bfloat16* X, int res, int cc) {
     const cuuint64_t r = cuuint64_t(res), row = cuuint64_t(cc) * 16;
     const cuuint64_t dims[5] = {8, r, r, cuuint64_t(cc), r};
     const cuuint64_t strides[4] = {row, r * row, 16, r * r * row};
-    const cuuint32_t box[5] = {8, cuuint32_t(kBX), cuuint32_t(kBY), cuuint32_t(cc), 1};
+    const cuuint32_t box[5] = {8, cuuint32_t(bx), cuuint32_t(by), cuuint32_t(cc), 1};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     return encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(X), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -373,7 +373,7 @@ int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
         a.zlen = (a.zlen + 1) / 2;
     a.nzs = (a.res + a.zlen - 1) / a.zlen;
     CUtensorMap map{};
-    a.use_tma = h->tma && a.res >= kBY && plane_map(&map, a.X, a.res, CC) ? 1 : 0;
+    a.use_tma = h->tma && a.res >= kBY && act_map(&map, a.X, a.res, CC, kBX, kBY) ? 1 : 0;
     h->tma_used = h->tma_used || a.use_tma;
     const int64_t items = int64_t(a.ntx) * a.nty * a.nzs;
     const int grid = int(std::min<int64_t>(items, slots));
@@ -433,6 +433,61 @@ int conv_tc_back(djb_nn* h, int l, const __nv_bfloat16* dy, __nv_bfloat16* dy_ne
     a.flip = 1;
     a.err = h->derr;
     return launch_tc<kBackData>(h, a);
+}
+
+template <int CCO, int N>
+int launch_wg_inst(djb_nn* h, const djb::conv::WArgs& a0) {
+    using namespace djb::conv;
+    constexpr int bytes = wg_smem_bytes<N>();
+    auto kern = k_conv3_wgrad<CCO, N>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    WArgs a = a0;
+    a.ntx = (a.res + kTX - 1) / kTX;
+    a.nty = (a.res + kTY - 1) / kTY;
+    a.zlen = a.res;
+    while (a.zlen > 4 && int64_t(a.ntx) * a.nty * ((a.res + a.zlen - 1) / a.zlen) < 4 * int64_t(sms))
+        a.zlen = (a.zlen + 1) / 2;
+    a.nzs = (a.res + a.zlen - 1) / a.zlen;
+    CUtensorMap xmap{}, ymap{};
+    a.use_tma = h->tma && a.res >= kBY && act_map(&xmap, a.X, a.res, 4, kBX, kBY) &&
+                        act_map(&ymap, a.dY, a.res, CCO, kTX, kTY)
+                    ? 1
+                    : 0;
+    h->tma_used = h->tma_used || a.use_tma;
+    const int64_t items = int64_t(a.ntx) * a.nty * a.nzs;
+    const int grid = int(std::min<int64_t>(items, sms));
+    kern<<<grid, kThreads, bytes, h->stream>>>(a, xmap, ymap);
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+// Layer l's weight gradient on the tensor cores (32 input channels), accumulated into
+// the zeroed gradient buffer.
+bool use_tc_wgrad(const djb_nn* h, int l) { return use_tc(h, l) && h->cinp[l] == 32; }
+
+int conv_tc_wgrad(djb_nn* h, int l, const __nv_bfloat16* dy) {
+    djb::conv::WArgs a{};
+    a.X = h->act[l];
+    a.dY = dy;
+    a.dW = h->g + h->woff[l];
+    a.res = h->res;
+    a.cout = h->coutp[l];
+    a.err = h->derr;
+    const int cco = h->coutp[l] / 8;
+    if (h->coutp[l] <= 16) {
+        switch (cco) {
+            case 1: return launch_wg_inst<1, 16>(h, a);
+            case 2: return launch_wg_inst<2, 16>(h, a);
+        }
+    } else {
+        switch (cco) {
+            case 3: return launch_wg_inst<3, 32>(h, a);
+            case 4: return launch_wg_inst<4, 32>(h, a);
+        }
+    }
+    return fail(DJB_ERR_INVALID, "tensor-core weight gradient: %d output channels", h->coutp[l]);
 }
 
 // Reads the device error word of the tensor-core convolutions (after a stream sync).
@@ -534,11 +589,15 @@ int backward(djb_nn* h, const float* target, double* loss) {
         const int n = (l == L - 1) ? nout : h->cout[l];
         k_bias_grad<<<int(std::min<int64_t>((nvox + 255) / 256, 148 * 4)), kNT, 0, h->stream>>>(dy, n, N, nvox,
                                                                                               h->g + h->boff[l]);
-        k_im2col<<<grid_of(nvox * 27 * (C / 8)), kNT, 0, h->stream>>>(h->act[l], res, C, 0, nvox, h->col);
-        // dWᶜ (N×K) = dYᶜ (N×M) · colᶜᵀ (M×K)
-        CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, N, K, int(nvox), &one, dy, CUDA_R_16BF, N,
-                                h->col, CUDA_R_16BF, K, &zero, h->g + h->woff[l], CUDA_R_32F, N, CUBLAS_COMPUTE_32F,
-                                CUBLAS_GEMM_DEFAULT));
+        if (use_tc_wgrad(h, l)) {
+            TRYN(conv_tc_wgrad(h, l, dy));
+        } else {
+            k_im2col<<<grid_of(nvox * 27 * (C / 8)), kNT, 0, h->stream>>>(h->act[l], res, C, 0, nvox, h->col);
+            // dWᶜ (N×K) = dYᶜ (N×M) · colᶜᵀ (M×K)
+            CUBLAS_TRY(cublasGemmEx(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, N, K, int(nvox), &one, dy, CUDA_R_16BF, N,
+                                    h->col, CUDA_R_16BF, K, &zero, h->g + h->woff[l], CUDA_R_32F, N,
+                                    CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT));
+        }
         if (l == 0) break;
         // dY of layer l − 1: the data gradient of this layer, masked by ReLU'(act[l])
         if (use_tc(h, l)) {

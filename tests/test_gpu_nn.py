@@ -139,12 +139,14 @@ def test_tensor_core_convolution_matches_im2col_and_torch(djb, res):
     assert np.max(np.abs(out_tc - r)) < NN_TOL * np.max(np.abs(r))
 
 
-def test_tensor_core_backward_matches_im2col(djb):
-    """Weight and bias gradients with the data gradients on the tensor cores (flipped,
-    transposed weights, ReLU mask fused) against the im2col + cuBLAS backward."""
+@pytest.mark.parametrize("res", [20, 40])
+def test_tensor_core_backward_matches_im2col(djb, res):
+    """Weight, bias and data gradients on the tensor cores (data gradients with the
+    flipped, transposed weights and the ReLU mask fused; weight gradients from four
+    staged planes as one 128-row operand, three passes) against the im2col + cuBLAS
+    backward; at 40³ interior planes arrive by bulk tensor copies."""
     from djb200.nn import ForceNet
-    rng = np.random.default_rng(3)
-    res = 20
+    rng = np.random.default_rng(res)
     x = rng.standard_normal((4, res, res, res)).astype(np.float32)
     t = rng.standard_normal((3, res, res, res)).astype(np.float32)
     with ForceNet(layers=4, cin=4, hidden=32, cout=3, seed=9) as net:
