@@ -432,19 +432,21 @@ __global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
 
 // ── weight gradient ─────────────────────────────────────────────────────────────
 // dW[tap][c][o] = Σ_v X[v + offset(tap)][c] · dY[v][o] for 32 input channels.
-// The operand trick: four consecutive staged planes, [slot][chunk][position][8], have
-// their 8-channel groups evenly spaced (slot stride = 4 × chunk stride), so one
-// MN-major A operand of 128 rows = (slot, channel) covers them all, with K = the 16
-// voxels of two tile rows read at a (dy, dx) position shift. B = the dY tile,
-// [chunk][voxel][8] (MN-major). A tile whose planes z − 1, z, z + 1 sit in slots
-// r, r + 1, r + 2 (mod 4) accumulates, in rows of slot r + dz, the tap dz (the fourth
-// slot's rows are discarded, and may be refilled while they are read). One
-// accumulator per (dx, r): 12 × N columns of tensor memory, so the three dy are three
-// passes over the mesh. After each pass the rows are reduced in shared memory and
-// added to dW with one float atomic per entry and CTA.
+// The operand trick: in the staged layout [slot][chunk][position][8] the 8-channel
+// groups of consecutive slots are evenly spaced (slot stride = 4 × chunk stride), so
+// one MN-major A operand of 128 rows = (4 slots, 32 channels) covers four consecutive
+// planes, with K = the 16 voxels of two tile rows read at a (dy, dx) position shift.
+// B = the dY tile, [chunk][voxel][8] (MN-major). The ring holds kWRing planes and
+// repeats its first three slots after its end (a plane landing in slot s < 3 is also
+// copied to slot kWRing + s), so the window starting at the slot of plane z − 1 is
+// always contiguous: rows of window slot q accumulate the tap dz = q − 1 (q = 3, the
+// plane after, is discarded and may still be landing). One accumulator per (dy, dx):
+// 9 × N columns of tensor memory, one pass over the mesh. At the end every row (tap,
+// channel) is added to dW with float atomics (one per entry and CTA).
 
-constexpr int kWRing = 4;                  // exactly four slots: the A operand spans them
-constexpr int kWgSmemMin = 116 * 1024;     // one CTA per SM (its tensor memory is 512 columns)
+constexpr int kWRing = 8;                  // planes in the ring
+constexpr int kWMirror = 3;                // slots repeated after the ring's end
+constexpr int kWY = 4;                     // dY tile buffers
 
 struct WArgs {
     const __nv_bfloat16* X;   // [nvox][32]
@@ -458,26 +460,13 @@ struct WArgs {
 
 template <int N>
 constexpr int wg_smem_bytes() {
-    const int b = kWRing * 4 * kPlane * 16 + 2 * N * 128 * 2 + 9 * 32 * N * 4 + (2 * kWRing + 2 * 2 + 3) * 8 + 16;
-    return b < kWgSmemMin ? kWgSmemMin : b;
+    return (kWRing + kWMirror) * 4 * kPlane * 16 + kWY * N * 128 * 2 + (2 * kWRing + 2 * kWY + 2) * 8 + 16;
 }
 
 template <int N>
 __device__ __forceinline__ uint32_t idesc_mn() {
     return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | (uint32_t(N >> 3) << 17) |
            (uint32_t(128 >> 4) << 24);
-}
-
-__device__ __forceinline__ void bar_epi() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-// Barrier of the four epilogue warps that returns whether any of them passed true.
-__device__ __forceinline__ bool bar_epi_or(bool v) {
-    uint32_t r;
-    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, 128, q;\n"
-                 " selp.u32 %0, 1, 0, p;\n}"
-                 : "=r"(r)
-                 : "r"(v ? 1u : 0u)
-                 : "memory");
-    return r != 0;
 }
 
 template <int CCO, int N>
@@ -487,18 +476,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr int CC = 4;
     constexpr uint32_t kSlot = CC * kPlane * 16;            // 11520 = 4 × the chunk stride
     constexpr uint32_t kYBuf = N * 128 * 2;                 // [N/8][128 voxels][8]
-    constexpr uint32_t kCols = 12 * N <= 256 ? 256 : 512;
+    constexpr uint32_t kCols = 9 * N <= 256 ? 256 : 512;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* ringp = smem;
-    uint8_t* ybufp = ringp + kWRing * kSlot;
-    float* dws = reinterpret_cast<float*>(ybufp + 2 * kYBuf);   // [9 (dz, dx)][32][N]
-    uint64_t* fullx = reinterpret_cast<uint64_t*>(dws + 9 * 32 * N);
+    uint8_t* ybufp = ringp + (kWRing + kWMirror) * kSlot;
+    uint64_t* fullx = reinterpret_cast<uint64_t*>(ybufp + kWY * kYBuf);
     uint64_t* emptyx = fullx + kWRing;
     uint64_t* fully = emptyx + kWRing;
-    uint64_t* emptyy = fully + 2;
-    uint64_t* accf = emptyy + 2;
-    uint64_t* acce = accf + 1;
-    uint64_t* fin = acce + 1;
+    uint64_t* emptyy = fully + kWY;
+    uint64_t* accf = emptyy + kWY;
+    uint64_t* fin = accf + 1;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -506,7 +493,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     // dY channel padding (chunks CCO .. N/8 − 1) is zero for good
     if constexpr (N / 8 > CCO) {
-        for (int i = tid; i < 2 * (N / 8 - CCO) * 128; i += kThreads) {
+        for (int i = tid; i < kWY * (N / 8 - CCO) * 128; i += kThreads) {
             const int v = i % 128, r = i / 128, kc = CCO + r % (N / 8 - CCO), b = r / (N / 8 - CCO);
             *reinterpret_cast<uint4*>(ybufp + size_t(b) * kYBuf + size_t(kc * 128 + v) * 16) = make_uint4(0, 0, 0, 0);
         }
@@ -516,12 +503,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&fullx[i], 32);
             mbar_init(&emptyx[i], 1);
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kWY; ++i) {
             mbar_init(&fully[i], 32);
             mbar_init(&emptyy[i], 1);
         }
         mbar_init(accf, 1);
-        mbar_init(acce, 4);
         mbar_init(fin, 1);
         *abort_flag = 0;
     }
@@ -545,11 +531,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int slot = int(kx % kWRing);
             if (!role_wait(&emptyx[slot], ((kx / kWRing) & 1u) ^ 1u, abort_flag)) return false;
             const int gz = wrap(it.z0 - 1 + j, a.res);
+            const bool mirror = slot < kWMirror;
             const uint32_t dst = ring + uint32_t(slot) * kSlot;
+            const uint32_t dst2 = ring + uint32_t(kWRing + slot) * kSlot;
             if (interior) {
                 if (lane == 0) {
-                    mbar_arrive_expect_tx(&fullx[slot], kSlot);
+                    mbar_arrive_expect_tx(&fullx[slot], mirror ? 2 * kSlot : kSlot);
                     tma_load_5d(dst, &xmap, 0, it.x0 - 1, it.y0 - 1, 0, gz, &fullx[slot]);
+                    if (mirror) tma_load_5d(dst2, &xmap, 0, it.x0 - 1, it.y0 - 1, 0, gz, &fullx[slot]);
                 } else {
                     mbar_arrive(&fullx[slot]);
                 }
@@ -558,8 +547,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const int pos = e / CC, kc = e - pos * CC;
                     const int by = pos / kBX, bx = pos - by * kBX;
                     const int gy = wrap(it.y0 - 1 + by, a.res), gx = wrap(it.x0 - 1 + bx, a.res);
-                    cp_async16(dst + uint32_t((kc * kPlane + pos) * 16),
-                               a.X + ((int64_t(gz) * a.res + gy) * a.res + gx) * (CC * 8) + kc * 8);
+                    const __nv_bfloat16* src = a.X + ((int64_t(gz) * a.res + gy) * a.res + gx) * (CC * 8) + kc * 8;
+                    const uint32_t off = uint32_t((kc * kPlane + pos) * 16);
+                    cp_async16(dst + off, src);
+                    if (mirror) cp_async16(dst2 + off, src);
                 }
                 cp_async_arrive(&fullx[slot]);
             }
@@ -567,8 +558,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             return true;
         };
         auto load_dy = [&](const Item& it, int i) -> bool {
-            const int b = int(ky % 2);
-            if (!role_wait(&emptyy[b], ((ky / 2) & 1u) ^ 1u, abort_flag)) return false;
+            const int b = int(ky % kWY);
+            if (!role_wait(&emptyy[b], ((ky / kWY) & 1u) ^ 1u, abort_flag)) return false;
             const uint32_t dst = ybuf + uint32_t(b) * kYBuf;
             const int z = it.z0 + i;
             if (a.use_tma) {
@@ -595,20 +586,19 @@ __global__ void __launch_bounds__(kThreads, 1)
             ++ky;
             return true;
         };
-        for (int pass = 0; pass < 3 && ok; ++pass)
-            for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
-                const Item it = item_of(a, item);
-                const bool interior = a.use_tma && it.x0 >= 1 && it.x0 - 1 + kBX <= a.res && it.y0 >= 1 &&
-                                      it.y0 - 1 + kBY <= a.res;
-                for (int i = 0; i < it.nt && ok; ++i) {
-                    if (i == 0) ok = load_plane(it, 0, interior) && load_plane(it, 1, interior);
-                    ok = ok && load_plane(it, i + 2, interior) && load_dy(it, i);
-                }
+        for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+            const Item it = item_of(a, item);
+            const bool interior = a.use_tma && it.x0 >= 1 && it.x0 - 1 + kBX <= a.res && it.y0 >= 1 &&
+                                  it.y0 - 1 + kBY <= a.res;
+            for (int i = 0; i < it.nt && ok; ++i) {
+                if (i == 0) ok = load_plane(it, 0, interior) && load_plane(it, 1, interior);
+                ok = ok && load_plane(it, i + 2, interior) && load_dy(it, i);
             }
+        }
         cp_async_wait_all();
         if (!ok) {
             for (uint32_t q = kx > kWRing ? kx - kWRing : 0; q < kx; ++q) mbar_wait(&fullx[q % kWRing], (q / kWRing) & 1u);
-            for (uint32_t q = ky > 2 ? ky - 2 : 0; q < ky; ++q) mbar_wait(&fully[q % 2], (q / 2) & 1u);
+            for (uint32_t q = ky > kWY ? ky - kWY : 0; q < ky; ++q) mbar_wait(&fully[q % kWY], (q / kWY) & 1u);
         }
     } else if (warp == kMmaWarp) {
         const uint32_t id = idesc_mn<N>();
@@ -619,106 +609,76 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t alo0 = uint32_t(ad0), ahi = uint32_t(ad0 >> 32);
         const uint32_t blo0 = uint32_t(bd0), bhi = uint32_t(bd0 >> 32);
         uint32_t kx = 0, ky = 0;
-        bool ok = true;
-        for (int pass = 0; pass < 3 && ok; ++pass) {
-            const int dy = pass;
-            bool used[4] = {false, false, false, false};
-            if (pass > 0) {
-                ok = __all_sync(0xffffffffu, role_wait(acce, (pass - 1) & 1, abort_flag));
+        bool ok = true, first = true;
+        for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
+            const Item it = item_of(a, item);
+            const uint32_t base = kx;
+            for (int i = 0; i < it.nt; ++i, ++ky) {
+                bool w = role_wait(&fully[ky % kWY], (ky / kWY) & 1u, abort_flag);
+                for (int j = (i == 0 ? 0 : i + 2); w && j <= i + 2; ++j) {
+                    const uint32_t p = base + uint32_t(j);
+                    w = role_wait(&fullx[p % kWRing], (p / kWRing) & 1u, abort_flag);
+                }
+                ok = __all_sync(0xffffffffu, w);
                 if (!ok) break;
                 tc_after_sync();
-            }
-            for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
-                const Item it = item_of(a, item);
-                const uint32_t base = kx;
-                for (int i = 0; i < it.nt; ++i, ++ky) {
-                    bool w = role_wait(&fully[ky % 2], (ky / 2) & 1u, abort_flag);
-                    for (int j = (i == 0 ? 0 : i + 2); w && j <= i + 2; ++j) {
-                        const uint32_t p = base + uint32_t(j);
-                        w = role_wait(&fullx[p % kWRing], (p / kWRing) & 1u, abort_flag);
-                    }
-                    ok = __all_sync(0xffffffffu, w);
-                    if (!ok) break;
-                    tc_after_sync();
-                    const int r = int((base + i) % kWRing);
-                    const uint32_t yb = blo0 + (((ky % 2) * kYBuf) >> 4);
-                    if (elect_one()) {
+                // window: the slot of plane i (z − 1) and the three after it
+                const uint32_t aw = alo0 + ((((base + i) % kWRing) * kSlot) >> 4);
+                const uint32_t yb = blo0 + (((ky % kWY) * kYBuf) >> 4);
+                if (elect_one()) {
+#pragma unroll
+                    for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
                         for (int dx = 0; dx < 3; ++dx) {
-                            const uint32_t d = tmem + uint32_t((dx * 4 + r) * N);
+                            const uint32_t d = tmem + uint32_t((dy * 3 + dx) * N);
 #pragma unroll
                             for (int s = 0; s < 8; ++s)
-                                mma_bf16_w(d, alo0 + uint32_t((((dy + 2 * s) * kBX + dx) * 16) >> 4), ahi,
-                                           yb + uint32_t((s * 256) >> 4), bhi, id, (used[r] || s > 0) ? 1u : 0u);
+                                mma_bf16_w(d, aw + uint32_t((((dy + 2 * s) * kBX + dx) * 16) >> 4), ahi,
+                                           yb + uint32_t((s * 256) >> 4), bhi, id, (!first || s > 0) ? 1u : 0u);
                         }
-                        mma_commit(&emptyx[(base + i) % kWRing]);   // tile i is the last reader of plane i
-                        mma_commit(&emptyy[ky % 2]);
-                    }
-                    __syncwarp();
-                    used[r] = true;
-                }
-                if (!ok) break;
-                if (elect_one()) {
-                    mma_commit(&emptyx[(base + it.nt) % kWRing]);
-                    mma_commit(&emptyx[(base + it.nt + 1) % kWRing]);
+                    mma_commit(&emptyx[(base + i) % kWRing]);   // tile i is the last reader of plane i
+                    mma_commit(&emptyy[ky % kWY]);
                 }
                 __syncwarp();
-                kx = base + it.nt + 2;
+                first = false;
             }
             if (!ok) break;
-            if (elect_one()) mma_commit(accf);
+            if (elect_one()) {
+                mma_commit(&emptyx[(base + it.nt) % kWRing]);
+                mma_commit(&emptyx[(base + it.nt + 1) % kWRing]);
+            }
             __syncwarp();
+            kx = base + it.nt + 2;
         }
-        if (elect_one()) mma_commit(fin);
+        if (elect_one()) {
+            if (ok) mma_commit(accf);
+            mma_commit(fin);
+        }
         __syncwarp();
         mbar_wait(fin, 0);
     } else {
-        // ── epilogue: warps 0-3, row tid = (slot, channel) ─────────────────────────
+        // ── epilogue: warps 0-3, row tid = (window slot q, channel); q = 3 is discarded ──
         const uint32_t lane_base = uint32_t(warp * 32) << 16;
-        const int slot = tid >> 5, c = tid & 31;
-        // planes per pass: the MMA role's plane counter runs on across passes
-        uint32_t per_pass = 0;
-        for (int item = blockIdx.x; item < items; item += gridDim.x) per_pass += uint32_t(item_of(a, item).nt + 2);
-        for (int pass = 0; pass < 3; ++pass) {
-            // the accumulator sets (slot of plane z − 1) this CTA touched in the pass
-            bool used[4] = {false, false, false, false};
-            uint32_t kx = uint32_t(pass) * per_pass;
-            for (int item = blockIdx.x; item < items; item += gridDim.x) {
-                const Item it = item_of(a, item);
-                for (int i = 0; i < it.nt; ++i) used[(kx + i) % kWRing] = true;
-                kx += it.nt + 2;
-            }
-            const bool w = role_wait(accf, pass & 1, abort_flag);
-            if (bar_epi_or(!w || *abort_flag)) break;
+        const int q = tid >> 5, c = tid & 31;
+        // one wait for the whole run: bounded in rounds of about a second each, ended early
+        // when another role aborts
+        bool w = false;
+        for (int k = 0; k < 120 && !w && !*abort_flag; ++k) w = mbar_wait(accf, 0);
+        if (!w) *abort_flag = 1;
+        if (w) {
             tc_after_sync();
-            for (int e = tid; e < 9 * 32 * N; e += 128) dws[e] = 0.0f;
-            bar_epi();
-            for (int dx = 0; dx < 3; ++dx)
-                for (int r = 0; r < 4; ++r) {
-                    if (!used[r]) continue;
-                    uint32_t v[N];
+            for (int tap9 = 0; tap9 < 9; ++tap9) {   // (dy, dx)
+                uint32_t v[N];
 #pragma unroll
-                    for (int q = 0; q < N / 16; ++q)
-                        tmem_ld16(tmem + lane_base + uint32_t((dx * 4 + r) * N + q * 16), v + q * 16);
-                    tmem_wait_ld();
-                    const int dz = (slot - r + 4) & 3;
-                    if (dz < 3) {
-                        float* row = dws + size_t((dz * 3 + dx) * 32 + c) * N;
+                for (int h = 0; h < N / 16; ++h) tmem_ld16(tmem + lane_base + uint32_t(tap9 * N + h * 16), v + h * 16);
+                tmem_wait_ld();
+                if (q < 3) {
+                    float* dst = a.dW + (size_t(q * 9 + tap9) * 32 + c) * a.cout;
 #pragma unroll
-                        for (int o = 0; o < N; ++o) row[o] += __uint_as_float(v[o]);
-                    }
-                    bar_epi();   // another slot's rows meet the same (dz, c) at the next r
+                    for (int o = 0; o < N; ++o)
+                        if (o < a.cout) atomicAdd(dst + o, __uint_as_float(v[o]));
                 }
-            tc_before_sync();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(acce);
-            for (int e = tid; e < 9 * 32 * N; e += 128) {
-                const int o = e % N, rest = e / N, cc = rest % 32, tz = rest / 32;   // tz = dz·3 + dx
-                if (o >= a.cout) continue;
-                const int tap = (tz / 3) * 9 + pass * 3 + tz % 3;
-                atomicAdd(a.dW + (size_t(tap) * 32 + cc) * a.cout + o, dws[e]);
             }
-            bar_epi();
         }
     }
     tc_before_sync();
