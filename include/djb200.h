@@ -260,11 +260,10 @@ DJB_API int djb_nn_train_step(djb_nn* h, const float* in, const float* target, i
 
 /* ── non-allocating shell sums ──────────────────────────────────────────────
  * No counterpart in the reference. For callers that cannot allocate device
- * memory at the point of the call: code running while a stream is being
- * captured into a CUDA graph (where cudaMalloc is not allowed), applications
- * whose device memory is owned by a pool or an external framework that forbids
- * allocations outside it, and step loops that must not synchronise the device
- * through an allocator. The caller passes the half spectrum of a (res,res,res)
+ * memory at the point of the call: applications whose device memory is owned by
+ * a pool or an external framework that forbids allocations outside it, and step
+ * loops that must not synchronise the device through an allocator (cudaMalloc
+ * and cudaFree can wait for the whole device). The caller passes the half spectrum of a (res,res,res)
  * field (device memory, complex64 [kz][ky][kx], kx in [0, res/2], as an in-place
  * R2C of the x-fastest field produces it) and host outputs k, pk (double) and
  * nmodes (int64) of `bins` entries; scale2 multiplies |delta(k)|^2 (1 for a field

@@ -2,8 +2,9 @@
 entry point `djb_power_spectrum` on the same field, twice in a row (the second call
 reuses the shared scratch left by the first). Collected last on purpose.
 
-Callers that cannot allocate (inside a CUDA-graph capture, or under an external
-memory pool) use this entry point; it must agree with the ordinary one."""
+Callers that cannot allocate (under an external memory pool, or in a step loop that
+must not synchronise through the allocator) use this entry point; it must agree with
+the ordinary one."""
 from __future__ import annotations
 
 import numpy as np
