@@ -48,9 +48,12 @@ constexpr int kPlane = kBX * kBY;                      // 180 positions
 #define DJB_CONV_CTAS 1
 #endif
 constexpr int kRing = DJB_CONV_RING;                   // staged planes
-constexpr int kAcc = 4;                                // accumulators in tensor memory
-constexpr int kLoaderWarp = 4, kMmaWarp = 5;
-constexpr int kThreads = 192;
+constexpr int kAccTiles = 16;                          // tile accumulators in tensor memory
+constexpr int kMaxSegment = kAccTiles;                 // z segment length (tiles) at most
+constexpr int kOneCtaSmem = 116 * 1024;                // more than half an SM: one CTA per SM
+constexpr int kEpiGroups = 2;                          // epilogue groups of four warps, alternate tiles
+constexpr int kLoaderWarp = 4 * kEpiGroups, kMmaWarp = kLoaderWarp + 1;
+constexpr int kThreads = 32 * (kMmaWarp + 1);
 
 enum Mode { kHidden = 0, kLast = 1, kBackData = 2 };
 
@@ -69,7 +72,8 @@ struct Args {
 
 template <int KC, int N>
 constexpr int smem_bytes() {
-    return 27 * KC * N * 16 + kRing * KC * kPlane * 16 + (2 * kRing + 2 * kAcc + 1) * 8 + 16;
+    const int b = 27 * KC * N * 16 + kRing * KC * kPlane * 16 + (2 * kRing + (kEpiGroups + 1) * kAccTiles + 1) * 8 + 16;
+    return b < kOneCtaSmem ? kOneCtaSmem : b;   // the CTA's tensor memory may be all 512 columns
 }
 
 // Shared-memory matrix descriptor, no swizzle: start, leading (K-chunk) and stride
@@ -102,6 +106,26 @@ __device__ __forceinline__ void mma_bf16_w(uint32_t dtmem, uint32_t alo, uint32_
         " mov.b64 da, {%1, %2};\n mov.b64 db, {%3, %4};\n"
         " tcgen05.mma.cta_group::1.kind::f16 [%0], da, db, %5, p;\n}" ::"r"(dtmem),
         "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(id), "r"(acc)
+        : "memory");
+}
+
+// The same, executed by the whole converged warp: one lane, chosen by elect.sync inside
+// the instruction sequence, issues it; the operands stay warp-uniform.
+__device__ __forceinline__ void mma_bf16_warp(uint32_t dtmem, uint32_t alo, uint32_t ahi, uint32_t blo, uint32_t bhi,
+                                              uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p, e;\n .reg .b64 da, db;\n setp.ne.b32 p, %6, 0;\n"
+        " mov.b64 da, {%1, %2};\n mov.b64 db, {%3, %4};\n elect.sync _|e, 0xffffffff;\n"
+        " @e tcgen05.mma.cta_group::1.kind::f16 [%0], da, db, %5, p;\n}" ::"r"(dtmem),
+        "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(id), "r"(acc)
+        : "memory");
+}
+
+// tcgen05.commit by one elected lane of the converged warp.
+__device__ __forceinline__ void mma_commit_warp(uint64_t* bar) {
+    asm volatile(
+        "{\n .reg .pred e;\n elect.sync _|e, 0xffffffff;\n"
+        " @e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n}" ::"r"(smem_u32(bar))
         : "memory");
 }
 
@@ -189,27 +213,28 @@ __device__ __forceinline__ Item item_of(const A& a, int item) {
 }
 
 template <int CC, int N, int MODE>
-__global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
+__global__ void __launch_bounds__(kThreads, 1)
     k_conv3_tc(const __grid_constant__ Args a, const __grid_constant__ CUtensorMap tmap) {
     constexpr int KC = (CC + 1) / 2 * 2;          // K chunks staged (K a multiple of 16)
-    constexpr uint32_t kCols = kAcc * N < 32 ? 32 : kAcc * N;
+    constexpr uint32_t kCols = kAccTiles * N;     // 512 (N = 32) or 256 (N = 16)
     constexpr uint32_t kSlot = KC * kPlane * 16;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* ws = smem;
     uint8_t* ringp = smem + 27 * KC * N * 16;
     uint64_t* full = reinterpret_cast<uint64_t*>(ringp + kRing * kSlot);
     uint64_t* empty = full + kRing;
-    uint64_t* accf = empty + kRing;
-    uint64_t* acce = accf + kAcc;
-    uint64_t* fin = acce + kAcc;
+    uint64_t* accf = empty + kRing;                  // [group][accumulator]
+    uint64_t* acce = accf + kEpiGroups * kAccTiles;
+    uint64_t* fin = acce + kAccTiles;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t ws_u = smem_u32(ws), ring = smem_u32(ringp);
 
-    // weights → [tap][chunk][n][8 k], zeros beyond cin and cout
+    // weights → [shift (dy, dx)][chunk][n = kz·N + o][8 k], zeros beyond cin and cout
     for (int i = tid; i < 27 * KC * N; i += kThreads) {
-        const int n = i % N, kc = (i / N) % KC, tap = i / (N * KC);
+        const int n3 = i % (3 * N), kc = (i / (3 * N)) % KC, shift = i / (3 * N * KC);
+        const int n = n3 % N, tap = (n3 / N) * 9 + shift;
         uint32_t w[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -239,10 +264,8 @@ __global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
             mbar_init(&full[i], 32);
             mbar_init(&empty[i], 1);
         }
-        for (int i = 0; i < kAcc; ++i) {
-            mbar_init(&accf[i], 1);
-            mbar_init(&acce[i], 4);
-        }
+        for (int i = 0; i < kEpiGroups * kAccTiles; ++i) mbar_init(&accf[i], 1);
+        for (int i = 0; i < kAccTiles; ++i) mbar_init(&acce[i], 4);
         mbar_init(fin, 1);
         *abort_flag = 0;
     }
@@ -258,6 +281,9 @@ __global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
     tc_after_sync();
     const uint32_t tmem = *tslot;
     const int items = a.ntx * a.nty * a.nzs;
+    // accumulator of the column segment's tile t (t < zlen ≤ kAccTiles): adjacent tiles
+    // sit in adjacent accumulators, tile t + 1 just below tile t
+    auto acc_of = [&](int t) { return a.zlen - 1 - t; };
 
     if (warp == kLoaderWarp) {
         // ── loader ──────────────────────────────────────────────────────────────
@@ -302,91 +328,117 @@ __global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
             for (uint32_t q = k - n; q < k; ++q) mbar_wait(&full[q % kRing], (q / kRing) & 1u);
         }
     } else if (warp == kMmaWarp) {
-        // ── MMA issue: the warp runs the loop (uniform), one elected lane issues ──
-        const uint32_t id = idesc<N>();
+        // ── MMA issue: per staged plane u (z0 − 1 .. z0 + L), one MMA per (shift, K step)
+        // of N · (tiles it feeds): the plane is the kz = 0, 1, 2 input of tiles u + 1, u,
+        // u − 1, whose accumulators are adjacent; the warp runs the loop, one lane issues.
+        const uint32_t id0 = idesc<0>();   // N field filled in per MMA: (n >> 3) << 17
         const uint64_t adesc0 = sdesc(ring, kPlane * 16, kBX * 16);
-        const uint64_t bdesc0 = sdesc(ws_u, N * 16, 128);
+        const uint64_t bdesc0 = sdesc(ws_u, 3 * N * 16, 128);
         const uint32_t alo0 = uint32_t(adesc0), ahi = uint32_t(adesc0 >> 32);
         const uint32_t blo0 = uint32_t(bdesc0), bhi = uint32_t(bdesc0 >> 32);
-        uint32_t kp = 0, t = 0;
+        uint32_t live[kAccTiles], waited[kAccTiles];   // accf commits / acce completions seen
+        for (int i = 0; i < kAccTiles; ++i) live[i] = waited[i] = 0;
+        uint32_t kp = 0, done = 0;   // planes issued; tiles completed (tile n goes to group n % kEpiGroups)
         bool ok = true;
         for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
             const Item it = item_of(a, item);
+            const int L = it.nt;
             const uint32_t base = kp;
-            for (int i = 0; i < it.nt; ++i, ++t) {
-                const uint32_t b = t % kAcc;
-                ok = role_wait(&acce[b], ((t / kAcc) & 1u) ^ 1u, abort_flag);
-                for (int j = (i == 0 ? 0 : i + 2); ok && j <= i + 2; ++j) {
-                    const uint32_t p = base + uint32_t(j);
-                    ok = role_wait(&full[p % kRing], (p / kRing) & 1u, abort_flag);
+            for (int u = -1; u <= L; ++u) {
+                const uint32_t p = base + uint32_t(u + 1);
+                const int lo = max(u - 1, 0), hi = min(u + 1, L - 1), nv = hi - lo + 1;
+                const bool first = u + 1 <= L - 1;     // tile u + 1 starts here
+                bool w = role_wait(&full[p % kRing], (p / kRing) & 1u, abort_flag);
+                if (w && first) {
+                    const int c = acc_of(u + 1);
+                    if (waited[c] < live[c]) {          // its last tile's epilogue has read it
+                        w = role_wait(&acce[c], waited[c] & 1u, abort_flag);
+                        ++waited[c];
+                    }
                 }
-                ok = __all_sync(0xffffffffu, ok);
+                ok = __all_sync(0xffffffffu, w);
                 if (!ok) break;
                 tc_after_sync();
-                const uint32_t d = tmem + b * N;
-                if (elect_one()) {
-#pragma unroll 1
-                    for (int dz = 0; dz < 3; ++dz) {
-                        const uint32_t alo = alo0 + ((((base + i + dz) % kRing) * kSlot) >> 4);
+                const uint32_t d0 = tmem + uint32_t(acc_of(hi) * N);
+                const int b0 = u + 1 - hi;               // weight block (kz) of tile hi
+                const uint32_t alo = alo0 + (((p % kRing) * kSlot) >> 4);
+                const uint32_t idv = id0 | (uint32_t(nv * N / 8) << 17);
 #pragma unroll
-                        for (int dy = 0; dy < 3; ++dy)
+                for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-                            for (int dx = 0; dx < 3; ++dx)
+                    for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-                                for (int s = 0; s < KC / 2; ++s) {
-                                    const int tap = dz * 9 + dy * 3 + dx;
-                                    mma_bf16_w(d, alo + uint32_t(((2 * s * kPlane + dy * kBX + dx) * 16) >> 4), ahi,
-                                               blo0 + uint32_t(((tap * KC + 2 * s) * N * 16) >> 4), bhi, id,
-                                               (dz | dy | dx | s) != 0 ? 1u : 0u);
-                                }
-                    }
-                    mma_commit(&accf[b]);
-                    mma_commit(&empty[(base + i) % kRing]);   // tile i is the last reader of plane i
-                }
+                        for (int s = 0; s < KC / 2; ++s) {
+                            const int sh = dy * 3 + dx;
+                            const uint32_t av = alo + uint32_t(((2 * s * kPlane + dy * kBX + dx) * 16) >> 4);
+                            const uint32_t bv =
+                                blo0 + uint32_t((((sh * KC + 2 * s) * 3 * N) * 16) >> 4) + uint32_t(b0 * N);
+                            if (sh == 0 && s == 0 && first) {
+                                mma_bf16_warp(d0, av, ahi, bv, bhi, id0 | (uint32_t(N / 8) << 17), 0u);
+                                if (nv > 1)
+                                    mma_bf16_warp(d0 + N, av, ahi, bv + N, bhi, id0 | (uint32_t((nv - 1) * N / 8) << 17),
+                                                  1u);
+                            } else {
+                                mma_bf16_warp(d0, av, ahi, bv, bhi, idv, 1u);
+                            }
+                        }
+                mma_commit_warp(&empty[p % kRing]);
+                if (u >= 1)   // tile u − 1 is complete
+                    mma_commit_warp(&accf[(done % kEpiGroups) * kAccTiles + acc_of(u - 1)]);
                 __syncwarp();
+                if (u >= 1) {
+                    ++live[acc_of(u - 1)];
+                    ++done;
+                }
             }
             if (!ok) break;
-            if (elect_one()) {
-                mma_commit(&empty[(base + it.nt) % kRing]);
-                mma_commit(&empty[(base + it.nt + 1) % kRing]);
-            }
-            __syncwarp();
-            kp = base + it.nt + 2;
+            kp = base + uint32_t(L + 2);
         }
         // every MMA has completed before the tensor memory is released
         if (elect_one()) mma_commit(fin);
         __syncwarp();
         mbar_wait(fin, 0);
     } else {
-        // ── epilogue (warps 0-3: tensor-memory lanes 32·warp .. +31) ───────────────
-        const uint32_t lane_base = uint32_t(warp * 32) << 16;
+        // ── epilogue: group g = warp / 4 takes the CTA's tiles n ≡ g (mod kEpiGroups);
+        // warp w reads tensor-memory lanes 32·(w % 4) .. +31 ──────────────────────────
+        const int g = warp >> 2, row = tid & 127;
+        const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
         const int64_t nvox = int64_t(a.res) * a.res * a.res;
-        uint32_t t = 0;
+        float bias[N];
+#pragma unroll
+        for (int cc = 0; cc < N; ++cc)
+            bias[cc] = (MODE != kBackData && cc < (MODE == kLast ? a.nout : a.cout)) ? __ldg(a.bias + cc) : 0.0f;
+        uint32_t uses[kAccTiles];   // this group's earlier tiles per accumulator
+        for (int i = 0; i < kAccTiles; ++i) uses[i] = 0;
+        uint32_t n = 0;             // the CTA's tiles so far
         bool ok = true;
         for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
             const Item it = item_of(a, item);
-            const int x = it.x0 + (tid & 7), y = it.y0 + (tid >> 3);
+            const int x = it.x0 + (row & 7), y = it.y0 + (row >> 3);
             const bool valid = x < a.res && y < a.res;
-            for (int i = 0; i < it.nt; ++i, ++t) {
-                const uint32_t b = t % kAcc;
-                if (!role_wait(&accf[b], (t / kAcc) & 1u, abort_flag)) {
+            for (int i = 0; i < it.nt; ++i, ++n) {
+                if (int(n % kEpiGroups) != g) continue;
+                const int c = acc_of(i);
+                if (!role_wait(&accf[g * kAccTiles + c], uses[c] & 1u, abort_flag)) {
                     ok = false;
                     break;
                 }
+                ++uses[c];
                 tc_after_sync();
                 uint32_t r[N];
 #pragma unroll
-                for (int q = 0; q < N / 16; ++q) tmem_ld16(tmem + lane_base + b * N + uint32_t(q * 16), r + q * 16);
+                for (int q = 0; q < N / 16; ++q)
+                    tmem_ld16(tmem + lane_base + uint32_t(c * N + q * 16), r + q * 16);
                 tmem_wait_ld();
                 tc_before_sync();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&acce[b]);
+                if (lane == 0) mbar_arrive(&acce[c]);
                 if (!valid) continue;
                 const int64_t v = (int64_t(it.z0 + i) * a.res + y) * a.res + x;
                 if constexpr (MODE == kLast) {
 #pragma unroll
-                    for (int c = 0; c < N; ++c)
-                        if (c < a.nout) a.Yf[int64_t(c) * nvox + v] = __uint_as_float(r[c]) + __ldg(a.bias + c);
+                    for (int cc = 0; cc < N; ++cc)
+                        if (cc < a.nout) a.Yf[int64_t(cc) * nvox + v] = __uint_as_float(r[cc]) + bias[cc];
                 } else {
                     uint4* dst = reinterpret_cast<uint4*>(a.Y + v * a.cout);
                     const uint4* msk = nullptr;
@@ -409,9 +461,9 @@ __global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
                         } else {
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
-                                const int c = c8 * 8 + 2 * j;
-                                w[j] = pack_bf16(fmaxf(__uint_as_float(r[c]) + __ldg(a.bias + c), 0.0f),
-                                                 fmaxf(__uint_as_float(r[c + 1]) + __ldg(a.bias + c + 1), 0.0f));
+                                const int cc = c8 * 8 + 2 * j;
+                                w[j] = pack_bf16(fmaxf(__uint_as_float(r[cc]) + bias[cc], 0.0f),
+                                                 fmaxf(__uint_as_float(r[cc + 1]) + bias[cc + 1], 0.0f));
                             }
                         }
                         dst[c8] = make_uint4(w[0], w[1], w[2], w[3]);
@@ -428,7 +480,6 @@ __global__ void __launch_bounds__(kThreads, DJB_CONV_CTAS)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
     }
 }
-
 
 // ── weight gradient ─────────────────────────────────────────────────────────────
 // dW[tap][c][o] = Σ_v X[v + offset(tap)][c] · dY[v][o] for 32 input channels.
@@ -656,7 +707,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         __syncwarp();
         mbar_wait(fin, 0);
-    } else {
+    } else if (warp < 4) {
         // ── epilogue: warps 0-3, row tid = (window slot q, channel); q = 3 is discarded ──
         const uint32_t lane_base = uint32_t(warp * 32) << 16;
         const int q = tid >> 5, c = tid & 31;

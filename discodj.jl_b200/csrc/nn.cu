@@ -365,12 +365,10 @@ int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
     Args a = a0;
     a.ntx = (a.res + kTX - 1) / kTX;
     a.nty = (a.res + kTY - 1) / kTY;
-    // z segments: whole columns when there are enough of them for every CTA slot four
-    // times over, else shorter segments (each costs two extra planes)
+    // z segments of at most kMaxSegment tiles (one tensor-memory accumulator each); the
+    // two planes beyond a segment's ends feed only its first and last tile
     const int64_t slots = int64_t(occ) * sms;
-    a.zlen = a.res;
-    while (a.zlen > 4 && int64_t(a.ntx) * a.nty * ((a.res + a.zlen - 1) / a.zlen) < 4 * slots)
-        a.zlen = (a.zlen + 1) / 2;
+    a.zlen = std::min(a.res, kMaxSegment);
     a.nzs = (a.res + a.zlen - 1) / a.zlen;
     CUtensorMap map{};
     a.use_tma = h->tma && a.res >= kBY && act_map(&map, a.X, a.res, CC, kBX, kBY) ? 1 : 0;
