@@ -70,9 +70,20 @@ struct Args {
     int* err;                 // set to 1 when a wait runs out
 };
 
-template <int KC, int N>
+// Bytes per staged plane: KC chunks of kPlane 16-byte positions, rounded up to 128 bytes
+// (the alignment of a bulk tensor copy's shared-memory destination; one chunk alone is
+// 2880 bytes, an odd multiple of 64).
+template <int KC>
+__host__ __device__ constexpr uint32_t slot_bytes() {
+    return (uint32_t(KC * kPlane * 16) + 127u) / 128u * 128u;
+}
+
+// Shared memory of k_conv3_tc: weights (27 taps × KC chunks × N rows of 16 bytes, the
+// same for the x-pair form's 3 dy × 2 chunks × 3N), the plane ring, barriers.
+template <int KC, int N, bool PAIR = false>
 constexpr int smem_bytes() {
-    const int b = 27 * KC * N * 16 + kRing * KC * kPlane * 16 + (2 * kRing + (kEpiGroups + 1) * kAccTiles + 1) * 8 + 16;
+    const int w = PAIR ? 3 * 2 * 3 * N * 16 : 27 * KC * N * 16;
+    const int b = w + kRing * int(slot_bytes<KC>()) + (2 * kRing + (kEpiGroups + 1) * kAccTiles + 1) * 8 + 16;
     return b < kOneCtaSmem ? kOneCtaSmem : b;   // the CTA's tensor memory may be all 512 columns
 }
 
@@ -212,15 +223,23 @@ __device__ __forceinline__ Item item_of(const A& a, int item) {
     return it;
 }
 
-template <int CC, int N, int MODE>
+// PAIR: the first layer with at most 4 input channels, staged from the x-pair layout
+// [v][8] = (4 channels of v, 4 channels of v + x̂): one K = 16 step reads the pairs at
+// x − 1 and x + 1 (K chunks 32 bytes apart) and so covers dx = −1, 0, 1 (and a zero
+// weight for dx = 2): three MMAs per plane instead of nine.
+template <int CC, int N, int MODE, bool PAIR = false>
 __global__ void __launch_bounds__(kThreads, 1)
     k_conv3_tc(const __grid_constant__ Args a, const __grid_constant__ CUtensorMap tmap) {
-    constexpr int KC = (CC + 1) / 2 * 2;          // K chunks staged (K a multiple of 16)
+    static_assert(!PAIR || CC == 1, "the x-pair layout has one 16-byte chunk per position");
+    constexpr int KC = PAIR ? 1 : (CC + 1) / 2 * 2;   // chunks staged per position
+    constexpr int NSH = PAIR ? 3 : 9;                  // weight shifts: dy (PAIR) or (dy, dx)
+    constexpr int KW = PAIR ? 2 : KC;                  // weight K chunks per shift
     constexpr uint32_t kCols = kAccTiles * N;     // 512 (N = 32) or 256 (N = 16)
-    constexpr uint32_t kSlot = KC * kPlane * 16;
+    constexpr uint32_t kSlot = slot_bytes<KC>();        // 128-byte aligned plane slots
+    static_assert((NSH * KW * 3 * N * 16) % 128 == 0, "the plane ring starts 128-byte aligned");
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* ws = smem;
-    uint8_t* ringp = smem + 27 * KC * N * 16;
+    uint8_t* ringp = smem + NSH * KW * 3 * N * 16;
     uint64_t* full = reinterpret_cast<uint64_t*>(ringp + kRing * kSlot);
     uint64_t* empty = full + kRing;
     uint64_t* accf = empty + kRing;                  // [group][accumulator]
@@ -231,21 +250,29 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t ws_u = smem_u32(ws), ring = smem_u32(ringp);
 
-    // weights → [shift (dy, dx)][chunk][n = kz·N + o][8 k], zeros beyond cin and cout
-    for (int i = tid; i < 27 * KC * N; i += kThreads) {
-        const int n3 = i % (3 * N), kc = (i / (3 * N)) % KC, shift = i / (3 * N * KC);
-        const int n = n3 % N, tap = (n3 / N) * 9 + shift;
+    // weights → [shift][chunk][n = kz·N + o][8 k], zeros beyond cin and cout; PAIR:
+    // shift = dy, k = chunk·8 + half·4 + channel with dx = chunk·2 + half − 1
+    for (int i = tid; i < NSH * KW * 3 * N; i += kThreads) {
+        const int n3 = i % (3 * N), kc = (i / (3 * N)) % KW, shift = i / (3 * N * KW);
+        const int n = n3 % N, kz = n3 / N;
         uint32_t w[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             float f[2];
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
-                const int k = kc * 8 + 2 * j + u;
+                const int e = 2 * j + u;
                 float v = 0.0f;
-                if (k < a.cin && n < a.cout)
-                    v = __bfloat162float(a.flip ? a.W[(int64_t(26 - tap) * a.cout + n) * a.cin + k]
-                                                : a.W[(int64_t(tap) * a.cin + k) * a.cout + n]);
+                if constexpr (PAIR) {
+                    const int dx = kc * 2 + e / 4 - 1, ch = e % 4;
+                    if (dx <= 1 && n < a.cout)
+                        v = __bfloat162float(a.W[(int64_t(kz * 9 + shift * 3 + dx + 1) * a.cin + ch) * a.cout + n]);
+                } else {
+                    const int k = kc * 8 + e, tap = kz * 9 + shift;
+                    if (k < a.cin && n < a.cout)
+                        v = __bfloat162float(a.flip ? a.W[(int64_t(26 - tap) * a.cout + n) * a.cin + k]
+                                                    : a.W[(int64_t(tap) * a.cin + k) * a.cout + n]);
+                }
                 f[u] = v;
             }
             w[j] = pack_bf16(f[0], f[1]);
@@ -256,7 +283,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     if constexpr (KC > CC) {
         for (int i = tid; i < kRing * (KC - CC) * kPlane; i += kThreads) {
             const int pos = i % kPlane, r = i / kPlane, kc = CC + r % (KC - CC), slot = r / (KC - CC);
-            *reinterpret_cast<uint4*>(ringp + size_t((slot * KC + kc) * kPlane + pos) * 16) = make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(ringp + size_t(slot) * kSlot + size_t(kc * kPlane + pos) * 16) =
+                make_uint4(0, 0, 0, 0);
         }
     }
     if (tid == 0) {
@@ -332,7 +360,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         // of N · (tiles it feeds): the plane is the kz = 0, 1, 2 input of tiles u + 1, u,
         // u − 1, whose accumulators are adjacent; the warp runs the loop, one lane issues.
         const uint32_t id0 = idesc<0>();   // N field filled in per MMA: (n >> 3) << 17
-        const uint64_t adesc0 = sdesc(ring, kPlane * 16, kBX * 16);
+        // A: K chunks kPlane positions apart, or (PAIR) the pair two positions on
+        const uint64_t adesc0 = sdesc(ring, PAIR ? 32 : kPlane * 16, kBX * 16);
         const uint64_t bdesc0 = sdesc(ws_u, 3 * N * 16, 128);
         const uint32_t alo0 = uint32_t(adesc0), ahi = uint32_t(adesc0 >> 32);
         const uint32_t blo0 = uint32_t(bdesc0), bhi = uint32_t(bdesc0 >> 32);
@@ -366,13 +395,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-                    for (int dx = 0; dx < 3; ++dx)
+                    for (int dx = 0; dx < (PAIR ? 1 : 3); ++dx)
 #pragma unroll
-                        for (int s = 0; s < KC / 2; ++s) {
-                            const int sh = dy * 3 + dx;
+                        for (int s = 0; s < (PAIR ? 1 : KC / 2); ++s) {
+                            const int sh = PAIR ? dy : dy * 3 + dx;
                             const uint32_t av = alo + uint32_t(((2 * s * kPlane + dy * kBX + dx) * 16) >> 4);
                             const uint32_t bv =
-                                blo0 + uint32_t((((sh * KC + 2 * s) * 3 * N) * 16) >> 4) + uint32_t(b0 * N);
+                                blo0 + uint32_t((((sh * KW + 2 * s) * 3 * N) * 16) >> 4) + uint32_t(b0 * N);
                             if (sh == 0 && s == 0 && first) {
                                 mma_bf16_warp(d0, av, ahi, bv, bhi, id0 | (uint32_t(N / 8) << 17), 0u);
                                 if (nv > 1)
@@ -526,6 +555,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                   const __grid_constant__ CUtensorMap ymap) {
     constexpr int CC = 4;
     constexpr uint32_t kSlot = CC * kPlane * 16;            // 11520 = 4 × the chunk stride
+    static_assert(kSlot % 128 == 0 && kSlot == slot_bytes<CC>(), "slots 128-byte aligned, no padding");
     constexpr uint32_t kYBuf = N * 128 * 2;                 // [N/8][128 voxels][8]
     constexpr uint32_t kCols = 9 * N <= 256 ? 256 : 512;
     extern __shared__ __align__(1024) uint8_t smem[];

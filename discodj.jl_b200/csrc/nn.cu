@@ -70,13 +70,35 @@ __device__ __forceinline__ int64_t nbr(int x, int y, int z, int dx, int dy, int 
     return (int64_t(z) * res + y) * res + x;
 }
 
-// float32 [c][z][y][x] (c < cin) → bf16 [v][cp] (zeros beyond cin), for voxels [v0, v0 + m).
-__global__ void k_pack(const float* __restrict__ in, int cin, int cp, int64_t nvox, int64_t v0, int64_t m,
-                       __nv_bfloat16* __restrict__ out) {
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m * cp; t += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t v = t / cp;
-        const int c = int(t - v * cp);
-        out[t] = __float2bfloat16_rn(c < cin ? in[int64_t(c) * nvox + v0 + v] : 0.0f);
+// float32 [c][z][y][x] (c < cin) → bf16 [v][cp] (zeros beyond cin, cp a multiple of 8),
+// one voxel per thread. `pair` (cin <= 4, may be null): also the x-pair rows
+// [v][8] = (4 channels of v, 4 channels of its +x neighbour, periodic), the first
+// layer's tensor-core input.
+__global__ void k_pack(const float* __restrict__ in, int cin, int cp, int res, int64_t nvox,
+                       __nv_bfloat16* __restrict__ out, __nv_bfloat16* __restrict__ pair) {
+    for (int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < nvox; v += int64_t(gridDim.x) * blockDim.x) {
+        const int x = int(v % res);
+        const int64_t vn = v - x + (x + 1 == res ? 0 : x + 1);
+        float f[8], g[4];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) f[c] = c < cin ? in[int64_t(c) * nvox + v] : 0.0f;
+        uint4* o = reinterpret_cast<uint4*>(out + v * cp);
+        o[0] = make_uint4(djb::conv::pack_bf16(f[0], f[1]), djb::conv::pack_bf16(f[2], f[3]),
+                          djb::conv::pack_bf16(f[4], f[5]), djb::conv::pack_bf16(f[6], f[7]));
+        for (int c8 = 1; c8 < cp / 8; ++c8) {
+            float h[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) h[j] = c8 * 8 + j < cin ? in[int64_t(c8 * 8 + j) * nvox + v] : 0.0f;
+            o[c8] = make_uint4(djb::conv::pack_bf16(h[0], h[1]), djb::conv::pack_bf16(h[2], h[3]),
+                               djb::conv::pack_bf16(h[4], h[5]), djb::conv::pack_bf16(h[6], h[7]));
+        }
+        if (pair) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) g[c] = c < cin ? in[int64_t(c) * nvox + vn] : 0.0f;
+            reinterpret_cast<uint4*>(pair)[v] =
+                make_uint4(djb::conv::pack_bf16(f[0], f[1]), djb::conv::pack_bf16(f[2], f[3]),
+                           djb::conv::pack_bf16(g[0], g[1]), djb::conv::pack_bf16(g[2], g[3]));
+        }
     }
 }
 
@@ -257,6 +279,7 @@ struct djb_nn {
     int res = 0;
     int64_t chunk = 0;
     __nv_bfloat16* act[kMaxLayers + 1] = {};  // [v][cinp] per layer input (act[L] unused)
+    __nv_bfloat16* act0p = nullptr;            // [v][8] x-pair rows of the input (use_pair)
     __nv_bfloat16* col = nullptr;              // [chunk][27·Cmax]
     float* Y = nullptr;                        // [chunk][Nmax] (also dA)
     float* dcol = nullptr;                     // [nvox][27·Cmax] (training only)
@@ -296,6 +319,7 @@ void free_work(djb_nn* h) {
     for (void* q : h->work) cudaFree(q);
     h->work.clear();
     for (auto& a : h->act) a = nullptr;
+    h->act0p = nullptr;
     h->col = nullptr;
     h->Y = nullptr;
     h->work_train = false;
@@ -351,12 +375,12 @@ bool act_map(CUtensorMap* m, const __nv_bfloat16* X, int res, int cc, int bx, in
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int CC, int N, int MODE>
+template <int CC, int N, int MODE, bool PAIR = false>
 int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
     using namespace djb::conv;
-    constexpr int KC = (CC + 1) / 2 * 2;
-    constexpr int bytes = smem_bytes<KC, N>();
-    auto kern = k_conv3_tc<CC, N, MODE>;
+    constexpr int KC = PAIR ? 1 : (CC + 1) / 2 * 2;
+    constexpr int bytes = smem_bytes<KC, N, PAIR>();
+    auto kern = k_conv3_tc<CC, N, MODE, PAIR>;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int occ = 0, sms = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, bytes));
@@ -397,6 +421,9 @@ int launch_tc(djb_nn* h, const djb::conv::Args& a) {
     return a.cout <= 16 ? launch_tc_cc<16, MODE>(h, cc, a, h->stream) : launch_tc_cc<32, MODE>(h, cc, a, h->stream);
 }
 
+// The first layer reads the x-pair rows (at most 4 input channels, not the last layer).
+bool use_pair(const djb_nn* h) { return use_tc(h, 0) && h->cin[0] <= 4 && h->cinp[0] == 8 && h->layers > 1; }
+
 // Layer l on the tensor cores: act[l] → act[l + 1] (hidden) or outm (last).
 int conv_tc(djb_nn* h, int l) {
     using namespace djb::conv;
@@ -412,6 +439,11 @@ int conv_tc(djb_nn* h, int l) {
     a.cout = h->coutp[l];
     a.nout = h->cout[l];
     a.err = h->derr;
+    if (l == 0 && use_pair(h)) {
+        a.X = h->act0p;
+        return h->coutp[0] <= 16 ? launch_tc_inst<1, 16, kHidden, true>(h, a, h->stream)
+                                 : launch_tc_inst<1, 32, kHidden, true>(h, a, h->stream);
+    }
     return last ? launch_tc<kLast>(h, a) : launch_tc<kHidden>(h, a);
 }
 
@@ -516,6 +548,7 @@ int ensure_work(djb_nn* h, int res, bool train) {
     h->chunk = train ? nvox : planes * res * res;
     for (int l = 0; l < h->layers; ++l)
         TRYN(dalloc(h, (void**)&h->act[l], size_t(nvox) * h->cinp[l] * sizeof(__nv_bfloat16), true));
+    TRYN(dalloc(h, (void**)&h->act0p, size_t(nvox) * 8 * sizeof(__nv_bfloat16), true));
     if (train || im2col)
         TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
     if (im2col) TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
@@ -538,7 +571,8 @@ int forward(djb_nn* h, const float* in) {
     const int res = h->res;
     const int64_t nvox = int64_t(res) * res * res;
     const float one = 1.0f, zero = 0.0f;
-    k_pack<<<grid_of(nvox * h->cinp[0]), kNT, 0, h->stream>>>(in, h->cin[0], h->cinp[0], nvox, 0, nvox, h->act[0]);
+    k_pack<<<grid_of(nvox), kNT, 0, h->stream>>>(in, h->cin[0], h->cinp[0], res, nvox, h->act[0],
+                                                 use_pair(h) ? h->act0p : nullptr);
     for (int l = 0; l < h->layers; ++l) {
             if (use_tc(h, l)) {
             TRYN(conv_tc(h, l));
