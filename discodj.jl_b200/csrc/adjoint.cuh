@@ -70,6 +70,7 @@ __device__ __forceinline__ void particle_stencil(const float* __restrict__ psi, 
     }
 }
 
+// Thread t takes particle perm[t] (or t): brick order keeps the mesh traffic local.
 // f1 == null: Ψ̄_a += scale · Σ_n ∂_a W · f0(n).
 // else:       Ψ̄_a += scale · Σ_c ā_c Σ_n ∂_a W · f_c(n).
 template <int W>
@@ -78,9 +79,11 @@ __global__ void __launch_bounds__(256) k_gather_grad(const float* __restrict__ p
                                                      float sy, float sz, const float* __restrict__ f0,
                                                      const float* __restrict__ f1, const float* __restrict__ f2,
                                                      const float* __restrict__ abar, float scale,
-                                                     float* __restrict__ psibar, int* err) {
-    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= np) return;
+                                                     float* __restrict__ psibar, int* err,
+                                                     const int* __restrict__ perm = nullptr) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int64_t p = perm ? int64_t(perm[t]) : t;
     const float sh[3] = {sx, sy, sz};
     float w[3][W], dw[3][W];
     int idx[3][W];
@@ -113,9 +116,11 @@ __global__ void __launch_bounds__(256) k_scatter_weighted(const float* __restric
                                                           int res, int pitch, float sx, float sy, float sz,
                                                           const float* __restrict__ abar, float scale,
                                                           float* __restrict__ m0, float* __restrict__ m1,
-                                                          float* __restrict__ m2, int* err) {
-    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= np) return;
+                                                          float* __restrict__ m2, int* err,
+                                                          const int* __restrict__ perm = nullptr) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int64_t p = perm ? int64_t(perm[t]) : t;
     const float sh[3] = {sx, sy, sz};
     float w[3][W], dw[3][W];
     int idx[3][W];

@@ -112,13 +112,15 @@ namespace djb {
 // Mass assignment of NS shifted copies of the particles (pm.jl:57-74; interlacing
 // copies as in pm.jl:515-517). When `mom` is non-null the first drift of the
 // step is applied first and written back: Psi <- Psi + dd1*Mom (run_nbody.jl:156).
+// `perm` (optional): thread t takes particle perm[t].
 template <int W, int NS>
 __global__ void __launch_bounds__(kThreads) k_scatter(
     float* __restrict__ psi, const float* __restrict__ mom, float dd1, const float* __restrict__ q1,
     int n, int64_t np, float L, int res, int pitch, GroupShifts sh, float* __restrict__ mesh0,
-    float* __restrict__ mesh1, int* err) {
-    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= np) return;
+    float* __restrict__ mesh1, int* err, const int* __restrict__ perm = nullptr) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int64_t p = perm ? int64_t(perm[t]) : t;   // perm: visit in brick order (local atomics)
     const int i = int(p % n);
     const int j = int((p / n) % n);
     const int k = int(p / (int64_t(n) * n));
@@ -1292,28 +1294,29 @@ int poisson(djb_solver* s, int m) {
 
 template <int W>
 void launch_vjp_kernels(djb_solver* s, int stage, const float* psi, const float* abar, float* psibar,
-                        const Shift3& sh, float scale) {
+                        const Shift3& sh, float scale, const int* perm) {
     float* rho = rho_mesh(s, 0);
     const int pitch = rho_pitch(s);
     const int b = blocks(s->np);
     if (stage == 0)
         djb::k_gather_grad<W><<<b, 256, 0, s->stream>>>(psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y,
                                                          sh.z, s->adj[0], s->adj[1], s->adj[2], abar, scale, psibar,
-                                                         s->err);
+                                                         s->err, perm);
     else if (stage == 1)
         djb::k_scatter_weighted<W><<<b, 256, 0, s->stream>>>(psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x,
                                                               sh.y, sh.z, abar, scale, s->adj[0], s->adj[1],
-                                                              s->adj[2], s->err);
+                                                              s->adj[2], s->err, perm);
     else
         djb::k_gather_grad<W><<<b, 256, 0, s->stream>>>(psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y,
-                                                         sh.z, rho, nullptr, nullptr, nullptr, scale, psibar, s->err);
+                                                         sh.z, rho, nullptr, nullptr, nullptr, scale, psibar, s->err,
+                                                         perm);
 }
 
 void vjp_kernels(djb_solver* s, int stage, const float* psi, const float* abar, float* psibar, const Shift3& sh,
-                 float scale) {
-    if (s->W == 2) launch_vjp_kernels<2>(s, stage, psi, abar, psibar, sh, scale);
-    else if (s->W == 3) launch_vjp_kernels<3>(s, stage, psi, abar, psibar, sh, scale);
-    else launch_vjp_kernels<4>(s, stage, psi, abar, psibar, sh, scale);
+                 float scale, const int* perm) {
+    if (s->W == 2) launch_vjp_kernels<2>(s, stage, psi, abar, psibar, sh, scale, perm);
+    else if (s->W == 3) launch_vjp_kernels<3>(s, stage, psi, abar, psibar, sh, scale, perm);
+    else launch_vjp_kernels<4>(s, stage, psi, abar, psibar, sh, scale, perm);
 }
 
 // psibar += (∂acc/∂Ψ)ᵀ abar at the displacements psi (device arrays, Lagrangian order).
@@ -1326,27 +1329,39 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
     float* rho = rho_mesh(s, 0);
     const int pitch = rho_pitch(s);
     const float inv_ns = 1.0f / float(s->nshift);
+    // visit the particles in brick order (the forward's counting sort on these positions):
+    // the gathers and float atomics below then stay within L2-resident neighbourhoods
+    const int* perm = nullptr;
+    if (s->tiled && s->sorted) {
+        CUDA_TRY(cudaMemsetAsync(s->count, 0, size_t(s->nbins) * sizeof(unsigned), s->stream));
+        djb::k_bin<<<blocks(s->np), 256, 0, s->stream>>>(psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->sg,
+                                                          s->count, s->keyrank, s->err);
+        djb::k_scan_block<<<s->nscan, djb::kScanThreads, 0, s->stream>>>(s->count, s->nbins, s->offset, s->bsum);
+        djb::k_scan_sums<<<1, djb::kScanThreads, 0, s->stream>>>(s->bsum, s->nscan);
+        djb::k_place<<<blocks(s->np), 256, 0, s->stream>>>(s->keyrank, s->np, s->offset, s->bsum, s->perm);
+        perm = s->perm;
+    }
     for (int si = 0; si < s->nshift; ++si) {
         const GroupShifts g = group_shifts(s, si, 1);
         const Shift3 sh = g.s[0];
         CUDA_TRY(cudaMemsetAsync(rho, 0, rho_floats * sizeof(float), s->stream));
         if (s->W == 2) djb::k_scatter<2, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
-            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, perm);
         if (s->W == 3) djb::k_scatter<3, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
-            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, perm);
         if (s->W == 4) djb::k_scatter<4, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
-            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, perm);
         TRY(poisson(s, 0));  // φ
         const int cb = grid_for(int64_t(s->res) * s->res * s->res);
         djb::k_fd_grad3<<<cb, 256, 0, s->stream>>>(rho, s->res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
                                                     s->adj[2]);
-        vjp_kernels(s, 0, psi, abar, psibar, sh, inv_ns);  // interpolation weights
+        vjp_kernels(s, 0, psi, abar, psibar, sh, inv_ns, perm);  // interpolation weights
         for (int c = 0; c < 3; ++c) CUDA_TRY(cudaMemsetAsync(s->adj[c], 0, rho_floats * sizeof(float), s->stream));
-        vjp_kernels(s, 1, psi, abar, psibar, sh, inv_ns);  // Ḡ
+        vjp_kernels(s, 1, psi, abar, psibar, sh, inv_ns, perm);  // Ḡ
         djb::k_fd_div3<<<cb, 256, 0, s->stream>>>(s->adj[0], s->adj[1], s->adj[2], s->res, pitch, s->c1, s->c2,
                                                    s->c3, rho);  // φ̄
         TRY(poisson(s, 0));                                    // ρ̄
-        vjp_kernels(s, 2, psi, abar, psibar, sh, 1.0f);        // deposit weights
+        vjp_kernels(s, 2, psi, abar, psibar, sh, 1.0f, perm);  // deposit weights
     }
     CUDA_TRY(cudaGetLastError());
     return DJB_OK;
