@@ -16,6 +16,7 @@
 
 #include <cstdint>
 
+#include "brick.cuh"
 #include "pm_kernels.cuh"
 
 namespace djb {
@@ -141,59 +142,106 @@ __global__ void __launch_bounds__(256) k_scatter_weighted(const float* __restric
         }
 }
 
+// Both stencil kernels sweep a column of kFdTX × kFdTY cells along z over kFdZ planes:
+// the z stencil from a register window of 2·kFdR + 1 values of the thread's own column,
+// the x and y stencils from the plane's tile with its halo, staged in shared memory.
+constexpr int kFdTX = 32, kFdTY = 8, kFdZ = 32, kFdR = 3;
+
+// Periodic index of any integer (tiles and windows reach past 2·res on small meshes).
+__device__ __forceinline__ int fd_wrap(int v, int res) {
+    v %= res;
+    return v < 0 ? v + res : v;
+}
+
+__device__ __forceinline__ float fd_at(const float* __restrict__ f, int x, int y, int z, int res, int pitch) {
+    return f[(int64_t(fd_wrap(z, res)) * res + fd_wrap(y, res)) * pitch + fd_wrap(x, res)];
+}
+
+// Tile of plane z: rows y0 − hy .. y0 + kFdTY − 1 + hy, columns x0 − hx .. x0 + kFdTX − 1 + hx.
+__device__ __forceinline__ void fd_stage(float* t, const float* __restrict__ f, int x0, int y0, int z, int hx, int hy,
+                                         int res, int pitch) {
+    const int w = kFdTX + 2 * hx, h = kFdTY + 2 * hy;
+    for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
+        const int r = i / w, c = i - r * w;
+        t[i] = fd_at(f, x0 - hx + c, y0 - hy + r, z, res, pitch);
+    }
+}
+
 // g_c = −D_c φ, (D_c f)(n) = Σ_t c_t (f(n + t e_c) − f(n − t e_c)) (pm.jl:330-342).
-__global__ void __launch_bounds__(256) k_fd_grad3(const float* __restrict__ phi, int res, int pitch, float c1,
-                                                  float c2, float c3, float* __restrict__ g0,
-                                                  float* __restrict__ g1, float* __restrict__ g2) {
-    const int64_t total = int64_t(res) * res * res;
-    const float cc[3] = {c1, c2, c3};
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-         t += int64_t(gridDim.x) * blockDim.x) {
-        const int x = int(t % res), y = int((t / res) % res), z = int(t / (int64_t(res) * res));
-        float d[3] = {0.0f, 0.0f, 0.0f};
+__global__ void __launch_bounds__(kFdTX * kFdTY) k_fd_grad3(const float* __restrict__ phi, int res, int pitch,
+                                                             float c1, float c2, float c3, float* __restrict__ g0,
+                                                             float* __restrict__ g1, float* __restrict__ g2) {
+    __shared__ float tile[(kFdTY + 2 * kFdR) * (kFdTX + 2 * kFdR)];
+    const float cc[kFdR] = {c1, c2, c3};
+    const int tx = threadIdx.x % kFdTX, ty = threadIdx.x / kFdTX;
+    const int x0 = blockIdx.x * kFdTX, y0 = blockIdx.y * kFdTY, z0 = blockIdx.z * kFdZ;
+    const int x = x0 + tx, y = y0 + ty;
+    const int z1 = min(z0 + kFdZ, res);
+    float win[2 * kFdR + 1];   // φ(x, y, z − R .. z + R)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const int s = k + 1;
-            if (cc[k] == 0.0f) continue;
-            const float fxp = phi[(int64_t(z) * res + y) * pitch + wrapi(x + s, res)];
-            const float fxm = phi[(int64_t(z) * res + y) * pitch + wrapi(x - s, res)];
-            const float fyp = phi[(int64_t(z) * res + wrapi(y + s, res)) * pitch + x];
-            const float fym = phi[(int64_t(z) * res + wrapi(y - s, res)) * pitch + x];
-            const float fzp = phi[(int64_t(wrapi(z + s, res)) * res + y) * pitch + x];
-            const float fzm = phi[(int64_t(wrapi(z - s, res)) * res + y) * pitch + x];
-            d[0] += cc[k] * (fxp - fxm);
-            d[1] += cc[k] * (fyp - fym);
-            d[2] += cc[k] * (fzp - fzm);
+    for (int k = 0; k < 2 * kFdR; ++k) win[k + 1] = fd_at(phi, x, y, z0 - kFdR + k, res, pitch);
+    constexpr int W2 = kFdTX + 2 * kFdR;
+    for (int z = z0; z < z1; ++z) {
+#pragma unroll
+        for (int k = 0; k < 2 * kFdR; ++k) win[k] = win[k + 1];
+        win[2 * kFdR] = fd_at(phi, x, y, z + kFdR, res, pitch);
+        __syncthreads();
+        fd_stage(tile, phi, x0, y0, z, kFdR, kFdR, res, pitch);
+        __syncthreads();
+        if (x < res && y < res) {
+            const float* c0 = tile + (ty + kFdR) * W2 + tx + kFdR;
+            float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kFdR; ++k) {
+                const int t = k + 1;
+                d0 += cc[k] * (c0[t] - c0[-t]);
+                d1 += cc[k] * (c0[t * W2] - c0[-t * W2]);
+                d2 += cc[k] * (win[kFdR + t] - win[kFdR - t]);
+            }
+            const int64_t o = (int64_t(z) * res + y) * pitch + x;
+            g0[o] = -d0;
+            g1[o] = -d1;
+            g2[o] = -d2;
         }
-        const int64_t o = (int64_t(z) * res + y) * pitch + x;
-        g0[o] = -d[0];
-        g1[o] = -d[1];
-        g2[o] = -d[2];
     }
 }
 
 // out = Σ_c D_c g_c.
-__global__ void __launch_bounds__(256) k_fd_div3(const float* __restrict__ g0, const float* __restrict__ g1,
-                                                 const float* __restrict__ g2, int res, int pitch, float c1,
-                                                 float c2, float c3, float* __restrict__ out) {
-    const int64_t total = int64_t(res) * res * res;
-    const float cc[3] = {c1, c2, c3};
-    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
-         t += int64_t(gridDim.x) * blockDim.x) {
-        const int x = int(t % res), y = int((t / res) % res), z = int(t / (int64_t(res) * res));
-        float d = 0.0f;
+__global__ void __launch_bounds__(kFdTX * kFdTY) k_fd_div3(const float* __restrict__ g0, const float* __restrict__ g1,
+                                                            const float* __restrict__ g2, int res, int pitch, float c1,
+                                                            float c2, float c3, float* __restrict__ out) {
+    __shared__ float tx_tile[kFdTY * (kFdTX + 2 * kFdR)];     // g0 with its x halo
+    __shared__ float ty_tile[(kFdTY + 2 * kFdR) * kFdTX];     // g1 with its y halo
+    const float cc[kFdR] = {c1, c2, c3};
+    const int tx = threadIdx.x % kFdTX, ty = threadIdx.x / kFdTX;
+    const int x0 = blockIdx.x * kFdTX, y0 = blockIdx.y * kFdTY, z0 = blockIdx.z * kFdZ;
+    const int x = x0 + tx, y = y0 + ty;
+    const int z1 = min(z0 + kFdZ, res);
+    float win[2 * kFdR + 1];   // g2(x, y, z − R .. z + R)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const int s = k + 1;
-            if (cc[k] == 0.0f) continue;
-            d += cc[k] * (g0[(int64_t(z) * res + y) * pitch + wrapi(x + s, res)] -
-                          g0[(int64_t(z) * res + y) * pitch + wrapi(x - s, res)]);
-            d += cc[k] * (g1[(int64_t(z) * res + wrapi(y + s, res)) * pitch + x] -
-                          g1[(int64_t(z) * res + wrapi(y - s, res)) * pitch + x]);
-            d += cc[k] * (g2[(int64_t(wrapi(z + s, res)) * res + y) * pitch + x] -
-                          g2[(int64_t(wrapi(z - s, res)) * res + y) * pitch + x]);
+    for (int k = 0; k < 2 * kFdR; ++k) win[k + 1] = fd_at(g2, x, y, z0 - kFdR + k, res, pitch);
+    constexpr int WX = kFdTX + 2 * kFdR;
+    for (int z = z0; z < z1; ++z) {
+#pragma unroll
+        for (int k = 0; k < 2 * kFdR; ++k) win[k] = win[k + 1];
+        win[2 * kFdR] = fd_at(g2, x, y, z + kFdR, res, pitch);
+        __syncthreads();
+        fd_stage(tx_tile, g0, x0, y0, z, kFdR, 0, res, pitch);
+        fd_stage(ty_tile, g1, x0, y0, z, 0, kFdR, res, pitch);
+        __syncthreads();
+        if (x < res && y < res) {
+            const float* a0 = tx_tile + ty * WX + tx + kFdR;
+            const float* a1 = ty_tile + (ty + kFdR) * kFdTX + tx;
+            float d = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kFdR; ++k) {
+                const int t = k + 1;
+                d += cc[k] * (a0[t] - a0[-t]);
+                d += cc[k] * (a1[t * kFdTX] - a1[-t * kFdTX]);
+                d += cc[k] * (win[kFdR + t] - win[kFdR - t]);
+            }
+            out[(int64_t(z) * res + y) * pitch + x] = d;
         }
-        out[(int64_t(z) * res + y) * pitch + x] = d;
     }
 }
 
@@ -229,6 +277,192 @@ __global__ void k_mesh_affine(const float* __restrict__ in, int res, int pitch, 
         const int64_t row = t / res;
         const int x = int(t - row * res);
         out[t] = scale * in[row * pitch + x] - offset;
+    }
+}
+
+// ── brick-owned forms (particles sorted by brick, see brick.cuh) ─────────────────
+// One CTA owns one brick and its particles; its W-node stencils fall inside the
+// brick's deposit box (BrickList::ssx, sSs, sos), which lives in shared memory.
+
+// Position of particle p and, per axis, the weights, their derivatives (grid units per
+// length dgdx) and the stencil's first node relative to the box (clamped into the box
+// with error bit 2 when the binning and this evaluation disagree).
+template <int W>
+__device__ __forceinline__ void brick_stencil(const float* __restrict__ psi, const float* __restrict__ q1,
+                                              const LatticeDiv& ld, int64_t np, int64_t p, float L, float resf,
+                                              int res, const float sh[3], const TileBox& box, int* err,
+                                              float (&w)[3][W], float (&dw)[3][W], int (&d)[3]) {
+    int ijk[3];
+    ld.ijk(p, ijk[0], ijk[1], ijk[2]);
+    const float dgdx = resf / L;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float X = psi[p + a * np] + q1[ijk[a]];
+        const float g = grid_coord(X + sh[a], L, resf, err);
+        const int bb = wbase<W>(g);
+#pragma unroll
+        for (int o = 0; o < W; ++o) {
+            const float dd = g - float(bb + WLo<W>::v + o);
+            w[a][o] = wk<W>(fabsf(dd));
+            dw[a][o] = dwk<W>(dd) * dgdx;
+        }
+        d[a] = box_rel(bb + WLo<W>::v, box.o[a], res);
+        if (d[a] < 0 || d[a] > box.S[a] - W) {
+            if (err) atomicOr(err, 2);
+            d[a] = d[a] < 0 ? 0 : box.S[a] - W;
+        }
+    }
+}
+
+// m_c(n) += scale · ā_c(p) · W(X_p − n) for c = 0, 1, 2: one component per pass over the
+// brick's particles into a shared-memory box, then added to the mesh with vector
+// reductions. Bricks of at most kFixedMax particles accumulate in 32-bit fixed point
+// (integer shared atomics, signed values in two's complement): the node sums are
+// bounded by cnt · max|scale · ā| (a particle's weights sum to 1), kept below 2^30, so
+// the unit is at most 4096 · max|scale · ā| · 2^−30. Denser bricks use float shared
+// atomics.
+constexpr unsigned kFixedMax = 4096;
+
+template <int W>
+__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scatter_weighted_brick(
+    const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
+    float sx, float sy, float sz, const float* __restrict__ abar, float scale, float* __restrict__ m0,
+    float* __restrict__ m1, float* __restrict__ m2, int* err, BrickList bl) {
+    extern __shared__ __align__(128) float wbox[];
+    unsigned* qbox = reinterpret_cast<unsigned*>(wbox);
+    __shared__ float s_max[kTileThreads / 32];
+    const int b = brick_of_block(bl, blockIdx.x);
+    unsigned start, cnt;
+    brick_range(bl, b, start, cnt);
+    if (cnt == 0) return;
+    const int tid = threadIdx.x;
+    const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
+    const bool vec = ((pitch | res) & 3) == 0;
+    const float resf = float(res);
+    const int cells = box.plane * box.S[2];   // a multiple of 4
+    const float sh[3] = {sx, sy, sz};
+    const bool fixed = cnt <= kFixedMax;
+    LatticeDiv ld;
+    ld.init(n);
+#pragma unroll 1
+    for (int comp = 0; comp < 3; ++comp) {
+        float up = 1.0f, down = 1.0f;
+        for (int t = 4 * tid; t < cells; t += 4 * kTileThreads)
+            *reinterpret_cast<uint4*>(qbox + t) = make_uint4(0u, 0u, 0u, 0u);
+        if (fixed) {   // the largest |scale · ā_c| of the brick sets the unit
+            float m = 0.0f;
+            for (unsigned slot = tid; slot < cnt; slot += kTileThreads)
+                m = fmaxf(m, fabsf(scale * abar[int64_t(bl.perm[start + slot]) + comp * np]));
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if ((tid & 31) == 0) s_max[tid >> 5] = m;
+        }
+        __syncthreads();
+        if (fixed) {
+            float amax = 0.0f;
+            for (int i = 0; i < kTileThreads / 32; ++i) amax = fmaxf(amax, s_max[i]);
+            if (!(amax > 0.0f) || !isfinite(amax)) {   // nothing to deposit (or not finite: skip)
+                __syncthreads();
+                continue;
+            }
+            int ex;
+            frexpf(amax * float(cnt), &ex);            // amax · cnt < 2^ex
+            const int e = min(30 - ex, 120);
+            up = ldexpf(1.0f, e);
+            down = ldexpf(1.0f, -e);
+        }
+        for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
+            // lanes 8 slots apart: particles of one cell land in different warps
+            const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
+            if (slot >= cnt) continue;
+            const int64_t p = bl.perm[start + slot];
+            const float av = scale * abar[p + comp * np] * up;
+            float w[3][W], dw[3][W];
+            int d[3];
+            brick_stencil<W>(psi, q1, ld, np, p, L, resf, res, sh, box, comp == 0 ? err : nullptr, w, dw, d);
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+#pragma unroll
+                for (int bb = 0; bb < W; ++bb) {
+                    const int o = ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+                    const float wyz = av * w[1][bb] * w[2][c];
+#pragma unroll
+                    for (int a = 0; a < W; ++a) {
+                        if (fixed) atomicAdd(qbox + o + a, unsigned(__float2int_rn(w[0][a] * wyz)));
+                        else atomicAdd(wbox + o + a, w[0][a] * wyz);
+                    }
+                }
+        }
+        __syncthreads();
+        float* mesh = comp == 0 ? m0 : (comp == 1 ? m1 : m2);
+        for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
+            if (vec) {
+                const uint4 u = *reinterpret_cast<const uint4*>(qbox + so);
+                if ((u.x | u.y | u.z | u.w) == 0u) return;
+                if (fixed)
+                    red_add_v4(mesh + go, float(int(u.x)) * down, float(int(u.y)) * down, float(int(u.z)) * down,
+                               float(int(u.w)) * down);
+                else
+                    red_add_v4(mesh + go, __uint_as_float(u.x), __uint_as_float(u.y), __uint_as_float(u.z),
+                               __uint_as_float(u.w));
+            } else {
+                const unsigned u = qbox[so];
+                if (u != 0u) atomicAdd(mesh + go, fixed ? float(int(u)) * down : __uint_as_float(u));
+            }
+        });
+        __syncthreads();
+    }
+}
+
+// f1 == null: Ψ̄_a += scale · Σ_n ∂_a W · f0(n); else Ψ̄_a += scale · Σ_c ā_c Σ_n ∂_a W · f_c(n).
+// Each field is staged once per brick over its deposit box; every particle of the brick
+// then adds its share to Ψ̄ (a particle belongs to one brick: no other CTA writes it).
+template <int W>
+__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gather_grad_brick(
+    const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
+    float sx, float sy, float sz, const float* __restrict__ f0, const float* __restrict__ f1,
+    const float* __restrict__ f2, const float* __restrict__ abar, float scale, float* __restrict__ psibar, int* err,
+    BrickList bl) {
+    extern __shared__ __align__(128) float fbox[];
+    const int b = brick_of_block(bl, blockIdx.x);
+    unsigned start, cnt;
+    brick_range(bl, b, start, cnt);
+    if (cnt == 0) return;
+    const int tid = threadIdx.x;
+    const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
+    const bool vec = ((pitch | res) & 3) == 0;
+    const float resf = float(res);
+    const float sh[3] = {sx, sy, sz};
+    const int nf = f1 ? 3 : 1;
+    LatticeDiv ld;
+    ld.init(n);
+#pragma unroll 1
+    for (int f = 0; f < nf; ++f) {
+        stage_box_wrapped(fbox, f == 0 ? f0 : (f == 1 ? f1 : f2), box, res, pitch, vec);
+        __syncthreads();
+        for (unsigned slot = tid; slot < cnt; slot += kTileThreads) {
+            const int64_t p = bl.perm[start + slot];
+            float w[3][W], dw[3][W];
+            int d[3];
+            brick_stencil<W>(psi, q1, ld, np, p, L, resf, res, sh, box, f == 0 ? err : nullptr, w, dw, d);
+            const float af = scale * (f1 ? abar[p + f * np] : 1.0f);
+            float v[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+#pragma unroll
+                for (int bb = 0; bb < W; ++bb) {
+                    const float* row = fbox + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+#pragma unroll
+                    for (int a = 0; a < W; ++a) {
+                        const float fv = row[a];
+                        v[0] += dw[0][a] * w[1][bb] * w[2][c] * fv;
+                        v[1] += w[0][a] * dw[1][bb] * w[2][c] * fv;
+                        v[2] += w[0][a] * w[1][bb] * dw[2][c] * fv;
+                    }
+                }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) psibar[p + a * np] += af * v[a];
+        }
+        __syncthreads();
     }
 }
 

@@ -753,6 +753,8 @@ struct djb_solver {
     bool zpass = false;
     float2* wN = nullptr;
     float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
+    float* scr[8] = {};     // staging and work buffers of the adjoint entry points, kept between calls
+    size_t scr_n[8] = {};
     int nsm = 148;  // SMs of the device (persistent grids)
     // brick boxes (brick.cuh): width along x, extent along y and z, first node relative
     // to the brick's first cell; g = interpolation, s = mass assignment
@@ -1060,6 +1062,10 @@ int scatter_attrs_w() {
                                   kBrickSmemMax));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kBrickSmemMax));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_weighted_brick<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kBrickSmemMax));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_grad_brick<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kBrickSmemMax));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   int(cudaSharedmemCarveoutMaxShared)));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1292,12 +1298,36 @@ int poisson(djb_solver* s, int m) {
     return DJB_OK;
 }
 
+// Grid of the column-sweep stencil kernels for a res^3 mesh.
+dim3 fd_grid(int res) {
+    return dim3(unsigned((res + djb::kFdTX - 1) / djb::kFdTX), unsigned((res + djb::kFdTY - 1) / djb::kFdTY),
+                unsigned((res + djb::kFdZ - 1) / djb::kFdZ));
+}
+
 template <int W>
 void launch_vjp_kernels(djb_solver* s, int stage, const float* psi, const float* abar, float* psibar,
                         const Shift3& sh, float scale, const int* perm) {
     float* rho = rho_mesh(s, 0);
     const int pitch = rho_pitch(s);
     const int b = blocks(s->np);
+    if (perm) {   // brick-owned forms: boxes in shared memory, one CTA per brick
+        const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
+        const size_t smem = scatter_smem(s);
+        const djb::BrickList bl = brick_list(s);
+        if (stage == 0)
+            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
+                psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, s->adj[0], s->adj[1], s->adj[2],
+                abar, scale, psibar, s->err, bl);
+        else if (stage == 1)
+            djb::k_scatter_weighted_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
+                psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, abar, scale, s->adj[0], s->adj[1],
+                s->adj[2], s->err, bl);
+        else
+            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
+                psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, rho, nullptr, nullptr, nullptr,
+                scale, psibar, s->err, bl);
+        return;
+    }
     if (stage == 0)
         djb::k_gather_grad<W><<<b, 256, 0, s->stream>>>(psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y,
                                                          sh.z, s->adj[0], s->adj[1], s->adj[2], abar, scale, psibar,
@@ -1345,20 +1375,31 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
         const GroupShifts g = group_shifts(s, si, 1);
         const Shift3 sh = g.s[0];
         CUDA_TRY(cudaMemsetAsync(rho, 0, rho_floats * sizeof(float), s->stream));
-        if (s->W == 2) djb::k_scatter<2, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
-            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, perm);
-        if (s->W == 3) djb::k_scatter<3, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
-            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, perm);
-        if (s->W == 4) djb::k_scatter<4, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
-            psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, perm);
+        if (perm) {   // the forward's brick-owned deposit on these positions
+            const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
+            const int tma = (s->phi[0] != nullptr && s->tma) ? 1 : 0;
+#define DJB_VS(W_)                                                                                             \
+    if (s->W == W_)                                                                                            \
+        djb::k_scatter_brick<W_, 1><<<nbricks, djb::kTileThreads, scatter_smem(s), s->stream>>>(                \
+            psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, brick_list(s), s->tmap_s[0], \
+            s->tmap_s[0], tma);
+            DJB_VS(2) DJB_VS(3) DJB_VS(4)
+#undef DJB_VS
+        } else {
+            if (s->W == 2) djb::k_scatter<2, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+                psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+            if (s->W == 3) djb::k_scatter<3, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+                psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+            if (s->W == 4) djb::k_scatter<4, 1><<<blocks(s->np), kThreads, 0, s->stream>>>(
+                psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
+        }
         TRY(poisson(s, 0));  // φ
-        const int cb = grid_for(int64_t(s->res) * s->res * s->res);
-        djb::k_fd_grad3<<<cb, 256, 0, s->stream>>>(rho, s->res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
+        djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(rho, s->res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
                                                     s->adj[2]);
         vjp_kernels(s, 0, psi, abar, psibar, sh, inv_ns, perm);  // interpolation weights
         for (int c = 0; c < 3; ++c) CUDA_TRY(cudaMemsetAsync(s->adj[c], 0, rho_floats * sizeof(float), s->stream));
         vjp_kernels(s, 1, psi, abar, psibar, sh, inv_ns, perm);  // Ḡ
-        djb::k_fd_div3<<<cb, 256, 0, s->stream>>>(s->adj[0], s->adj[1], s->adj[2], s->res, pitch, s->c1, s->c2,
+        djb::k_fd_div3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(s->adj[0], s->adj[1], s->adj[2], s->res, pitch, s->c1, s->c2,
                                                    s->c3, rho);  // φ̄
         TRY(poisson(s, 0));                                    // ρ̄
         vjp_kernels(s, 2, psi, abar, psibar, sh, 1.0f, perm);  // deposit weights
@@ -1405,6 +1446,8 @@ void release(djb_solver* s) {
     if (s->have_c2r_d) cufftDestroy(s->c2r_d);
     if (s->have_r2c_d) cufftDestroy(s->r2c_d);
     for (void* p : s->allocs) cudaFree(p);
+    for (float* p : s->scr)
+        if (p) cudaFree(p);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     if (prev >= 0) cudaSetDevice(prev);
     delete s;
@@ -1688,26 +1731,42 @@ struct Stage {
     bool owned = false;
 };
 
-int stage_in(djb_solver* s, Stage& st, const float* src, size_t count, int mem, bool copy) {
+// Work buffer `slot` of at least `count` floats, kept by the solver between calls (a
+// per-call allocation and release of gigabytes made the adjoint's time vary by 3x).
+int scratch(djb_solver* s, int slot, size_t count, float** out) {
+    if (s->scr_n[slot] < count) {
+        if (s->scr[slot]) {
+            CUDA_TRY(cudaStreamSynchronize(s->stream));
+            cudaFree(s->scr[slot]);
+            s->scr[slot] = nullptr;
+            s->scr_n[slot] = 0;
+        }
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&s->scr[slot]), count * sizeof(float));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            s->scr[slot] = nullptr;
+            return fail(DJB_ERR_ALLOC, "work buffer allocation of %zu floats failed: %s", count, cudaGetErrorString(e));
+        }
+        s->scr_n[slot] = count;
+    }
+    *out = s->scr[slot];
+    return DJB_OK;
+}
+
+// Device inputs are used in place; host inputs are copied (or work buffers zeroed) into
+// the solver's work buffer `slot`.
+int stage_in(djb_solver* s, Stage& st, const float* src, size_t count, int mem, bool copy, int slot) {
     if (mem == DJB_MEM_DEVICE && src) {
         st.p = const_cast<float*>(src);
         return DJB_OK;
     }
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&st.p), count * sizeof(float), s->stream);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(DJB_ERR_ALLOC, "staging allocation failed: %s", cudaGetErrorString(e));
-    }
-    st.owned = true;
+    TRY(scratch(s, slot, count, &st.p));
     if (copy && src) return copy_in(s, st.p, src, count, mem);
     CUDA_TRY(cudaMemsetAsync(st.p, 0, count * sizeof(float), s->stream));
     return DJB_OK;
 }
 
-void stage_free(djb_solver* s, Stage& st) {
-    if (st.owned && st.p) cudaFreeAsync(st.p, s->stream);
-    st = Stage{};
-}
+void stage_free(djb_solver*, Stage& st) { st = Stage{}; }
 
 int djb_pm_acceleration_vjp(djb_solver* s, const float* psi, const float* acc_bar, float* psi_bar, int32_t mem) {
     djb::clear_error();
@@ -1715,9 +1774,9 @@ int djb_pm_acceleration_vjp(djb_solver* s, const float* psi, const float* acc_ba
     CUDA_TRY(cudaSetDevice(s->cfg.device));
     const size_t count = size_t(3 * s->np);
     Stage sp, sa, sb;
-    int rc = stage_in(s, sp, psi, count, mem, true);
-    if (rc == DJB_OK) rc = stage_in(s, sa, acc_bar, count, mem, true);
-    if (rc == DJB_OK) rc = stage_in(s, sb, mem == DJB_MEM_DEVICE ? nullptr : psi_bar, count, mem, false);
+    int rc = stage_in(s, sp, psi, count, mem, true, 0);
+    if (rc == DJB_OK) rc = stage_in(s, sa, acc_bar, count, mem, true, 1);
+    if (rc == DJB_OK) rc = stage_in(s, sb, mem == DJB_MEM_DEVICE ? nullptr : psi_bar, count, mem, false, 2);
     float* pb = (mem == DJB_MEM_DEVICE) ? psi_bar : sb.p;
     if (rc == DJB_OK && mem == DJB_MEM_DEVICE) {
         cudaError_t e = cudaMemsetAsync(pb, 0, count * sizeof(float), s->stream);
@@ -1740,12 +1799,12 @@ int djb_step_vjp(djb_solver* s, double dd1, double alpha, double beta, double dd
     const size_t count = size_t(3 * s->np);
     const int64_t m = int64_t(count);
     Stage sp, sm, sb, smb, s1, sa;
-    int rc = stage_in(s, sp, psi0, count, mem, true);
-    if (rc == DJB_OK) rc = stage_in(s, sm, mom0, count, mem, true);
-    if (rc == DJB_OK) rc = stage_in(s, sb, psi_bar, count, mem, true);
-    if (rc == DJB_OK) rc = stage_in(s, smb, mom_bar, count, mem, true);
-    if (rc == DJB_OK) rc = stage_in(s, s1, nullptr, count, DJB_MEM_HOST, false);
-    if (rc == DJB_OK) rc = stage_in(s, sa, nullptr, count, DJB_MEM_HOST, false);
+    int rc = stage_in(s, sp, psi0, count, mem, true, 0);
+    if (rc == DJB_OK) rc = stage_in(s, sm, mom0, count, mem, true, 1);
+    if (rc == DJB_OK) rc = stage_in(s, sb, psi_bar, count, mem, true, 2);
+    if (rc == DJB_OK) rc = stage_in(s, smb, mom_bar, count, mem, true, 3);
+    if (rc == DJB_OK) rc = stage_in(s, s1, nullptr, count, DJB_MEM_HOST, false, 4);
+    if (rc == DJB_OK) rc = stage_in(s, sa, nullptr, count, DJB_MEM_HOST, false, 5);
     if (rc == DJB_OK) {
         djb::k_drifted<<<grid_for(m), kThreads, 0, s->stream>>>(sp.p, sm.p, float(dd1), s1.p, m);
         djb::k_step_vjp_pre<<<grid_for(m), kThreads, 0, s->stream>>>(sb.p, smb.p, float(dd2), float(beta), sa.p, m);
@@ -1782,8 +1841,8 @@ int djb_mesh_fields(djb_solver* s, const float* psi, float* out, int32_t mem) {
     for (int c = 0; c < 3; ++c)
         if (!s->adj[c]) TRY(dmalloc(s, (void**)&s->adj[c], rho_floats * sizeof(float)));
     Stage sp, so;
-    int rc = stage_in(s, sp, psi, count, mem, true);
-    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = stage_in(s, so, nullptr, size_t(4 * cells), DJB_MEM_HOST, false);
+    int rc = stage_in(s, sp, psi, count, mem, true, 0);
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = stage_in(s, so, nullptr, size_t(4 * cells), DJB_MEM_HOST, false, 1);
     float* o = (mem == DJB_MEM_HOST) ? so.p : out;
     if (rc == DJB_OK) {
         float* rho = rho_mesh(s, 0);
@@ -1801,7 +1860,7 @@ int djb_mesh_fields(djb_solver* s, const float* psi, float* out, int32_t mem) {
         djb::k_mesh_affine<<<cb, 256, 0, s->stream>>>(rho, res, pitch, f, 1.0f, o);  // δ
         rc = poisson(s, 0);
         if (rc == DJB_OK) {
-            djb::k_fd_grad3<<<cb, 256, 0, s->stream>>>(rho, res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
+            djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(rho, res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
                                                         s->adj[2]);
             for (int c = 0; c < 3; ++c)
                 djb::k_mesh_affine<<<cb, 256, 0, s->stream>>>(s->adj[c], res, pitch, 1.0f, 0.0f, o + (c + 1) * cells);
