@@ -303,7 +303,7 @@ def nn_timing(dev, stream, world):
                              frac_eval=eval_tflops / peak, peak_source=f"{kind} bf16_tflops"),
                note="4 layers 4->32->32->32->3, 3^3 kernels, periodic; forward, data-gradient and weight-"
                     "gradient convolutions as implicit GEMMs on the tcgen05 tensor cores (bf16 operands, float32 "
-                    "accumulation in tensor memory; the first layer's weight gradient via im2col + cuBLAS); "
+                    "accumulation in tensor memory; narrow inputs zero-widened for the weight gradient); "
                     "train = forward + backward + Adam at 128^3 (FLOPs counted as 3x forward); eval = one "
                     "forward at 512^3; FLOPs with the real channel counts")
     return out

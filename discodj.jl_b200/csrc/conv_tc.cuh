@@ -531,8 +531,9 @@ constexpr int kWY = 4;                     // dY tile buffers
 struct WArgs {
     const __nv_bfloat16* X;   // [nvox][32]
     const __nv_bfloat16* dY;  // [nvox][cout] (cout = 8·CCO)
-    float* dW;                // [27][32][cout], accumulated with atomics
+    float* dW;                // [27][cin_w][cout], accumulated with atomics
     int res, cout;
+    int cin_w;                // input-channel rows of dW (<= 32: the input may be zero-widened)
     int ntx, nty, nzs, zlen;
     int use_tma;              // plane map (X) and tile map (dY) accepted
     int* err;
@@ -753,8 +754,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int h = 0; h < N / 16; ++h) tmem_ld16(tmem + lane_base + uint32_t(tap9 * N + h * 16), v + h * 16);
                 tmem_wait_ld();
-                if (q < 3) {
-                    float* dst = a.dW + (size_t(q * 9 + tap9) * 32 + c) * a.cout;
+                if (q < 3 && c < a.cin_w) {
+                    float* dst = a.dW + (size_t(q * 9 + tap9) * a.cin_w + c) * a.cout;
 #pragma unroll
                     for (int o = 0; o < N; ++o)
                         if (o < a.cout) atomicAdd(dst + o, __uint_as_float(v[o]));

@@ -280,6 +280,7 @@ struct djb_nn {
     int64_t chunk = 0;
     __nv_bfloat16* act[kMaxLayers + 1] = {};  // [v][cinp] per layer input (act[L] unused)
     __nv_bfloat16* act0p = nullptr;            // [v][8] x-pair rows of the input (use_pair)
+    __nv_bfloat16* actw = nullptr;             // [v][32] a narrow layer input widened (training)
     __nv_bfloat16* col = nullptr;              // [chunk][27·Cmax]
     float* Y = nullptr;                        // [chunk][Nmax] (also dA)
     float* dcol = nullptr;                     // [nvox][27·Cmax] (training only)
@@ -320,6 +321,7 @@ void free_work(djb_nn* h) {
     h->work.clear();
     for (auto& a : h->act) a = nullptr;
     h->act0p = nullptr;
+    h->actw = nullptr;
     h->col = nullptr;
     h->Y = nullptr;
     h->work_train = false;
@@ -493,13 +495,30 @@ int launch_wg_inst(djb_nn* h, const djb::conv::WArgs& a0) {
     return DJB_OK;
 }
 
-// Layer l's weight gradient on the tensor cores (32 input channels), accumulated into
-// the zeroed gradient buffer.
-bool use_tc_wgrad(const djb_nn* h, int l) { return use_tc(h, l) && h->cinp[l] == 32; }
+// Layer l's weight gradient on the tensor cores, accumulated into the zeroed gradient
+// buffer. The kernel reads 32 input channels: narrower inputs are first widened with
+// zeros into h->actw, and only the layer's own rows of dW are written.
+bool use_tc_wgrad(const djb_nn* h, int l) { return use_tc(h, l); }
+
+// [v][c] (c < cp, a multiple of 8) → [v][32], zeros beyond cp.
+__global__ void k_widen32(const __nv_bfloat16* __restrict__ in, int cp, int64_t nvox, __nv_bfloat16* __restrict__ out) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nvox * 4; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / 4;
+        const int c8 = int(t - v * 4);
+        reinterpret_cast<uint4*>(out)[t] =
+            c8 * 8 < cp ? reinterpret_cast<const uint4*>(in + v * cp)[c8] : make_uint4(0u, 0u, 0u, 0u);
+    }
+}
 
 int conv_tc_wgrad(djb_nn* h, int l, const __nv_bfloat16* dy) {
     djb::conv::WArgs a{};
     a.X = h->act[l];
+    const int64_t nvox = int64_t(h->res) * h->res * h->res;
+    if (h->cinp[l] < 32) {
+        k_widen32<<<grid_of(nvox * 4), kNT, 0, h->stream>>>(h->act[l], h->cinp[l], nvox, h->actw);
+        a.X = h->actw;
+    }
+    a.cin_w = h->cinp[l];
     a.dY = dy;
     a.dW = h->g + h->woff[l];
     a.res = h->res;
@@ -533,8 +552,8 @@ int check_derr(djb_nn* h) {
 }
 
 // Work areas for res³ voxels; training needs the whole mesh at once (chunk = nvox).
-// The im2col buffers exist only for what runs on that path: the weight gradients (col),
-// and layers that do not fit the tensor-core kernel (col, Y, and dcol when training).
+// The im2col buffers exist only for layers that do not fit the tensor-core kernels (or
+// every layer after djb_nn_set_conv(h, 1)): col, Y, and dcol when training.
 int ensure_work(djb_nn* h, int res, bool train) {
     const int64_t nvox = int64_t(res) * res * res;
     const bool im2col = any_im2col(h);
@@ -549,8 +568,7 @@ int ensure_work(djb_nn* h, int res, bool train) {
     for (int l = 0; l < h->layers; ++l)
         TRYN(dalloc(h, (void**)&h->act[l], size_t(nvox) * h->cinp[l] * sizeof(__nv_bfloat16), true));
     TRYN(dalloc(h, (void**)&h->act0p, size_t(nvox) * 8 * sizeof(__nv_bfloat16), true));
-    if (train || im2col)
-        TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
+    if (im2col) TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
     if (im2col) TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
     TRYN(dalloc(h, (void**)&h->outm, size_t(nvox) * h->cout[h->layers - 1] * sizeof(float), true));
     TRYN(dalloc(h, (void**)&h->lsum, sizeof(double), true));
@@ -559,6 +577,7 @@ int ensure_work(djb_nn* h, int res, bool train) {
         TRYN(dalloc(h, (void**)&h->dA, size_t(nvox) * C * sizeof(float), true));
         TRYN(dalloc(h, (void**)&h->dY, size_t(nvox) * C * sizeof(__nv_bfloat16), true));
         TRYN(dalloc(h, (void**)&h->dY2, size_t(nvox) * C * sizeof(__nv_bfloat16), true));
+        TRYN(dalloc(h, (void**)&h->actw, size_t(nvox) * 32 * sizeof(__nv_bfloat16), true));
     }
     h->work_train = train;
     h->work_im2col = im2col;
