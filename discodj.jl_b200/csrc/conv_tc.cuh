@@ -67,6 +67,7 @@ struct Args {
     int res, cin, cout, nout, flip;
     int ntx, nty, nzs, zlen;  // tiles along x, y; z segments of zlen planes
     int use_tma;              // the map covers X: interior planes by bulk tensor copy
+    int use_ostore;           // kHidden / kBackData with cout == N: tiles leave by bulk tensor stores
     int* err;                 // set to 1 when a wait runs out
 };
 
@@ -83,7 +84,8 @@ __host__ __device__ constexpr uint32_t slot_bytes() {
 template <int KC, int N, bool PAIR = false>
 constexpr int smem_bytes() {
     const int w = PAIR ? 3 * 2 * 3 * N * 16 : 27 * KC * N * 16;
-    const int b = w + kRing * int(slot_bytes<KC>()) + (2 * kRing + (kEpiGroups + 1) * kAccTiles + 1) * 8 + 16;
+    const int stage = kEpiGroups * 2 * 128 * N * 2;   // output staging: two tiles per epilogue group
+    const int b = w + kRing * int(slot_bytes<KC>()) + stage + (2 * kRing + (kEpiGroups + 1) * kAccTiles + 1) * 8 + 16;
     return b < kOneCtaSmem ? kOneCtaSmem : b;   // the CTA's tensor memory may be all 512 columns
 }
 
@@ -189,6 +191,29 @@ __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
+// Tile from shared memory to global memory at (c0, c1, c2, c3) of `map` (a bulk group).
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3, uint32_t src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(src)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// Waits until at most one of this thread's bulk groups still reads shared memory.
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Barrier `id` of the 128 threads of one epilogue group; returns whether any passed true.
+__device__ __forceinline__ bool group_bar_or(int id, bool v) {
+    uint32_t r;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 q, %2, 0;\n bar.red.or.pred p, %1, 128, q;\n"
+                 " selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(r)
+                 : "r"(id), "r"(v ? 1u : 0u)
+                 : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void group_bar(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
 __device__ __forceinline__ int wrap(int v, int res) {
     v %= res;
     return v < 0 ? v + res : v;
@@ -229,7 +254,8 @@ __device__ __forceinline__ Item item_of(const A& a, int item) {
 // weight for dx = 2): three MMAs per plane instead of nine.
 template <int CC, int N, int MODE, bool PAIR = false>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_conv3_tc(const __grid_constant__ Args a, const __grid_constant__ CUtensorMap tmap) {
+    k_conv3_tc(const __grid_constant__ Args a, const __grid_constant__ CUtensorMap tmap,
+               const __grid_constant__ CUtensorMap omap) {
     static_assert(!PAIR || CC == 1, "the x-pair layout has one 16-byte chunk per position");
     constexpr int KC = PAIR ? 1 : (CC + 1) / 2 * 2;   // chunks staged per position
     constexpr int NSH = PAIR ? 3 : 9;                  // weight shifts: dy (PAIR) or (dy, dx)
@@ -240,7 +266,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* ws = smem;
     uint8_t* ringp = smem + NSH * KW * 3 * N * 16;
-    uint64_t* full = reinterpret_cast<uint64_t*>(ringp + kRing * kSlot);
+    uint8_t* ostage = ringp + kRing * kSlot;                     // [group][2][128 rows][N bf16]
+    uint64_t* full = reinterpret_cast<uint64_t*>(ostage + kEpiGroups * 2 * 128 * N * 2);
     uint64_t* empty = full + kRing;
     uint64_t* accf = empty + kRing;                  // [group][accumulator]
     uint64_t* acce = accf + kEpiGroups * kAccTiles;
@@ -440,6 +467,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         uint32_t uses[kAccTiles];   // this group's earlier tiles per accumulator
         for (int i = 0; i < kAccTiles; ++i) uses[i] = 0;
         uint32_t n = 0;             // the CTA's tiles so far
+        uint32_t kst = 0;           // this group's tiles so far (staging buffer kst & 1)
+        const bool ostore = MODE != kLast && a.use_ostore;
+        const uint32_t stage0 = smem_u32(ostage) + uint32_t(g * 2 * 128 * N * 2);
         bool ok = true;
         for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
             const Item it = item_of(a, item);
@@ -448,7 +478,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int i = 0; i < it.nt; ++i, ++n) {
                 if (int(n % kEpiGroups) != g) continue;
                 const int c = acc_of(i);
-                if (!role_wait(&accf[g * kAccTiles + c], uses[c] & 1u, abort_flag)) {
+                bool bad = !role_wait(&accf[g * kAccTiles + c], uses[c] & 1u, abort_flag);
+                if (ostore) bad = group_bar_or(1 + g, bad);   // the group's barriers stay matched
+                if (bad) {
                     ok = false;
                     break;
                 }
@@ -462,22 +494,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc_before_sync();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&acce[c]);
-                if (!valid) continue;
+                if (!valid && !ostore) continue;
                 const int64_t v = (int64_t(it.z0 + i) * a.res + y) * a.res + x;
                 if constexpr (MODE == kLast) {
 #pragma unroll
                     for (int cc = 0; cc < N; ++cc)
                         if (cc < a.nout) a.Yf[int64_t(cc) * nvox + v] = __uint_as_float(r[cc]) + bias[cc];
                 } else {
-                    uint4* dst = reinterpret_cast<uint4*>(a.Y + v * a.cout);
-                    const uint4* msk = nullptr;
-                    if constexpr (MODE == kBackData) msk = reinterpret_cast<const uint4*>(a.M + v * a.cout);
+                    uint4 out[N / 8];
 #pragma unroll
                     for (int c8 = 0; c8 < N / 8; ++c8) {
-                        if (c8 * 8 >= a.cout) break;
                         uint32_t w[4];
                         if constexpr (MODE == kBackData) {
-                            const uint4 m4 = __ldg(msk + c8);
+                            const uint4 m4 = (valid && c8 * 8 < a.cout)
+                                                 ? __ldg(reinterpret_cast<const uint4*>(a.M + v * a.cout) + c8)
+                                                 : make_uint4(0u, 0u, 0u, 0u);
                             const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
@@ -495,11 +526,34 @@ __global__ void __launch_bounds__(kThreads, 1)
                                                  fmaxf(__uint_as_float(r[cc + 1]) + bias[cc + 1], 0.0f));
                             }
                         }
-                        dst[c8] = make_uint4(w[0], w[1], w[2], w[3]);
+                        out[c8] = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                    if (ostore) {
+                        // the bulk store that last read this buffer (two tiles ago) is done
+                        if (row == 0) bulk_wait_read1();
+                        group_bar(1 + g);
+                        const uint32_t buf = stage0 + (kst & 1u) * uint32_t(128 * N * 2) + uint32_t(row * N * 2);
+#pragma unroll
+                        for (int c8 = 0; c8 < N / 8; ++c8)
+                            asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(buf + c8 * 16),
+                                         "r"(out[c8].x), "r"(out[c8].y), "r"(out[c8].z), "r"(out[c8].w)
+                                         : "memory");
+                        fence_proxy_async_smem();   // the rows are read by the bulk store
+                        group_bar(1 + g);
+                        if (row == 0)   // rows outside the mesh are clipped by the store
+                            tma_store_4d(&omap, 0, it.x0, it.y0, it.z0 + i,
+                                         stage0 + (kst & 1u) * uint32_t(128 * N * 2));
+                        ++kst;
+                    } else {
+                        uint4* dst = reinterpret_cast<uint4*>(a.Y + v * a.cout);
+#pragma unroll
+                        for (int c8 = 0; c8 < N / 8; ++c8)
+                            if (c8 * 8 < a.cout) dst[c8] = out[c8];
                     }
                 }
             }
         }
+        if (ostore && row == 0) bulk_wait_all();   // the last stores have landed
     }
     tc_before_sync();
     __syncthreads();

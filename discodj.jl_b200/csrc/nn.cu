@@ -377,6 +377,32 @@ bool act_map(CUtensorMap* m, const __nv_bfloat16* X, int res, int cc, int bx, in
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map of a bf16 [res]^3 × cout output as [z][y][x][cout] with boxes of one output
+// tile (8 × 16 voxels of one plane, all channels), for the bulk tensor stores.
+bool out_map(CUtensorMap* m, __nv_bfloat16* Y, int res, int cout) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && fn)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        cudaGetLastError();
+    }
+    if (!encode || !Y) return false;
+    using namespace djb::conv;
+    const cuuint64_t r = cuuint64_t(res), row = cuuint64_t(cout) * 2;
+    const cuuint64_t dims[4] = {cuuint64_t(cout), r, r, r};
+    const cuuint64_t strides[3] = {row, r * row, r * r * row};
+    const cuuint32_t box[4] = {cuuint32_t(cout), cuuint32_t(kTX), cuuint32_t(kTY), 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, Y, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int CC, int N, int MODE, bool PAIR = false>
 int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
     using namespace djb::conv;
@@ -396,12 +422,13 @@ int launch_tc_inst(djb_nn* h, const djb::conv::Args& a0, cudaStream_t st) {
     const int64_t slots = int64_t(occ) * sms;
     a.zlen = std::min(a.res, kMaxSegment);
     a.nzs = (a.res + a.zlen - 1) / a.zlen;
-    CUtensorMap map{};
+    CUtensorMap map{}, omap{};
     a.use_tma = h->tma && a.res >= kBY && act_map(&map, a.X, a.res, CC, kBX, kBY) ? 1 : 0;
     h->tma_used = h->tma_used || a.use_tma;
+    a.use_ostore = (MODE != kLast && h->tma && a.cout == N && a.res >= kTY && out_map(&omap, a.Y, a.res, a.cout)) ? 1 : 0;
     const int64_t items = int64_t(a.ntx) * a.nty * a.nzs;
     const int grid = int(std::min<int64_t>(items, slots));
-    kern<<<grid, kThreads, bytes, st>>>(a, map);
+    kern<<<grid, kThreads, bytes, st>>>(a, map, omap);
     CUDA_TRY(cudaGetLastError());
     return DJB_OK;
 }
