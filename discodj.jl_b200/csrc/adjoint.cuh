@@ -414,27 +414,69 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
 }
 
 // f1 == null: Ψ̄_a += scale · Σ_n ∂_a W · f0(n); else Ψ̄_a += scale · Σ_c ā_c Σ_n ∂_a W · f_c(n).
-// Each field is staged once per brick over its deposit box; every particle of the brick
-// then adds its share to Ψ̄ (a particle belongs to one brick: no other CTA writes it).
+// fused != 0: every field is staged at once, over the brick's unaligned deposit box,
+// and each particle reads its position, builds its stencil and
+// updates Ψ̄ once. fused == 0 (the boxes do not fit together): one field at a time,
+// each particle adding its share to Ψ̄ per field (a particle belongs to one brick, so
+// no other CTA writes it).
 template <int W>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gather_grad_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     float sx, float sy, float sz, const float* __restrict__ f0, const float* __restrict__ f1,
     const float* __restrict__ f2, const float* __restrict__ abar, float scale, float* __restrict__ psibar, int* err,
-    BrickList bl) {
+    BrickList bl, int fused) {
     extern __shared__ __align__(128) float fbox[];
     const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
     if (cnt == 0) return;
     const int tid = threadIdx.x;
-    const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
     const bool vec = ((pitch | res) & 3) == 0;
     const float resf = float(res);
     const float sh[3] = {sx, sy, sz};
     const int nf = f1 ? 3 : 1;
     LatticeDiv ld;
     ld.init(n);
+    if (fused) {
+        TileBox box = brick_box(bl, b, bl.sos, bl.sSs);
+        box.P = box.S[0];   // rows as for_box_wrapped stages them
+        box.plane = box.P * box.S[1];
+        const int stride = box_stride(box.plane * box.S[2]);
+        for (int f = 0; f < nf; ++f)
+            stage_box_wrapped(fbox + f * stride, f == 0 ? f0 : (f == 1 ? f1 : f2), box, res, pitch, false);
+        __syncthreads();
+        for (unsigned slot = tid; slot < cnt; slot += kTileThreads) {
+            const int64_t p = bl.perm[start + slot];
+            float w[3][W], dw[3][W];
+            int d[3];
+            brick_stencil<W>(psi, q1, ld, np, p, L, resf, res, sh, box, err, w, dw, d);
+            float ac[3] = {1.0f, 0.0f, 0.0f};
+            if (f1) {
+                ac[0] = abar[p];
+                ac[1] = abar[p + np];
+                ac[2] = abar[p + 2 * np];
+            }
+            float v[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+#pragma unroll
+                for (int bb = 0; bb < W; ++bb) {
+                    const int o = ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+#pragma unroll
+                    for (int a = 0; a < W; ++a) {
+                        float fv = ac[0] * fbox[o + a];
+                        if (f1) fv += ac[1] * fbox[stride + o + a] + ac[2] * fbox[2 * stride + o + a];
+                        v[0] += dw[0][a] * w[1][bb] * w[2][c] * fv;
+                        v[1] += w[0][a] * dw[1][bb] * w[2][c] * fv;
+                        v[2] += w[0][a] * w[1][bb] * dw[2][c] * fv;
+                    }
+                }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) psibar[p + a * np] += scale * v[a];
+        }
+        return;
+    }
+    const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
 #pragma unroll 1
     for (int f = 0; f < nf; ++f) {
         stage_box_wrapped(fbox, f == 0 ? f0 : (f == 1 ? f1 : f2), box, res, pitch, vec);

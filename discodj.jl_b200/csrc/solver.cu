@@ -1314,18 +1314,23 @@ void launch_vjp_kernels(djb_solver* s, int stage, const float* psi, const float*
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const size_t smem = scatter_smem(s);
         const djb::BrickList bl = brick_list(s);
+        // unaligned deposit box: the fields of a gather staged together
+        const size_t fbox = size_t(djb::box_stride(s->sS * s->sS * s->sS)) * 4;
+        const int nf = stage == 0 ? 3 : 1;
+        const int fused = nf * fbox <= size_t(kBrickSmemMax) ? 1 : 0;
+        const size_t gsmem = fused ? nf * fbox : smem;
         if (stage == 0)
-            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
+            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, gsmem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, s->adj[0], s->adj[1], s->adj[2],
-                abar, scale, psibar, s->err, bl);
+                abar, scale, psibar, s->err, bl, fused);
         else if (stage == 1)
             djb::k_scatter_weighted_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, abar, scale, s->adj[0], s->adj[1],
                 s->adj[2], s->err, bl);
         else
-            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
+            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, gsmem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, rho, nullptr, nullptr, nullptr,
-                scale, psibar, s->err, bl);
+                scale, psibar, s->err, bl, fused);
         return;
     }
     if (stage == 0)
