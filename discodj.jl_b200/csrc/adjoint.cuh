@@ -145,7 +145,13 @@ __global__ void __launch_bounds__(256) k_scatter_weighted(const float* __restric
 // Both stencil kernels sweep a column of kFdTX × kFdTY cells along z over kFdZ planes:
 // the z stencil from a register window of 2·kFdR + 1 values of the thread's own column,
 // the x and y stencils from the plane's tile with its halo, staged in shared memory.
-constexpr int kFdTX = 32, kFdTY = 8, kFdZ = 32, kFdR = 3;
+#ifndef DJB_FD_TY
+#define DJB_FD_TY 8
+#endif
+#ifndef DJB_FD_Z
+#define DJB_FD_Z 32
+#endif
+constexpr int kFdTX = 32, kFdTY = DJB_FD_TY, kFdZ = DJB_FD_Z, kFdR = 3;
 
 // Periodic index of any integer (tiles and windows reach past 2·res on small meshes).
 __device__ __forceinline__ int fd_wrap(int v, int res) {
