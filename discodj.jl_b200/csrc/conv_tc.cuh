@@ -2,28 +2,34 @@
 // (tcgen05.mma, accumulator in tensor memory), for the force-correction network.
 //
 // Output tile: 8 (x) × 16 (y) voxels of one z plane = the 128 rows of one M = 128 MMA.
-// A CTA walks columns of such tiles along z. Its input planes are staged in shared
-// memory with a one-voxel halo (10 × 18 positions per plane, periodic wrap), as
-// [plane slot][8-channel chunk][position][8 channels]: in every chunk the 16-byte rows
-// of consecutive positions are contiguous. That is the no-swizzle K-major operand
-// layout with 8-row groups 160 bytes apart (one staged y row), so the A operand of a
-// tap (dx, dy, dz) is the same staged block read from a start address shifted by
-// (dy·10 + dx) rows: the 27 taps need no copies (no im2col).
-// Warp roles (persistent CTAs, producer/consumer mbarriers, no CTA-wide barrier in the
-// loop):
-//   loader (warp 4): planes into a ring of kRing slots, one bulk tensor copy per plane
-//     (5-D map over [z][chunk][y][x][8 channels]) where the halo does not wrap, else
-//     16-byte cp.async with the periodic wrap; completion on the slot's `full` barrier.
-//   MMA (warp 5, one thread): per tile 27 taps × (K / 16) tcgen05.mma of 128 × N × 16
-//     (bf16 operands, float32 accumulation) into one of kAcc tensor-memory
-//     accumulators; commits to the accumulator's `accf` barrier and to the `empty`
-//     barrier of the plane the tile was the last reader of.
-//   epilogue (warps 0-3, tensor-memory lanes 0-127): tcgen05.ld of the accumulator,
-//     `acce` arrive, then bias + ReLU → bf16 rows (hidden layers), bias → float32
-//     channel-major mesh (last layer), or the ReLU mask of the layer below → bf16
-//     (data gradient: the convolution with the flipped, transposed weights).
-// The weights of the layer, [tap][chunk][n][8] (K-major B operand), stay in shared
-// memory for the CTA's whole run.
+// A CTA walks columns of such tiles along z, in segments of up to kMaxSegment tiles.
+// Its input planes are staged in shared memory with a one-voxel halo (10 × 18
+// positions per plane, periodic wrap), as [plane slot][8-channel chunk][position][8
+// channels]: in every chunk the 16-byte rows of consecutive positions are contiguous.
+// That is the no-swizzle K-major operand layout with 8-row groups 160 bytes apart (one
+// staged y row), so the A operand of a tap (dx, dy) is the staged plane read from a
+// start address shifted by (dy·10 + dx) rows: the taps need no copies (no im2col).
+// A staged plane is the kz = 0, 1, 2 input of the tiles z + 1, z, z − 1, whose
+// accumulators are adjacent in tensor memory: one MMA of N = 3 × (output channels) per
+// (dy, dx, K step) serves all three, so each plane is read once per shift.
+// Warp roles (persistent CTAs, producer/consumer mbarriers):
+//   loader (warp 8): planes into a ring of kRing slots (128-byte aligned), one bulk
+//     tensor copy per plane (5-D map over [z][chunk][y][x][8 channels]) where the halo
+//     does not wrap, else 16-byte cp.async with the periodic wrap; completion on the
+//     slot's `full` barrier.
+//   MMA (warp 9, converged; one elected lane issues): per plane, tcgen05.mma of
+//     128 × N·(tiles it feeds) × 16 (bf16 operands, float32 accumulation) per
+//     (dy, dx, K step); commits to the `empty` barrier of the plane and to the `accf`
+//     barrier of the tile the plane completes.
+//   epilogue (warps 0-7, two groups of four on alternate tiles; warp w reads tensor-
+//     memory lanes 32·(w % 4) .. +31): tcgen05.ld of the accumulator, `acce` arrive,
+//     then bias + ReLU → bf16 rows (hidden layers), bias → float32 channel-major mesh
+//     (last layer), or the ReLU mask of the layer below → bf16 (data gradient: the
+//     convolution with the flipped, transposed weights). bf16 tiles leave by one bulk
+//     tensor store each from double-buffered shared-memory staging.
+// The weights of the layer, [dy·3 + dx][chunk][kz·N + n][8] (K-major B operand), stay
+// in shared memory for the CTA's whole run. The x-pair form of the first layer and the
+// weight-gradient kernel are described where they are defined below.
 // Waits are bounded: a wait that runs out sets the error word and the CTA's abort
 // flag; every role then stops, the MMAs and copies in flight are waited for (bounded),
 // and the tensor memory is freed.
