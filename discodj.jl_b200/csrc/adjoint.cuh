@@ -293,17 +293,19 @@ __global__ void k_mesh_affine(const float* __restrict__ in, int res, int pitch, 
 // Position of particle p and, per axis, the weights, their derivatives (grid units per
 // length dgdx) and the stencil's first node relative to the box (clamped into the box
 // with error bit 2 when the binning and this evaluation disagree).
+// p: the particle (its lattice site); io: where its Ψ lives in `psi` (p, or its slot in
+// brick order when the arrays were gathered into that order).
 template <int W>
 __device__ __forceinline__ void brick_stencil(const float* __restrict__ psi, const float* __restrict__ q1,
-                                              const LatticeDiv& ld, int64_t np, int64_t p, float L, float resf,
-                                              int res, const float sh[3], const TileBox& box, int* err,
+                                              const LatticeDiv& ld, int64_t np, int64_t p, int64_t io, float L,
+                                              float resf, int res, const float sh[3], const TileBox& box, int* err,
                                               float (&w)[3][W], float (&dw)[3][W], int (&d)[3]) {
     int ijk[3];
     ld.ijk(p, ijk[0], ijk[1], ijk[2]);
     const float dgdx = resf / L;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float X = psi[p + a * np] + q1[ijk[a]];
+        const float X = psi[io + a * np] + q1[ijk[a]];
         const float g = grid_coord(X + sh[a], L, resf, err);
         const int bb = wbase<W>(g);
 #pragma unroll
@@ -333,7 +335,7 @@ template <int W>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scatter_weighted_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     float sx, float sy, float sz, const float* __restrict__ abar, float scale, float* __restrict__ m0,
-    float* __restrict__ m1, float* __restrict__ m2, int* err, BrickList bl) {
+    float* __restrict__ m1, float* __restrict__ m2, int* err, BrickList bl, int sorted_io) {
     extern __shared__ __align__(128) float wbox[];
     unsigned* qbox = reinterpret_cast<unsigned*>(wbox);
     __shared__ float s_max[kTileThreads / 32];
@@ -358,7 +360,8 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
         if (fixed) {   // the largest |scale · ā_c| of the brick sets the unit
             float m = 0.0f;
             for (unsigned slot = tid; slot < cnt; slot += kTileThreads)
-                m = fmaxf(m, fabsf(scale * abar[int64_t(bl.perm[start + slot]) + comp * np]));
+                m = fmaxf(m, fabsf(scale * abar[(sorted_io ? int64_t(start + slot) : int64_t(bl.perm[start + slot])) +
+                                                comp * np]));
             for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
             if ((tid & 31) == 0) s_max[tid >> 5] = m;
         }
@@ -381,10 +384,11 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
             const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
             if (slot >= cnt) continue;
             const int64_t p = bl.perm[start + slot];
-            const float av = scale * abar[p + comp * np] * up;
+            const int64_t io = sorted_io ? int64_t(start + slot) : p;
+            const float av = scale * abar[io + comp * np] * up;
             float w[3][W], dw[3][W];
             int d[3];
-            brick_stencil<W>(psi, q1, ld, np, p, L, resf, res, sh, box, comp == 0 ? err : nullptr, w, dw, d);
+            brick_stencil<W>(psi, q1, ld, np, p, io, L, resf, res, sh, box, comp == 0 ? err : nullptr, w, dw, d);
 #pragma unroll
             for (int c = 0; c < W; ++c)
 #pragma unroll
@@ -420,17 +424,16 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
 }
 
 // f1 == null: Ψ̄_a += scale · Σ_n ∂_a W · f0(n); else Ψ̄_a += scale · Σ_c ā_c Σ_n ∂_a W · f_c(n).
-// fused != 0: every field is staged at once, over the brick's unaligned deposit box,
-// and each particle reads its position, builds its stencil and
-// updates Ψ̄ once. fused == 0 (the boxes do not fit together): one field at a time,
-// each particle adding its share to Ψ̄ per field (a particle belongs to one brick, so
-// no other CTA writes it).
+// One field at a time is staged over the brick's deposit box (16-byte copies); every
+// particle of the brick adds its share to Ψ̄ per field (a particle belongs to one
+// brick, so no other CTA writes it). sorted_io: psi, abar and psibar are in brick order
+// (slot start + i), read and written coalesced.
 template <int W>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gather_grad_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     float sx, float sy, float sz, const float* __restrict__ f0, const float* __restrict__ f1,
     const float* __restrict__ f2, const float* __restrict__ abar, float scale, float* __restrict__ psibar, int* err,
-    BrickList bl, int fused) {
+    BrickList bl, int sorted_io) {
     extern __shared__ __align__(128) float fbox[];
     const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
@@ -443,45 +446,6 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gath
     const int nf = f1 ? 3 : 1;
     LatticeDiv ld;
     ld.init(n);
-    if (fused) {
-        TileBox box = brick_box(bl, b, bl.sos, bl.sSs);
-        box.P = box.S[0];   // rows as for_box_wrapped stages them
-        box.plane = box.P * box.S[1];
-        const int stride = box_stride(box.plane * box.S[2]);
-        for (int f = 0; f < nf; ++f)
-            stage_box_wrapped(fbox + f * stride, f == 0 ? f0 : (f == 1 ? f1 : f2), box, res, pitch, false);
-        __syncthreads();
-        for (unsigned slot = tid; slot < cnt; slot += kTileThreads) {
-            const int64_t p = bl.perm[start + slot];
-            float w[3][W], dw[3][W];
-            int d[3];
-            brick_stencil<W>(psi, q1, ld, np, p, L, resf, res, sh, box, err, w, dw, d);
-            float ac[3] = {1.0f, 0.0f, 0.0f};
-            if (f1) {
-                ac[0] = abar[p];
-                ac[1] = abar[p + np];
-                ac[2] = abar[p + 2 * np];
-            }
-            float v[3] = {0.0f, 0.0f, 0.0f};
-#pragma unroll
-            for (int c = 0; c < W; ++c)
-#pragma unroll
-                for (int bb = 0; bb < W; ++bb) {
-                    const int o = ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
-#pragma unroll
-                    for (int a = 0; a < W; ++a) {
-                        float fv = ac[0] * fbox[o + a];
-                        if (f1) fv += ac[1] * fbox[stride + o + a] + ac[2] * fbox[2 * stride + o + a];
-                        v[0] += dw[0][a] * w[1][bb] * w[2][c] * fv;
-                        v[1] += w[0][a] * dw[1][bb] * w[2][c] * fv;
-                        v[2] += w[0][a] * w[1][bb] * dw[2][c] * fv;
-                    }
-                }
-#pragma unroll
-            for (int a = 0; a < 3; ++a) psibar[p + a * np] += scale * v[a];
-        }
-        return;
-    }
     const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
 #pragma unroll 1
     for (int f = 0; f < nf; ++f) {
@@ -489,10 +453,11 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gath
         __syncthreads();
         for (unsigned slot = tid; slot < cnt; slot += kTileThreads) {
             const int64_t p = bl.perm[start + slot];
+            const int64_t io = sorted_io ? int64_t(start + slot) : p;
             float w[3][W], dw[3][W];
             int d[3];
-            brick_stencil<W>(psi, q1, ld, np, p, L, resf, res, sh, box, f == 0 ? err : nullptr, w, dw, d);
-            const float af = scale * (f1 ? abar[p + f * np] : 1.0f);
+            brick_stencil<W>(psi, q1, ld, np, p, io, L, resf, res, sh, box, f == 0 ? err : nullptr, w, dw, d);
+            const float af = scale * (f1 ? abar[io + f * np] : 1.0f);
             float v[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
             for (int c = 0; c < W; ++c)
@@ -508,9 +473,29 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gath
                     }
                 }
 #pragma unroll
-            for (int a = 0; a < 3; ++a) psibar[p + a * np] += af * v[a];
+            for (int a = 0; a < 3; ++a) psibar[io + a * np] += af * v[a];
         }
         __syncthreads();
+    }
+}
+
+// dst[c·np + t] = src[c·np + perm[t]]: three components into brick order.
+__global__ void k_gather_sorted3(const float* __restrict__ src, const int* __restrict__ perm, int64_t np,
+                                 float* __restrict__ dst) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < np; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t p = perm[t];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[c * np + t] = src[c * np + p];
+    }
+}
+
+// dst[c·np + perm[t]] += src[c·np + t]: back from brick order (perm is a permutation).
+__global__ void k_scatter_add_sorted3(const float* __restrict__ src, const int* __restrict__ perm, int64_t np,
+                                      float* __restrict__ dst) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < np; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t p = perm[t];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[c * np + p] += src[c * np + t];
     }
 }
 

@@ -753,8 +753,8 @@ struct djb_solver {
     bool zpass = false;
     float2* wN = nullptr;
     float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
-    float* scr[8] = {};     // staging and work buffers of the adjoint entry points, kept between calls
-    size_t scr_n[8] = {};
+    float* scr[10] = {};    // staging and work buffers of the adjoint entry points, kept between calls
+    size_t scr_n[10] = {};
     int nsm = 148;  // SMs of the device (persistent grids)
     // brick boxes (brick.cuh): width along x, extent along y and z, first node relative
     // to the brick's first cell; g = interpolation, s = mass assignment
@@ -788,6 +788,28 @@ struct djb_solver {
     int64_t bytes = 0;
     std::vector<void*> allocs;
 };
+
+// Work buffer `slot` of at least `count` floats, kept by the solver between calls (a
+// per-call allocation and release of gigabytes made the adjoint's time vary by 3x).
+int scratch(djb_solver* s, int slot, size_t count, float** out) {
+    if (s->scr_n[slot] < count) {
+        if (s->scr[slot]) {
+            CUDA_TRY(cudaStreamSynchronize(s->stream));
+            cudaFree(s->scr[slot]);
+            s->scr[slot] = nullptr;
+            s->scr_n[slot] = 0;
+        }
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&s->scr[slot]), count * sizeof(float));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            s->scr[slot] = nullptr;
+            return fail(DJB_ERR_ALLOC, "work buffer allocation of %zu floats failed: %s", count, cudaGetErrorString(e));
+        }
+        s->scr_n[slot] = count;
+    }
+    *out = s->scr[slot];
+    return DJB_OK;
+}
 
 namespace {
 
@@ -1304,6 +1326,7 @@ dim3 fd_grid(int res) {
                 unsigned((res + djb::kFdZ - 1) / djb::kFdZ));
 }
 
+// perm != null: psi, abar and psibar are in brick order (gathered through perm).
 template <int W>
 void launch_vjp_kernels(djb_solver* s, int stage, const float* psi, const float* abar, float* psibar,
                         const Shift3& sh, float scale, const int* perm) {
@@ -1314,23 +1337,18 @@ void launch_vjp_kernels(djb_solver* s, int stage, const float* psi, const float*
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const size_t smem = scatter_smem(s);
         const djb::BrickList bl = brick_list(s);
-        // unaligned deposit box: the fields of a gather staged together
-        const size_t fbox = size_t(djb::box_stride(s->sS * s->sS * s->sS)) * 4;
-        const int nf = stage == 0 ? 3 : 1;
-        const int fused = nf * fbox <= size_t(kBrickSmemMax) ? 1 : 0;
-        const size_t gsmem = fused ? nf * fbox : smem;
         if (stage == 0)
-            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, gsmem, s->stream>>>(
+            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, s->adj[0], s->adj[1], s->adj[2],
-                abar, scale, psibar, s->err, bl, fused);
+                abar, scale, psibar, s->err, bl, 1);
         else if (stage == 1)
             djb::k_scatter_weighted_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, abar, scale, s->adj[0], s->adj[1],
-                s->adj[2], s->err, bl);
+                s->adj[2], s->err, bl, 1);
         else
-            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, gsmem, s->stream>>>(
+            djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, rho, nullptr, nullptr, nullptr,
-                scale, psibar, s->err, bl, fused);
+                scale, psibar, s->err, bl, 1);
         return;
     }
     if (stage == 0)
@@ -1376,6 +1394,21 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
         djb::k_place<<<blocks(s->np), 256, 0, s->stream>>>(s->keyrank, s->np, s->offset, s->bsum, s->perm);
         perm = s->perm;
     }
+    // the brick kernels read positions and cotangents in brick order (coalesced) and
+    // accumulate Ψ̄ there; it goes back to the Lagrangian order once at the end
+    const size_t pcount = size_t(3 * s->np);
+    float *psi_s = nullptr, *abar_s = nullptr, *pb_s = nullptr;
+    if (perm) {
+        TRY(scratch(s, 7, pcount, &psi_s));
+        TRY(scratch(s, 8, pcount, &abar_s));
+        TRY(scratch(s, 9, pcount, &pb_s));
+        djb::k_gather_sorted3<<<blocks(s->np), 256, 0, s->stream>>>(psi, perm, s->np, psi_s);
+        djb::k_gather_sorted3<<<blocks(s->np), 256, 0, s->stream>>>(abar, perm, s->np, abar_s);
+        CUDA_TRY(cudaMemsetAsync(pb_s, 0, pcount * sizeof(float), s->stream));
+    }
+    const float* kpsi = perm ? psi_s : psi;
+    const float* kabar = perm ? abar_s : abar;
+    float* kpb = perm ? pb_s : psibar;
     for (int si = 0; si < s->nshift; ++si) {
         const GroupShifts g = group_shifts(s, si, 1);
         const Shift3 sh = g.s[0];
@@ -1401,14 +1434,15 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
         TRY(poisson(s, 0));  // φ
         djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(rho, s->res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
                                                     s->adj[2]);
-        vjp_kernels(s, 0, psi, abar, psibar, sh, inv_ns, perm);  // interpolation weights
+        vjp_kernels(s, 0, kpsi, kabar, kpb, sh, inv_ns, perm);  // interpolation weights
         for (int c = 0; c < 3; ++c) CUDA_TRY(cudaMemsetAsync(s->adj[c], 0, rho_floats * sizeof(float), s->stream));
-        vjp_kernels(s, 1, psi, abar, psibar, sh, inv_ns, perm);  // Ḡ
+        vjp_kernels(s, 1, kpsi, kabar, kpb, sh, inv_ns, perm);  // Ḡ
         djb::k_fd_div3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(s->adj[0], s->adj[1], s->adj[2], s->res, pitch, s->c1, s->c2,
                                                    s->c3, rho);  // φ̄
         TRY(poisson(s, 0));                                    // ρ̄
-        vjp_kernels(s, 2, psi, abar, psibar, sh, 1.0f, perm);  // deposit weights
+        vjp_kernels(s, 2, kpsi, kabar, kpb, sh, 1.0f, perm);  // deposit weights
     }
+    if (perm) djb::k_scatter_add_sorted3<<<blocks(s->np), 256, 0, s->stream>>>(pb_s, perm, s->np, psibar);
     CUDA_TRY(cudaGetLastError());
     return DJB_OK;
 }
@@ -1735,28 +1769,6 @@ struct Stage {
     float* p = nullptr;
     bool owned = false;
 };
-
-// Work buffer `slot` of at least `count` floats, kept by the solver between calls (a
-// per-call allocation and release of gigabytes made the adjoint's time vary by 3x).
-int scratch(djb_solver* s, int slot, size_t count, float** out) {
-    if (s->scr_n[slot] < count) {
-        if (s->scr[slot]) {
-            CUDA_TRY(cudaStreamSynchronize(s->stream));
-            cudaFree(s->scr[slot]);
-            s->scr[slot] = nullptr;
-            s->scr_n[slot] = 0;
-        }
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&s->scr[slot]), count * sizeof(float));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            s->scr[slot] = nullptr;
-            return fail(DJB_ERR_ALLOC, "work buffer allocation of %zu floats failed: %s", count, cudaGetErrorString(e));
-        }
-        s->scr_n[slot] = count;
-    }
-    *out = s->scr[slot];
-    return DJB_OK;
-}
 
 // Device inputs are used in place; host inputs are copied (or work buffers zeroed) into
 // the solver's work buffer `slot`.
