@@ -584,7 +584,8 @@ int check_derr(djb_nn* h) {
 int ensure_work(djb_nn* h, int res, bool train) {
     const int64_t nvox = int64_t(res) * res * res;
     const bool im2col = any_im2col(h);
-    if (h->res == res && (h->work_train || !train) && (h->work_im2col || !im2col)) return DJB_OK;
+    if (h->res == res && (h->work_train || !train) && (h->work_im2col || !im2col) && (h->act0p || !use_pair(h)))
+        return DJB_OK;
     free_work(h);
     const int C = cmax(h);
     // chunks of whole z planes holding at most 4 Mi voxels (col: 27·C bf16 per voxel,
@@ -594,7 +595,7 @@ int ensure_work(djb_nn* h, int res, bool train) {
     h->chunk = train ? nvox : planes * res * res;
     for (int l = 0; l < h->layers; ++l)
         TRYN(dalloc(h, (void**)&h->act[l], size_t(nvox) * h->cinp[l] * sizeof(__nv_bfloat16), true));
-    TRYN(dalloc(h, (void**)&h->act0p, size_t(nvox) * 8 * sizeof(__nv_bfloat16), true));
+    if (use_pair(h)) TRYN(dalloc(h, (void**)&h->act0p, size_t(nvox) * 8 * sizeof(__nv_bfloat16), true));
     if (im2col) TRYN(dalloc(h, (void**)&h->col, size_t(h->chunk) * 27 * C * sizeof(__nv_bfloat16), true));
     if (im2col) TRYN(dalloc(h, (void**)&h->Y, size_t(h->chunk) * C * sizeof(float), true));
     TRYN(dalloc(h, (void**)&h->outm, size_t(nvox) * h->cout[h->layers - 1] * sizeof(float), true));
