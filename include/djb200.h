@@ -190,7 +190,7 @@ DJB_API int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logari
  * restatements. They cover finite-difference gradients (grad_order 2/4/6) without
  * sheet resampling (DJB_ERR_INVALID otherwise). Arrays are (n,n,n,3) Float32 in
  * the memory `mem` names; the calls wait for the GPU before returning. The solver
- * keeps its adjoint work areas between calls (three meshes and up to six particle
+ * keeps its adjoint work areas between calls (three meshes and up to nine particle
  * arrays of 3*n^3 floats) until djb_solver_destroy.
  *
  * psi_bar = (d acc / d psi)^T acc_bar, acc = djb_pm_acceleration(psi): the
