@@ -5,19 +5,24 @@
 // Inputs and outputs cross the C ABI as float32 meshes in the solver's layout,
 // [channel][z][y][x]; inside, activations are bf16 channels-last, [voxel][channel].
 //
-// Each convolution whose padded channel counts are at most 32 runs as an implicit GEMM
-// on the tensor cores (tcgen05.mma, `conv_tc.cuh`): input planes staged in shared memory
-// once, the 27 taps read as shifted operand views, the accumulator in tensor memory,
-// bias + ReLU fused into the epilogue. Wider layers, the backward pass, and every layer
-// after djb_nn_set_conv(h, 1), make the implicit GEMM explicit per chunk of z planes:
+// Every convolution whose padded channel counts are at most 32 runs on the tensor cores
+// (tcgen05.mma, `conv_tc.cuh`), forward and backward:
+//   forward        k_conv3_tc: input planes staged in shared memory once, the taps
+//                  read as shifted operand views, accumulators in tensor memory, bias
+//                  + ReLU fused into the epilogue (the first layer from x-pair rows);
+//   data gradient  k_conv3_tc with the weights flipped and transposed, ReLU′ of the
+//                  layer below fused into the epilogue;
+//   weight grad.   k_conv3_wgrad (inputs narrower than 32 channels zero-widened first).
+// Wider layers, and every layer after djb_nn_set_conv(h, 1), make the implicit GEMM
+// explicit per chunk of z planes:
 //   col[v][tap·C + c] = X[v + offset(tap)][c]        k_im2col (bf16, periodic wrap)
 //   Y = col · W  (M = voxels, K = 27·C, N = channels out; bf16 operands, float32
 //                 accumulation on the tensor cores through cuBLAS)
 //   X' = relu(Y + b) → bf16                           k_bias_act
-// Backward, per layer from the last: dY (ReLU mask applied), dW = colᵀ·dY and
-// dcol = dY·Wᵀ (cuBLAS), db = Σ_v dY, dX[v] = Σ_tap dcol[v − offset(tap)][tap]
-// (k_col2im, a gather: no atomics). Loss: mean squared error over all outputs.
-// Optimizer: Adam on float32 master weights, then the bf16 copies the GEMMs read.
+// and their backward: dW = colᵀ·dY and dcol = dY·Wᵀ (cuBLAS), dX[v] = Σ_tap
+// dcol[v − offset(tap)][tap] (k_col2im, a gather: no atomics). db = Σ_v dY (a block
+// reduction). Loss: mean squared error over all outputs. Optimizer: Adam on float32
+// master weights, then the bf16 copies the kernels read.
 // Channel counts are padded to multiples of 8 (16-byte rows for the tensor cores);
 // the padding channels hold zeros and their weights stay zero.
 #include <cublas_v2.h>

@@ -237,9 +237,9 @@ DJB_API int djb_nn_param_count(const djb_nn* h, int64_t* count);
 DJB_API int djb_nn_get_params(djb_nn* h, float* params);
 DJB_API int djb_nn_load(djb_nn* h, const float* params);
 DJB_API int djb_nn_set_stream(djb_nn* h, void* stream);
-/* Convolution path: 0 (default) = implicit GEMM on the tcgen05 tensor cores for the
- * forward convolutions whose padded channel counts are at most 32 (others, and the
- * backward pass, use im2col + cuBLAS GEMMs); 1 = im2col + cuBLAS for every layer. */
+/* Convolution path: 0 (default) = implicit GEMMs on the tcgen05 tensor cores, forward
+ * and backward, for the layers whose padded channel counts are at most 32 (wider ones
+ * use im2col + cuBLAS GEMMs); 1 = im2col + cuBLAS for every layer. */
 DJB_API int djb_nn_set_conv(djb_nn* h, int32_t mode);
 /* The convolution path in use; *tma_used = 1 once a tensor-core convolution has staged
  * planes by bulk tensor copies (the driver accepted the plane tensor map). */
