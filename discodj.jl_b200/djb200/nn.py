@@ -1,8 +1,8 @@
 """Force-correction network on the PM mesh (no counterpart in the reference).
 
 A 3-D CNN with 3³ kernels and periodic boundaries over libdjb200's `djb_nn_*`
-entry points: bf16 tensor-core GEMMs with float32 accumulation, float32 master
-weights, Adam. Meshes are (channels, res, res, res) float32 in the library's memory
+entry points: implicit GEMMs on the tcgen05 tensor cores (bf16 operands, float32
+accumulation in tensor memory), float32 master weights, Adam. Meshes are (channels, res, res, res) float32 in the library's memory
 order [c][z][y][x]: numpy arrays on the host, or torch CUDA tensors.
 """
 from __future__ import annotations
@@ -61,9 +61,9 @@ class ForceNet:
         check(lib.djb_nn_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
 
     def set_conv(self, mode: str):
-        """"tensor" (default): forward convolutions as implicit GEMMs on the tcgen05
-        tensor cores where the padded channel counts are at most 32; "im2col": im2col +
-        cuBLAS GEMMs for every layer."""
+        """"tensor" (default): convolutions, forward and backward, as implicit GEMMs on
+        the tcgen05 tensor cores where the padded channel counts are at most 32;
+        "im2col": im2col + cuBLAS GEMMs for every layer."""
         modes = {"tensor": 0, "im2col": 1}
         if mode not in modes:
             raise ValueError(f"conv mode must be one of {sorted(modes)}")
