@@ -13,6 +13,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -41,18 +42,35 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(ROOT, "_build")
+    os.makedirs(objdir, exist_ok=True)
     nvcc = os.path.join(CUDA_HOME, "bin", "nvcc")
-    cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "-Xptxas", "-warn-spills",
-           f"-I{INCLUDE}", f"-I{CSRC}", *sources(), "-o", LIB + ".tmp",
-           f"-L{CUDA_HOME}/lib64", "-lcufft", "-lcublas", f"-Xlinker", f"-rpath,{CUDA_HOME}/lib64"]
+    common = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-fvisibility=hidden", "-Xptxas", "-warn-spills", f"-I{INCLUDE}", f"-I{CSRC}"]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [*common, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return obj, r
+
+    # one nvcc per translation unit, in parallel, then one link
+    with ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, sources()))
+    for obj, r in results:
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed ({r.returncode}) on {obj}:\n{r.stdout}\n{r.stderr}")
+        if verbose and (r.stdout or r.stderr):
+            print(r.stdout, r.stderr)
+    cmd = [nvcc, *ARCH, "--shared", *[o for o, _ in results], "-o", LIB + ".tmp",
+           f"-L{CUDA_HOME}/lib64", "-lcufft", "-lcublas", "-Xlinker", f"-rpath,{CUDA_HOME}/lib64"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
-    if verbose and (r.stdout or r.stderr):
-        print(r.stdout, r.stderr)
+        raise RuntimeError(f"nvcc link failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -173,6 +173,20 @@ __device__ __forceinline__ void for_box_wrapped(const TileBox& box, int res, int
 #endif
 constexpr int kScatterBoxes = DJB_SCATTER_BOXES;
 
+// Fixed-point unit of a brick of `cnt` particles. A node sum is at most
+// cnt * (MaxW3 * up + 1) (each rounded weight is below its value + 1), which must stay
+// below 2^32. Sparse bricks keep FixScale<W>::up; denser ones take the largest power of
+// two that keeps the bound, down to 2^20 (unit ~1e-6 of a particle's weight sum). Below
+// that the brick accumulates in float with shared float atomics (returns 0).
+template <int W>
+__device__ __forceinline__ float brick_fixed_unit(unsigned cnt) {
+    const float room = 4294967296.0f / float(cnt) - 1.0f;  // MaxW3 * up must stay below this
+    if (room >= MaxW3<W>::v * FixScale<W>::up) return FixScale<W>::up;
+    int e;
+    frexpf(room / MaxW3<W>::v, &e);  // room / MaxW3 in [2^(e-1), 2^e)
+    return (e - 1 >= 20) ? ldexpf(1.0f, e - 1) : 0.0f;
+}
+
 template <int W, int NS>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scatter_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
@@ -191,6 +205,11 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
     const float resf = float(res);
     const int cells = box.plane * box.S[2];  // a multiple of 4
     const int stride = box_stride(cells);    // boxes start on 128-byte boundaries (bulk tensor copies)
+    // 32-bit fixed point with a unit that keeps every node sum of this brick below 2^32;
+    // bricks too dense for that accumulate float sums (sacc then holds floats)
+    const float up = brick_fixed_unit<W>(cnt);
+    const bool fixed = up > 0.0f;
+    const float down = fixed ? 1.0f / up : 1.0f;
     LatticeDiv ld;
     ld.init(n);
 #pragma unroll 1
@@ -227,27 +246,40 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
                         d[a] = d[a] < 0 ? 0 : box.S[a] - W;
                     }
                 }
+                if (fixed) {
 #pragma unroll
-                for (int c = 0; c < W; ++c)
+                    for (int c = 0; c < W; ++c)
 #pragma unroll
-                    for (int bb = 0; bb < W; ++bb) {
-                        unsigned int* row = acc + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
-                        const float wyz = w[1][bb];
+                        for (int bb = 0; bb < W; ++bb) {
+                            unsigned int* row = acc + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+                            const float wyz = w[1][bb] * up;
 #pragma unroll
-                        for (int a = 0; a < W; ++a)
-                            atomicAdd(row + a, __float2uint_rn(w[0][a] * wyz * w[2][c] * FixScale<W>::up));
-                    }
+                            for (int a = 0; a < W; ++a) atomicAdd(row + a, __float2uint_rn(w[0][a] * wyz * w[2][c]));
+                        }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < W; ++c)
+#pragma unroll
+                        for (int bb = 0; bb < W; ++bb) {
+                            float* row =
+                                reinterpret_cast<float*>(acc) + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+                            const float wyz = w[1][bb];
+#pragma unroll
+                            for (int a = 0; a < W; ++a) atomicAdd(row + a, w[0][a] * wyz * w[2][c]);
+                        }
+                }
             }
         }
         __syncthreads();
         if (bulk) {
             // fixed point -> float in place, then one bulk reduction per box
-            for (int t = 4 * tid; t < NB * stride; t += 4 * kTileThreads) {
-                const uint4 v = *reinterpret_cast<const uint4*>(sacc + t);
-                *reinterpret_cast<float4*>(sacc + t) =
-                    make_float4(__uint2float_rn(v.x) * FixScale<W>::down, __uint2float_rn(v.y) * FixScale<W>::down,
-                                __uint2float_rn(v.z) * FixScale<W>::down, __uint2float_rn(v.w) * FixScale<W>::down);
-            }
+            if (fixed)
+                for (int t = 4 * tid; t < NB * stride; t += 4 * kTileThreads) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(sacc + t);
+                    *reinterpret_cast<float4*>(sacc + t) =
+                        make_float4(__uint2float_rn(v.x) * down, __uint2float_rn(v.y) * down,
+                                    __uint2float_rn(v.z) * down, __uint2float_rn(v.w) * down);
+                }
             fence_proxy_async_smem();  // the conversions are read by the bulk copies below
             __syncthreads();
             if (tid == 0) {
@@ -262,15 +294,15 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
                 float* mesh = (g0 + gb == 0) ? mesh0 : mesh1;
                 const unsigned int* acc = sacc + gb * stride;
                 for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
+                    // float sums (dense bricks) are read as their bit patterns: +0.0f is 0u
+                    const auto val = [&](unsigned v) { return fixed ? __uint2float_rn(v) * down : __uint_as_float(v); };
                     if (vec) {
                         const uint4 v = *reinterpret_cast<const uint4*>(acc + so);
                         if ((v.x | v.y | v.z | v.w) == 0u) return;
-                        red_add_v4(mesh + go, __uint2float_rn(v.x) * FixScale<W>::down,
-                                   __uint2float_rn(v.y) * FixScale<W>::down, __uint2float_rn(v.z) * FixScale<W>::down,
-                                   __uint2float_rn(v.w) * FixScale<W>::down);
+                        red_add_v4(mesh + go, val(v.x), val(v.y), val(v.z), val(v.w));
                     } else {
                         const unsigned v = acc[so];
-                        if (v != 0u) atomicAdd(mesh + go, __uint2float_rn(v) * FixScale<W>::down);
+                        if (v != 0u) atomicAdd(mesh + go, val(v));
                     }
                 });
             }

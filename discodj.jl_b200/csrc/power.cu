@@ -256,6 +256,15 @@ int noalloc_scratch(int device, unsigned char** out) {
     return DJB_OK;
 }
 
+// Makes a device current for the guard's lifetime and gives the calling thread its
+// previous current device back on every return path.
+struct DeviceGuard {
+    int prev = -1;
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -271,6 +280,8 @@ int djb_power_spectrum_shells_noalloc(const void* spectrum, int32_t res, double 
                     "bins = %d exceeds the %d bins of the non-allocating shell sums (use djb_power_spectrum)",
                     bins, kNoAllocBins);
     if (!(boxsize > 0)) return fail(DJB_ERR_INVALID, "boxsize must be positive");
+    DeviceGuard guard;  // the caller's current device is restored on return
+    CUDA_TRY(cudaGetDevice(&guard.prev));
     CUDA_TRY(cudaSetDevice(device));
     unsigned char* base = nullptr;
     int rc = noalloc_scratch(device, &base);

@@ -132,6 +132,18 @@ struct FixScale {
     static constexpr float down = 1.0f / up;
 };
 
+// Largest 3-D weight a particle gives one node: 1 (CIC, d = 0), 0.75^3 (TSC), (2/3)^3 (PCS).
+template <int W>
+struct MaxW3 {
+    static constexpr float v = (W == 2) ? 1.0f : (W == 3) ? 0.421875f : 0.2962963f;
+};
+
+// A tile deposits at most kTileThreads particles, so no node sum of the tiled kernel can
+// pass 2^32 at FixScale (each rounded weight is below its value + 1).
+static_assert(double(kTileThreads) * (MaxW3<2>::v * FixScale<2>::up + 1.0) < 4294967296.0, "CIC tile sum");
+static_assert(double(kTileThreads) * (MaxW3<3>::v * FixScale<3>::up + 1.0) < 4294967296.0, "TSC tile sum");
+static_assert(double(kTileThreads) * (MaxW3<4>::v * FixScale<4>::up + 1.0) < 4294967296.0, "PCS tile sum");
+
 #ifndef DJB_SCATTER_MIN_BLOCKS
 #define DJB_SCATTER_MIN_BLOCKS 2
 #endif

@@ -41,10 +41,18 @@ def power_spectrum_shells_noalloc(spectrum, boxsize: float, bins: int = 20, loga
     """Shell sums of a device half spectrum without any device allocation
     (`djb_power_spectrum_shells_noalloc`). `spectrum` is a contiguous complex64 CUDA
     tensor of shape (res, res, res//2+1) indexed [kz, ky, kx], e.g.
-    `torch.fft.rfftn(field_zyx, dim=(0, 1, 2))` of a field stored [iz, iy, ix]."""
+    `torch.fft.rfftn(field_zyx, dim=(0, 1, 2))` of a field stored [iz, iy, ix].
+    `stream` (a cudaStream_t as an int) defaults to torch's current stream on the
+    spectrum's device, so a spectrum still being written there is read after it is done."""
+    import torch
+
+    if not (isinstance(spectrum, torch.Tensor) and spectrum.is_cuda and spectrum.dtype == torch.complex64):
+        raise ValueError("spectrum must be a complex64 CUDA tensor")
     res = int(spectrum.shape[0])
     if tuple(spectrum.shape) != (res, res, res // 2 + 1) or not spectrum.is_contiguous():
         raise ValueError("spectrum must be a contiguous (res, res, res//2+1) complex64 tensor")
+    if stream is None:
+        stream = torch.cuda.current_stream(spectrum.device).cuda_stream
     k = np.empty(bins)
     pk = np.empty(bins)
     nm = np.empty(bins, dtype=np.int64)

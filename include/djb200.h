@@ -17,6 +17,9 @@
  *
  * Threading: one solver per stream; calls on one solver are not re-entrant.
  * Calls are synchronous with respect to the host unless stated otherwise.
+ * Entry points make the device they work on (the solver's, the network's, or the
+ * `device` argument) current on the calling thread and leave it current, except
+ * djb_power_spectrum_shells_noalloc, which restores the caller's device.
  */
 #ifndef DJB200_H
 #define DJB200_H
@@ -277,8 +280,10 @@ DJB_API int djb_nn_train_step(djb_nn* h, const float* in, const float* target, i
  * it, so make that first call before any stream capture begins. All calls share
  * the one array, which keeps the last call's contents (each call clears the sums
  * it uses): calls that overlap on the GPU, on different streams or threads, race.
- * Runs on `stream` (a cudaStream_t, NULL = legacy default) of `device` and waits
- * for it before returning. Same results as djb_power_spectrum for the same field. */
+ * Runs on `stream` (a cudaStream_t, NULL = legacy default) of `device`. Every call
+ * copies the sums into host stack arrays and synchronises `stream` before it
+ * returns. The calling thread's current device is the same after the call as
+ * before it. Same results as djb_power_spectrum for the same field. */
 DJB_API int djb_power_spectrum_shells_noalloc(const void* spectrum, int32_t res, double boxsize,
                                               int32_t bins, int32_t logarithmic, double scale2,
                                               double* k, double* pk, int64_t* nmodes, void* stream,

@@ -13,7 +13,11 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "discodj.jl_b200"))
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "jax_nbody_reference.npz")
-REFERENCE_H5 = "/root/reference/native/DiscoDJNative/test/reference/jax_nbody_reference.h5"
+# The reference checkout (yipihey/DiscoDJ.jl), when one is present: its root directory is
+# named by DISCODJ_REFERENCE. Tests that read it skip when it is unset or missing.
+REFERENCE_ROOT = os.environ.get("DISCODJ_REFERENCE", "")
+REFERENCE_H5 = os.path.join(REFERENCE_ROOT, "native", "DiscoDJNative", "test", "reference",
+                            "jax_nbody_reference.h5") if REFERENCE_ROOT else ""
 
 
 def pytest_configure(config):

@@ -23,7 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 from h5lite import H5File  # noqa: E402
 
-DEFAULT_SRC = "/root/reference/native/DiscoDJNative/test/reference/jax_nbody_reference.h5"
+DEFAULT_SRC = os.path.join(os.environ.get("DISCODJ_REFERENCE", "/root/reference"), "native", "DiscoDJNative",
+                           "test", "reference", "jax_nbody_reference.h5")
 OUT = os.path.join(HERE, "jax_nbody_reference.npz")
 
 

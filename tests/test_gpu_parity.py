@@ -185,3 +185,30 @@ def test_state_calls_need_state(djb, golden):
     with djb.PMSolver(cfg) as S:
         with pytest.raises(djb.DJBError, match="no particle state"):
             S.step(0.1, 1.0, 0.0, 0.1)
+
+
+@pytest.mark.parametrize("W,n,res,clump,aa", [(4, 24, 48, 3000, 0), (4, 24, 48, 3000, 1), (3, 24, 48, 6000, 0),
+                                               (2, 24, 48, 5000, 0), (4, 32, 64, 20000, 0)])
+def test_dense_clump_vs_oracle(djb, W, n, res, clump, aa):
+    """Thousands of particles on one node (a collapsed halo core): the brick deposit's
+    32-bit fixed point must not wrap. `clump` particles sit on one mesh node and the
+    rest stay near their lattice sites. The cases cover a reduced fixed-point unit
+    (PCS with 3000, TSC with 6000 in one brick) and float accumulation (CIC with 5000,
+    PCS with 20000 in one brick, beyond what 32-bit fixed point holds at a 2^-20 unit)."""
+    from oracle import nbody as onb
+    from oracle import pm as opm
+    L = 120.0
+    rng = np.random.default_rng(31 + W + n)
+    psi = 0.3 * rng.standard_normal((n, n, n, 3))
+    X = onb.add_q(psi, L)
+    node = np.array([17.0, 9.0, 30.0]) * (L / res)           # one mesh node
+    idx = rng.choice(n ** 3, size=clump, replace=False)
+    flat = X.reshape(-1, 3)
+    flat[idx] = node
+    q = onb.add_q(np.zeros_like(psi), L)
+    psi = (X - q).astype(np.float32)
+    cfg_o = opm.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=W, grad_order=4, antialias=aa)
+    cfg_d = djb.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=W, grad_order=4, antialias=aa)
+    ref = opm.pm_acceleration(cfg_o, psi.astype(np.float64))
+    got = djb.pm_acceleration(psi, cfg_d)
+    assert rel(got, ref) < ACC_TOL

@@ -21,8 +21,8 @@ def cosmo():
 
 def test_golden_archive_matches_reference_fixture():
     """The committed npz is a faithful conversion of the reference's HDF5 file."""
-    if not os.path.exists(REFERENCE_H5):
-        pytest.skip("reference checkout not present")
+    if not REFERENCE_H5 or not os.path.exists(REFERENCE_H5):
+        pytest.skip("reference checkout not present (set DISCODJ_REFERENCE to its root)")
     from golden.make_golden import extract
 
     src = extract(REFERENCE_H5)
@@ -109,3 +109,11 @@ def test_invalid_options_raise():
         opm.pm_acceleration(cfg, np.zeros((16, 16, 16, 3)))
     with pytest.raises(ValueError, match="antialias"):
         opm.aa_shifts(5, 0.1)
+
+
+def test_oracle_zeldovich_shape_matches_fixture(golden):
+    """The oracle's 1LPT shape −∇φ (used for the CPU-side ICs) reproduces the fixture's
+    psi1 from its fphi (nbody_parity_tests.jl:28-34 tolerance 1e-12)."""
+    from oracle import ics as oi
+    fphi = golden["ics/fphi_re"] + 1j * golden["ics/fphi_im"]
+    assert rel(oi.zeldovich_shape(fphi, 100.0), golden["ics/psi1"]) < 1e-12

@@ -43,7 +43,9 @@ def test_noalloc_matches_allocating_entry_point(djb, res, bins, log):
                            dim=(0, 1, 2)).contiguous()
     torch.cuda.synchronize()
     for _ in range(2):
+        before = torch.cuda.current_device()
         k, p, nm = power.power_spectrum_shells_noalloc(spec, L, bins=bins, logarithmic=log)
+        assert torch.cuda.current_device() == before   # the caller's device is left as it was
         assert np.array_equal(nm, n0)
         assert rel(k, k0) < 1e-13
         nz = n0 > 0
@@ -58,3 +60,14 @@ def test_noalloc_rejects_too_many_bins(djb):
     spec = torch.zeros((16, 16, 9), dtype=torch.complex64, device="cuda")
     with pytest.raises(djb.DJBInvalidOption, match="exceeds the 512 bins"):
         power.power_spectrum_shells_noalloc(spec, 100.0, bins=513)
+
+
+def test_noalloc_rejects_wrong_dtype_or_host_tensor(djb):
+    """Only complex64 device spectra are read; anything else raises before the C call."""
+    import torch
+
+    from djb200 import power
+    with pytest.raises(ValueError, match="complex64 CUDA tensor"):
+        power.power_spectrum_shells_noalloc(torch.zeros((16, 16, 9), dtype=torch.complex128, device="cuda"), 100.0)
+    with pytest.raises(ValueError, match="complex64 CUDA tensor"):
+        power.power_spectrum_shells_noalloc(torch.zeros((16, 16, 9), dtype=torch.complex64), 100.0)
