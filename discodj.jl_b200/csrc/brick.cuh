@@ -481,6 +481,11 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
                 a3[1] = a3[1] / A.nshift_f;
                 a3[2] = a3[2] / A.nshift_f;
             }
+            if (A.last && A.extra) {
+                a3[0] += A.extra[p];
+                a3[1] += A.extra[p + np];
+                a3[2] += A.extra[p + 2 * np];
+            }
             if (A.last && A.step) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {

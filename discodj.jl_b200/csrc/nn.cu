@@ -172,6 +172,15 @@ __global__ void k_mse(const float* __restrict__ out, const float* __restrict__ t
     if (threadIdx.x == 0) atomicAdd(sum, part[0]);
 }
 
+// dY[v][c] = dout[c][v]: a given gradient of the output mesh, in the layout k_mse writes.
+__global__ void k_out_grad(const float* __restrict__ dout, int n, int64_t nvox, float* __restrict__ dY) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nvox * n; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t v = t / n;
+        const int c = int(t - v * n);
+        dY[t] = dout[int64_t(c) * nvox + v];
+    }
+}
+
 // float32 [v][n] → bf16 [v][np] (zeros beyond n), optionally masked by A > 0 (ReLU backward).
 __global__ void k_grad_bf16(const float* __restrict__ dA, int n, int np, const __nv_bfloat16* __restrict__ A,
                             int64_t m, __nv_bfloat16* __restrict__ dY) {
@@ -651,8 +660,9 @@ int forward(djb_nn* h, const float* in) {
     return DJB_OK;
 }
 
-// Backward from the MSE loss against `target` (float32 mesh, device) into h->g; *loss.
-int backward(djb_nn* h, const float* target, double* loss) {
+// Backward from the MSE loss against `target` (float32 mesh, device), or from a given
+// gradient `dout` of the output mesh (target null), into h->g; *loss (MSE only).
+int backward(djb_nn* h, const float* target, double* loss, const float* dout = nullptr) {
     const int res = h->res;
     const int64_t nvox = int64_t(res) * res * res;
     const float one = 1.0f, zero = 0.0f;
@@ -660,8 +670,11 @@ int backward(djb_nn* h, const float* target, double* loss) {
     const int nout = h->cout[L - 1];
     CUDA_TRY(cudaMemsetAsync(h->g, 0, size_t(h->nparam) * sizeof(float), h->stream));
     CUDA_TRY(cudaMemsetAsync(h->lsum, 0, sizeof(double), h->stream));
-    k_mse<<<grid_of(nvox * nout), kNT, 0, h->stream>>>(h->outm, target, nout, nvox, 1.0 / double(nvox * nout), h->dA,
-                                                      h->lsum);
+    if (target)
+        k_mse<<<grid_of(nvox * nout), kNT, 0, h->stream>>>(h->outm, target, nout, nvox, 1.0 / double(nvox * nout),
+                                                          h->dA, h->lsum);
+    else
+        k_out_grad<<<grid_of(nvox * nout), kNT, 0, h->stream>>>(dout, nout, nvox, h->dA);
     // dY of the last layer (bf16, [v][coutp], no activation)
     __nv_bfloat16* dy = h->dY;
     __nv_bfloat16* dy_next = h->dY2;
@@ -696,7 +709,7 @@ int backward(djb_nn* h, const float* target, double* loss) {
         }
         std::swap(dy, dy_next);
     }
-    if (loss) {
+    if (loss && target) {
         double s = 0.0;
         CUDA_TRY(cudaMemcpyAsync(&s, h->lsum, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -896,6 +909,38 @@ int djb_nn_backward(djb_nn* h, const float* in, const float* target, int32_t res
     if (own_t) cudaFreeAsync(dt, h->stream);
     if (rc != DJB_OK) return rc;
     return check_derr(h);
+}
+
+// Gradients of Σ dout · net(in) (dout: the loss gradient with respect to the output mesh)
+// into the network's gradient buffer.
+int djb_nn_backward_output_grad(djb_nn* h, const float* in, const float* dout, int32_t res, int32_t mem) {
+    djb::clear_error();
+    if (!h || !in || !dout) return fail(DJB_ERR_INVALID, "null argument");
+    if (res < 3) return fail(DJB_ERR_INVALID, "res must be >= 3");
+    CUDA_TRY(cudaSetDevice(h->device));
+    TRYN(ensure_work(h, res, true));
+    const int64_t nvox = int64_t(res) * res * res;
+    float *din = nullptr, *dd = nullptr;
+    bool own_in = false, own_d = false;
+    TRYN(stage(h, in, size_t(nvox) * h->cin[0], mem, &din, &own_in));
+    int rc = stage(h, dout, size_t(nvox) * h->cout[h->layers - 1], mem, &dd, &own_d);
+    if (rc == DJB_OK) rc = forward(h, din);
+    if (rc == DJB_OK) rc = backward(h, nullptr, nullptr, dd);
+    if (own_in) cudaFreeAsync(din, h->stream);
+    if (own_d) cudaFreeAsync(dd, h->stream);
+    if (rc != DJB_OK) return rc;
+    return check_derr(h);
+}
+
+int djb_nn_info(const djb_nn* h, int32_t* layers, int32_t* cin, int32_t* hidden, int32_t* cout, int32_t* device) {
+    djb::clear_error();
+    if (!h) return fail(DJB_ERR_INVALID, "null network");
+    if (layers) *layers = h->layers;
+    if (cin) *cin = h->cin[0];
+    if (hidden) *hidden = h->layers > 1 ? h->cout[0] : 0;
+    if (cout) *cout = h->cout[h->layers - 1];
+    if (device) *device = h->device;
+    return DJB_OK;
 }
 
 int djb_nn_grads(djb_nn* h, float* grads, int32_t mem) {

@@ -396,6 +396,7 @@ struct GatherArgs {
     float alpha, beta, dd2;
     int* err;
     const int* perm;    // brick-sorted particle order for the tiled kernels (null: Lagrangian tiles)
+    const float* extra; // (3 blocks of np) added to the final acceleration, or null (network correction)
 };
 
 template <int W, int R, int NS>
@@ -438,6 +439,11 @@ __global__ void __launch_bounds__(kThreads) k_gather(GatherArgs A) {
         acc[1] = acc[1] / A.nshift_f;
         acc[2] = acc[2] / A.nshift_f;
     }
+    if (A.last && A.extra) {
+        acc[0] += A.extra[p];
+        acc[1] += A.extra[p + np];
+        acc[2] += A.extra[p + 2 * np];
+    }
     if (A.last && A.step) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -449,6 +455,97 @@ __global__ void __launch_bounds__(kThreads) k_gather(GatherArgs A) {
         A.acc[p] = acc[0];
         A.acc[p + np] = acc[1];
         A.acc[p + 2 * np] = acc[2];
+    }
+}
+
+// ── mesh <-> particle transfers of three-component fields (force correction) ──
+// out_c(p) = Σ_n W(X_p − n) f_c(n) over the W-order stencil of X_p = q + Ψ_p, for three
+// dense res³ meshes f_c = f + c·res³ ([z][y][x]); the interpolation of pm.jl:344-364
+// applied to given node values, without shifts.
+template <int W>
+__global__ void __launch_bounds__(kThreads) k_interp3(const float* __restrict__ psi, const float* __restrict__ q1,
+                                                      int n, int64_t np, float L, int res,
+                                                      const float* __restrict__ f, float scale,
+                                                      float* __restrict__ out, int* err) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    LatticeDiv ld;
+    ld.init(n);
+    int i, j, k;
+    ld.ijk(p, i, j, k);
+    const float resf = float(res);
+    float wx[W], wy[W], wz[W];
+    int ix[W], iy[W], iz[W];
+    axis_weights<W>(grid_coord(psi[p] + q1[i], L, resf, err), res, wx, ix);
+    axis_weights<W>(grid_coord(psi[p + np] + q1[j], L, resf, err), res, wy, iy);
+    axis_weights<W>(grid_coord(psi[p + 2 * np] + q1[k], L, resf, err), res, wz, iz);
+    const int64_t cells = int64_t(res) * res * res;
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+#pragma unroll
+        for (int b = 0; b < W; ++b) {
+            const int64_t row = (int64_t(iz[c]) * res + iy[b]) * res;
+            const float wyz = wy[b] * wz[c];
+#pragma unroll
+            for (int a = 0; a < W; ++a) {
+                const int64_t o = row + ix[a];
+                const float w = wx[a] * wyz;
+                s0 += w * __ldg(f + o);
+                s1 += w * __ldg(f + cells + o);
+                s2 += w * __ldg(f + 2 * cells + o);
+            }
+        }
+    out[p] = scale * s0;
+    out[p + np] = scale * s1;
+    out[p + 2 * np] = scale * s2;
+}
+
+// The transpose of k_interp3: f_c(n) += Σ_p W(X_p − n) v_c(p) (float atomics).
+template <int W>
+__global__ void __launch_bounds__(kThreads) k_deposit3(const float* __restrict__ psi, const float* __restrict__ q1,
+                                                       int n, int64_t np, float L, int res,
+                                                       const float* __restrict__ v, float* __restrict__ f, int* err) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    LatticeDiv ld;
+    ld.init(n);
+    int i, j, k;
+    ld.ijk(p, i, j, k);
+    const float resf = float(res);
+    float wx[W], wy[W], wz[W];
+    int ix[W], iy[W], iz[W];
+    axis_weights<W>(grid_coord(psi[p] + q1[i], L, resf, err), res, wx, ix);
+    axis_weights<W>(grid_coord(psi[p + np] + q1[j], L, resf, err), res, wy, iy);
+    axis_weights<W>(grid_coord(psi[p + 2 * np] + q1[k], L, resf, err), res, wz, iz);
+    const int64_t cells = int64_t(res) * res * res;
+    const float v0 = v[p], v1 = v[p + np], v2 = v[p + 2 * np];
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+#pragma unroll
+        for (int b = 0; b < W; ++b) {
+            const int64_t row = (int64_t(iz[c]) * res + iy[b]) * res;
+            const float wyz = wy[b] * wz[c];
+#pragma unroll
+            for (int a = 0; a < W; ++a) {
+                const int64_t o = row + ix[a];
+                const float w = wx[a] * wyz;
+                atomicAdd(f + o, w * v0);
+                atomicAdd(f + cells + o, w * v1);
+                atomicAdd(f + 2 * cells + o, w * v2);
+            }
+        }
+}
+
+// out[c][cell] = in[c][cell] · scale[c] for `nc` channels of `cells` floats.
+__global__ void k_scale_channels(const float* __restrict__ in, float* __restrict__ out, int64_t cells, int nc,
+                                 float s0, float s1, float s2, float s3) {
+    const int64_t total = cells * nc;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+         t += int64_t(gridDim.x) * blockDim.x) {
+        const int c = int(t / cells);
+        const float s = c == 0 ? s0 : c == 1 ? s1 : c == 2 ? s2 : s3;
+        out[t] = in[t] * s;
     }
 }
 
@@ -658,7 +755,7 @@ constexpr int kScatterBudget = DJB_SCATTER_BUDGET;
 constexpr int kGatherBudget = DJB_GATHER_BUDGET;
 
 // Phases of a force evaluation, timed with CUDA events on the solver's stream.
-enum Phase { PH_CLEAR = 0, PH_SCATTER, PH_RESAMPLE, PH_R2C, PH_KSPACE, PH_C2R, PH_GATHER, PH_SORT, PH_COUNT };
+enum Phase { PH_CLEAR = 0, PH_SCATTER, PH_RESAMPLE, PH_R2C, PH_KSPACE, PH_C2R, PH_GATHER, PH_SORT, PH_NN, PH_COUNT };
 
 // Launch counts of this library's kernels (always on) and, when enabled, per-phase
 // device time from event pairs recorded around each phase.
@@ -785,6 +882,13 @@ struct djb_solver {
     int* err = nullptr;
     bool have_state = false;
     bool tiled = true;  // shared-memory tiled scatter/gather (DJB_KERNELS=simple selects the per-particle ones)
+    // force correction (djb_solver_attach_nn): network inputs [δ, F_x, F_y, F_z] scaled by
+    // nn_in (δ) and nn_fin (F), its output scaled by nn_out, interpolated to the particles
+    djb_nn* nn = nullptr;
+    float nn_in = 1.0f, nn_fin = 1.0f, nn_out = 1.0f;
+    float* nnf = nullptr;    // 4 res³ meshes (network input)
+    float* nnd = nullptr;    // 3 res³ meshes (network output)
+    float* nnacc = nullptr;  // 3·np particle corrections
     int64_t bytes = 0;
     std::vector<void*> allocs;
 };
@@ -1195,14 +1299,23 @@ int sort_particles(djb_solver* s, const float* mom, float dd1) {
     return DJB_OK;
 }
 
+dim3 fd_grid(int res);
+int nn_correction(djb_solver* s);
+
 int force(djb_solver* s, bool step, double dd1, double alpha, double beta, double dd2) {
     const int nh = s->res / 2 + 1;
     const int64_t nspec = int64_t(s->res) * s->res * nh;
     const bool ik = (s->cfg.grad_order == 0);
     const bool resample = (s->cfg.n_resample > 1);
     s->cur_perm = nullptr;
+    if (s->nn && step && dd1 != 0.0) {
+        // the correction is evaluated at the drifted positions: drift first, then run
+        // the force pipeline without its fused first drift
+        djb::k_drift<<<grid_for(3 * s->np), kThreads, 0, s->stream>>>(s->psi, s->mom, float(dd1), 3 * s->np);
+        dd1 = 0.0;
+    }
     if (s->tiled && s->sorted) {
-        TRY(sort_particles(s, step ? s->mom : nullptr, float(dd1)));
+        TRY(sort_particles(s, (step && dd1 != 0.0) ? s->mom : nullptr, float(dd1)));
         s->cur_perm = s->perm;
     }
     for (int first = 0; first < s->nshift; first += s->group) {
@@ -1214,7 +1327,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             CUDA_TRY(cudaMemsetAsync(rho_mesh(s, m), 0, rho_floats * sizeof(float), s->stream));
         s->prof.end(s->stream, PH_CLEAR, 0);
         // with the brick sort the binning pass has applied the first drift already
-        const bool drift_here = step && first == 0 && !s->cur_perm;
+        const bool drift_here = step && first == 0 && !s->cur_perm && dd1 != 0.0;
         s->prof.begin(s->stream, PH_SCATTER);
         launch_scatter(s, drift_here ? s->mom : nullptr, float(dd1), g, ns);
         s->prof.end(s->stream, PH_SCATTER, 1);
@@ -1230,6 +1343,13 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
             else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
             s->prof.end(s->stream, PH_R2C, 0);
+            // network input, δ: the unshifted density is still in phi[0] after the R2C
+            const bool nn_here = s->nn && first == 0 && m == 0;
+            if (nn_here) {
+                const float f = float(double(s->res) * s->res * s->res / double(s->np));
+                djb::k_mesh_affine<<<grid_for(int64_t(s->res) * s->res * s->res), 256, 0, s->stream>>>(
+                    s->phi[0], s->res, s->res, f * s->nn_in, s->nn_in, s->nnf);
+            }
             if (s->zpass) {
                 s->prof.begin(s->stream, PH_KSPACE);
                 const int nh = s->res / 2 + 1;
@@ -1261,6 +1381,17 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
                                            s->fmesh[m][c]));
                 s->prof.end(s->stream, PH_C2R, 0);
             }
+            if (nn_here) {
+                // network input, F = −Dφ of the unshifted potential; then the network and
+                // the interpolation of its output to the particles
+                const int64_t cells = int64_t(s->res) * s->res * s->res;
+                s->prof.begin(s->stream, PH_NN);
+                djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(
+                    s->phi[0], s->res, s->res, s->c1 * s->nn_fin, s->c2 * s->nn_fin, s->c3 * s->nn_fin,
+                    s->nnf + cells, s->nnf + 2 * cells, s->nnf + 3 * cells);
+                TRY(nn_correction(s));
+                s->prof.end(s->stream, PH_NN, 3);
+            }
         }
         djb::GatherArgs a{};
         a.psi = s->psi;
@@ -1291,6 +1422,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         a.dd2 = float(dd2);
         a.err = s->err;
         a.perm = s->cur_perm;
+        a.extra = s->nn ? s->nnacc : nullptr;
         s->prof.begin(s->stream, PH_GATHER);
         launch_gather(s, a, ns);
         s->prof.end(s->stream, PH_GATHER, 1);
@@ -1324,6 +1456,23 @@ int poisson(djb_solver* s, int m) {
 dim3 fd_grid(int res) {
     return dim3(unsigned((res + djb::kFdTX - 1) / djb::kFdTX), unsigned((res + djb::kFdTY - 1) / djb::kFdTY),
                 unsigned((res + djb::kFdZ - 1) / djb::kFdZ));
+}
+
+// The attached network on its scaled inputs in s->nnf (filled by the force pipeline),
+// then its output, times nn_out, interpolated to the particles at s->psi into s->nnacc.
+int nn_correction(djb_solver* s) {
+    TRY(djb_nn_set_stream(s->nn, s->stream));
+    TRY(djb_nn_apply(s->nn, s->nnf, s->res, s->nnd, DJB_MEM_DEVICE));
+#define DJB_INTERP(W_)                                                                                          \
+    if (s->W == W_)                                                                                             \
+        djb::k_interp3<W_><<<blocks(s->np), kThreads, 0, s->stream>>>(s->psi, s->q1, s->n, s->np, s->Lf, s->res, \
+                                                                      s->nnd, s->nn_out, s->nnacc, s->err);
+    DJB_INTERP(2)
+    DJB_INTERP(3)
+    DJB_INTERP(4)
+#undef DJB_INTERP
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
 }
 
 // perm != null: psi, abar and psibar are in brick order (gathered through perm).
@@ -1891,6 +2040,106 @@ int djb_mesh_fields(djb_solver* s, const float* psi, float* out, int32_t mem) {
     return check_err(s);
 }
 
+int djb_solver_attach_nn(djb_solver* s, djb_nn* net, double delta_scale, double force_scale, double out_scale) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (!net) {
+        s->nn = nullptr;
+        return DJB_OK;
+    }
+    int32_t layers = 0, cin = 0, hidden = 0, cout = 0, dev = -1;
+    TRY(djb_nn_info(net, &layers, &cin, &hidden, &cout, &dev));
+    if (cin != 4 || cout != 3)
+        return fail(DJB_ERR_INVALID, "the force correction needs a network with 4 inputs and 3 outputs (got %d, %d)",
+                    cin, cout);
+    if (dev != s->cfg.device) return fail(DJB_ERR_INVALID, "network and solver are on different devices");
+    // the pipeline reads the unshifted density and potential of its first shift from the
+    // dense meshes of the finite-difference path
+    const bool zero_first = s->shifts.size() >= 3 && s->shifts[0] == 0.0 && s->shifts[1] == 0.0 &&
+                            s->shifts[2] == 0.0;
+    if (!s->phi[0] || s->cfg.grad_order == 0 || s->cfg.n_resample > 1 || !zero_first)
+        return fail(DJB_ERR_INVALID,
+                    "the force correction needs a finite-difference gradient (2/4/6), no resampling, a PMSolver "
+                    "(not lean) with res divisible by 4, and antialias 0 or 1");
+    if (!(std::isfinite(delta_scale) && std::isfinite(force_scale) && std::isfinite(out_scale)))
+        return fail(DJB_ERR_INVALID, "scales must be finite");
+    const int64_t cells = int64_t(s->res) * s->res * s->res;
+    if (!s->nnf) TRY(dmalloc(s, (void**)&s->nnf, sizeof(float) * size_t(4 * cells)));
+    if (!s->nnd) TRY(dmalloc(s, (void**)&s->nnd, sizeof(float) * size_t(3 * cells)));
+    if (!s->nnacc) TRY(dmalloc(s, (void**)&s->nnacc, sizeof(float) * size_t(3 * s->np)));
+    s->nn = net;
+    s->nn_in = float(delta_scale);
+    s->nn_fin = float(force_scale);
+    s->nn_out = float(out_scale);
+    return DJB_OK;
+}
+
+int djb_mesh_interp3(djb_solver* s, const float* psi, const float* mesh3, float* out, int32_t mem) {
+    djb::clear_error();
+    if (!s || !psi || !mesh3 || !out) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    const size_t mcount = size_t(3) * s->res * s->res * s->res;
+    Stage sp, sm, so;
+    int rc = stage_in(s, sp, psi, count, mem, true, 0);
+    if (rc == DJB_OK) rc = stage_in(s, sm, mesh3, mcount, mem, true, 1);
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = stage_in(s, so, nullptr, count, mem, false, 2);
+    float* o = (mem == DJB_MEM_HOST) ? so.p : out;
+    if (rc == DJB_OK) {
+#define DJB_INTERP(W_)                                                                                         \
+    if (s->W == W_)                                                                                            \
+        djb::k_interp3<W_><<<blocks(s->np), kThreads, 0, s->stream>>>(sp.p, s->q1, s->n, s->np, s->Lf, s->res, \
+                                                                      sm.p, 1.0f, o, s->err);
+        DJB_INTERP(2)
+        DJB_INTERP(3)
+        DJB_INTERP(4)
+#undef DJB_INTERP
+        if (cudaGetLastError() != cudaSuccess) rc = fail(DJB_ERR_CUDA, "interpolation kernel launch failed");
+    }
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = copy_out(s, out, o, count, DJB_MEM_HOST);
+    stage_free(s, sp);
+    stage_free(s, sm);
+    stage_free(s, so);
+    if (rc != DJB_OK) return rc;
+    return check_err(s);
+}
+
+int djb_mesh_deposit3(djb_solver* s, const float* psi, const float* vec, float* mesh3, int32_t mem) {
+    djb::clear_error();
+    if (!s || !psi || !vec || !mesh3) return fail(DJB_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    const size_t mcount = size_t(3) * s->res * s->res * s->res;
+    Stage sp, sv, so;
+    int rc = stage_in(s, sp, psi, count, mem, true, 0);
+    if (rc == DJB_OK) rc = stage_in(s, sv, vec, count, mem, true, 1);
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = stage_in(s, so, nullptr, mcount, mem, false, 2);
+    float* o = (mem == DJB_MEM_HOST) ? so.p : mesh3;
+    if (rc == DJB_OK && mem == DJB_MEM_DEVICE) {
+        cudaError_t e = cudaMemsetAsync(o, 0, mcount * sizeof(float), s->stream);
+        if (e != cudaSuccess) rc = fail(DJB_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    }
+    if (rc == DJB_OK) {
+#define DJB_DEPOSIT(W_)                                                                                         \
+    if (s->W == W_)                                                                                             \
+        djb::k_deposit3<W_><<<blocks(s->np), kThreads, 0, s->stream>>>(sp.p, s->q1, s->n, s->np, s->Lf, s->res, \
+                                                                       sv.p, o, s->err);
+        DJB_DEPOSIT(2)
+        DJB_DEPOSIT(3)
+        DJB_DEPOSIT(4)
+#undef DJB_DEPOSIT
+        if (cudaGetLastError() != cudaSuccess) rc = fail(DJB_ERR_CUDA, "deposit kernel launch failed");
+    }
+    if (rc == DJB_OK && mem == DJB_MEM_HOST) rc = copy_out(s, mesh3, o, mcount, DJB_MEM_HOST);
+    stage_free(s, sp);
+    stage_free(s, sv);
+    stage_free(s, so);
+    if (rc != DJB_OK) return rc;
+    return check_err(s);
+}
+
 int djb_pm_acceleration(djb_solver* s, const float* psi, float* acc, int32_t mem) {
     djb::clear_error();
     if (!s || !psi || !acc) return fail(DJB_ERR_INVALID, "null argument");
@@ -1981,8 +2230,7 @@ int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wrap, doub
     float* po = nullptr;
     float* stage = nullptr;
     if (mem == DJB_MEM_HOST) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&stage), 2 * count * sizeof(float), s->stream);
-        if (e != cudaSuccess) return fail(DJB_ERR_ALLOC, "staging allocation failed: %s", cudaGetErrorString(e));
+        TRY(scratch(s, 3, 2 * count, &stage));  // kept between calls, like the adjoint's work areas
         xo = x_out ? stage : nullptr;
         po = p_out ? stage + count : nullptr;
     } else {
@@ -1997,7 +2245,6 @@ int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wrap, doub
         if (x_out) rc = copy_out(s, x_out, xo, count, DJB_MEM_HOST);
         if (rc == DJB_OK && p_out) rc = copy_out(s, p_out, po, count, DJB_MEM_HOST);
     }
-    if (stage) cudaFreeAsync(stage, s->stream);
     if (rc != DJB_OK) return rc;
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return check_err(s);

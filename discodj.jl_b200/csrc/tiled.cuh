@@ -442,6 +442,11 @@ __global__ void __launch_bounds__(kTileThreads, DJB_GATHER_MIN_BLOCKS) k_gather_
         acc[1] = acc[1] / A.nshift_f;
         acc[2] = acc[2] / A.nshift_f;
     }
+    if (A.last && A.extra) {
+        acc[0] += A.extra[p];
+        acc[1] += A.extra[p + np];
+        acc[2] += A.extra[p + 2 * np];
+    }
     if (A.last && A.step) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {

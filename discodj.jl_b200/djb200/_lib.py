@@ -104,6 +104,11 @@ SIGNATURES = {
     "djb_nn_grads": [_P, _P, _I],
     "djb_nn_set_grads": [_P, _P, _I],
     "djb_nn_adam_step": [_P, _D],
+    "djb_nn_backward_output_grad": [_P, _P, _P, _I, _I],
+    "djb_nn_info": [_P, _IP, _IP, _IP, _IP, _IP],
+    "djb_solver_attach_nn": [_P, _P, _D, _D, _D],
+    "djb_mesh_interp3": [_P, _P, _P, _P, _I],
+    "djb_mesh_deposit3": [_P, _P, _P, _P, _I],
 }
 _RESTYPES = {"djb_version": C.c_char_p, "djb_last_error": C.c_char_p}
 

@@ -130,6 +130,16 @@ class ForceNet:
         del k1, k2
         return loss.value
 
+    def backward_output_grad(self, x, dout):
+        """Gradients of Σ dout·net(x) into the network's buffer (dout: the loss gradient
+        with respect to the output mesh, same memory and size as x)."""
+        p, mem, k1, res = self._mesh(x, self.cin)
+        d, mem2, k2, res2 = self._mesh(dout, self.cout)
+        if mem != mem2 or res != res2:
+            raise ValueError("x and dout must live in the same memory and have the same size")
+        check(lib.djb_nn_backward_output_grad(self._h, p, d, res, mem))
+        del k1, k2
+
     def grads(self) -> np.ndarray:
         g = np.empty(self.n_params, dtype=np.float32)
         check(lib.djb_nn_grads(self._h, C.c_void_p(g.ctypes.data), MEM_HOST))

@@ -214,6 +214,38 @@ class PMSolver:
         del keep
         return out
 
+    def attach_nn(self, net, delta_scale: float = 1.0, force_scale: float = 1.0, out_scale: float = 1.0):
+        """Adds out_scale·interp(net([delta_scale·δ, force_scale·F])) to every force of this
+        solver (`djb_solver_attach_nn`); net = None detaches."""
+        check(lib.djb_solver_attach_nn(self._h, net._h if net is not None else None, float(delta_scale),
+                                       float(force_scale), float(out_scale)))
+        self._net = net   # the network must outlive its attachment
+
+    def mesh_interp3(self, psi, mesh3):
+        """(3,n,n,n) device tensor of the W-order interpolation of three res³ meshes
+        ((3,res,res,res) device tensor [c][z][y][x]) at X = q + psi (device, native layout)."""
+        import torch
+        p, mem, keep = _ptr_mem(psi, self.n)
+        if mem != MEM_DEVICE or not mesh3.is_cuda or not mesh3.is_contiguous():
+            raise ValueError("mesh_interp3 takes device tensors")
+        out = torch.empty((3, self.n, self.n, self.n), dtype=torch.float32, device=psi.device)
+        check(lib.djb_mesh_interp3(self._h, p, C.c_void_p(mesh3.data_ptr()), C.c_void_p(out.data_ptr()), mem))
+        del keep
+        return out
+
+    def mesh_deposit3(self, psi, vec):
+        """The transpose of `mesh_interp3`: (3,res,res,res) device tensor."""
+        import torch
+        p, mem, keep = _ptr_mem(psi, self.n)
+        v, mem2, keep2 = _ptr_mem(vec, self.n)
+        if mem != MEM_DEVICE or mem2 != MEM_DEVICE:
+            raise ValueError("mesh_deposit3 takes device tensors")
+        r = int(self.cfg.res_pm)
+        out = torch.empty((3, r, r, r), dtype=torch.float32, device=psi.device)
+        check(lib.djb_mesh_deposit3(self._h, p, v, C.c_void_p(out.data_ptr()), mem))
+        del keep, keep2
+        return out
+
     def set_state(self, psi, mom, mom_scale: float = 1.0):
         n = self.n
         p, mem, k1 = _ptr_mem(psi, n)
@@ -246,7 +278,7 @@ class PMSolver:
     def synchronize(self):
         check(lib.djb_synchronize(self._h))
 
-    PHASES = ("clear", "scatter", "resample", "r2c", "kspace", "c2r", "gather", "sort")
+    PHASES = ("clear", "scatter", "resample", "r2c", "kspace", "c2r", "gather", "sort", "nn")
 
     def profile(self, enable: bool = True):
         """Start (or stop) per-phase CUDA-event timing; resets the sums."""
@@ -254,7 +286,7 @@ class PMSolver:
 
     def profile_read(self) -> dict:
         """{phase: (ms, kernel launches, executions)} since the last read; resets."""
-        n = 8
+        n = len(self.PHASES)
         ms = np.zeros(n)
         la = np.zeros(n, dtype=np.int64)
         ca = np.zeros(n, dtype=np.int64)

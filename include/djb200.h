@@ -163,11 +163,12 @@ DJB_API int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wr
 /* Per-phase timing with CUDA events on the solver's stream (enable = 1) and launch
  * counts of this library's kernels. Phases: 0 mesh clear, 1 mass assignment,
  * 2 sheet resampling, 3 R2C, 4 k-space multiply, 5 C2R, 6 force interpolation
- * (fused kick-drift), 7 particle brick sort. Enabling or disabling resets the sums. */
+ * (fused kick-drift), 7 particle brick sort, 8 network force correction (network inputs,
+ * network, interpolation of its output). Enabling or disabling resets the sums. */
 DJB_API int djb_solver_profile(djb_solver* s, int32_t enable);
 /* Reads and resets the sums: ms[phase] device milliseconds (0 when timing is off),
  * launches[phase] kernel launches of this library, calls[phase] phase executions.
- * nphase >= 8. */
+ * nphase >= 9. */
 DJB_API int djb_solver_profile_read(djb_solver* s, double* ms, int64_t* launches, int64_t* calls,
                                     int32_t nphase);
 /* Waits for the solver's queued work and reports a device-side error word, if any. */
@@ -262,6 +263,33 @@ DJB_API int djb_nn_adam_step(djb_nn* h, double lr);
 /* djb_nn_backward then djb_nn_adam_step; *loss is the loss before the step. */
 DJB_API int djb_nn_train_step(djb_nn* h, const float* in, const float* target, int32_t res, double lr,
                               double* loss, int32_t mem);
+/* Gradients of sum(dout * net(in)) into the gradient buffer, for a loss defined outside the
+ * network: dout (float32 [channel][z][y][x], cout meshes) is the loss gradient with respect
+ * to the network's output (e.g. the transpose of an interpolation to particles,
+ * djb_mesh_deposit3). */
+DJB_API int djb_nn_backward_output_grad(djb_nn* h, const float* in, const float* dout, int32_t res, int32_t mem);
+/* Layer count, input, hidden (0 for one layer) and output channels, and device. */
+DJB_API int djb_nn_info(const djb_nn* h, int32_t* layers, int32_t* cin, int32_t* hidden, int32_t* cout,
+                        int32_t* device);
+
+/* ── NN-corrected PM force ──────────────────────────────────────────────────────
+ * No counterpart in the reference. Attaches a network (4 inputs, 3 outputs) to the solver:
+ * every force evaluation (djb_pm_acceleration, djb_step, djb_run) then adds
+ *   out_scale * interp(net([delta_scale * delta, force_scale * F]))(X_p)
+ * to the PM acceleration of pm.jl:507-521, where delta and F are the unshifted density
+ * contrast and finite-difference force on the mesh (as djb_mesh_fields computes them) and
+ * interp is the solver's W-order interpolation at X = q + Psi (djb_mesh_interp3). The
+ * drift before the force is then a separate pass. Needs a finite-difference gradient
+ * (2/4/6), no resampling, a non-lean solver with res divisible by 4 and antialias 0 or 1;
+ * net = NULL detaches. The solver keeps 4 + 3 meshes and 3*n^3 floats for it. The
+ * network runs on the solver's stream (its stream is set to the solver's at every force). */
+DJB_API int djb_solver_attach_nn(djb_solver* s, djb_nn* net, double delta_scale, double force_scale,
+                                 double out_scale);
+/* out (n,n,n,3) = the solver's W-order interpolation (pm.jl:344-364, no shift) of the three
+ * res^3 meshes mesh3 ([channel][z][y][x]) at X = q + psi. */
+DJB_API int djb_mesh_interp3(djb_solver* s, const float* psi, const float* mesh3, float* out, int32_t mem);
+/* The transpose of djb_mesh_interp3: mesh3[c](node) = sum_p W(X_p - node) vec_c(p). */
+DJB_API int djb_mesh_deposit3(djb_solver* s, const float* psi, const float* vec, float* mesh3, int32_t mem);
 
 /* ── non-allocating shell sums ──────────────────────────────────────────────
  * No counterpart in the reference. For callers that cannot allocate device

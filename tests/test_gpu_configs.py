@@ -5,7 +5,11 @@
   The float32 floor of this run (float32 CPU port vs float64 oracle) is 8.8e-6 in Ψ,
   2.2e-5 in P, 8.4e-7 in max|ΔX|/L and 1.3e-6 in P(k).
 * 256³ / 512³, L = 500, TSC, interlacing, order-4 gradient and Laplacian, FastPM
-  (40-step schedule): the first two steps against the float64 C port.
+  (40-step schedule): the first two steps, and the whole 40-step run to a = 1, against
+  the float64 C port (displacements, momenta, positions, P(k) per bin).
+* 512³ / 1024³, L = 1000, 3LPT, PCS, interlacing, order-6 gradient, BullFrog (the
+  throughput configuration): the first two steps against the float64 C port, which
+  covers the 1024³-only paths (fused z pass, 16³ bricks in Morton order, box bounds).
 * The reference's own physics check (test/nbody_parity_tests.jl:68-90): a
   fundamental plane wave grows as D(a) for every stepper, converging with resolution.
 * 512³ / 1024³ (the throughput configuration), size-independent properties: the
@@ -95,6 +99,104 @@ def test_c2_tsc_interlaced_fastpm_first_steps_vs_float64(djb, cosmo_pair):
         p64, m64 = C.step(p64, m64, coef["ddrift1"][k], coef["alpha"][k], coef["beta"][k], coef["ddrift2"][k])
     assert rel(Pg, p64) < 2e-5
     assert rel(Mg, m64) < 5e-5
+
+
+def _report(capsys, name, **errs):
+    with capsys.disabled():
+        print(f"\n[{name}] " + ", ".join(f"{k} = {v:.3e}" for k, v in errs.items()))
+
+
+def _port_run(C, p64, m64, coef, k0, k1):
+    for k in range(k0, k1):
+        p64, m64 = C.step(p64, m64, coef["ddrift1"][k], coef["alpha"][k], coef["beta"][k], coef["ddrift2"][k])
+    return p64, m64
+
+
+@pytest.mark.slow
+def test_c2_full_fastpm_run_vs_float64(djb, cosmo_pair, capsys):
+    """The whole 40-step FastPM run of 256³ particles on a 512³ mesh (TSC, interlacing,
+    order-4 gradient and Laplacian) from a = 0.02 to 1, float32 on the GPU against the
+    float64 C port from the same float32 ICs. Bars: positions max|ΔX|/L < 1e-5 (the
+    target's relative 1e-5 in positions); P(k) of the final particles per bin < 1e-4;
+    displacements and momenta, which carry float32 round-off amplified by 40 steps of
+    gravitational growth, < 2e-4 and 5e-4 of their largest entries."""
+    from oracle import cpm
+    from oracle import nbody as onb
+    from oracle import pm as opm
+    from oracle import power as opw
+    cl, co = cosmo_pair
+    n, res, L = 256, 512, 500.0
+    psi_t, pi_t = _ics(djb, cl, n, L, 2, seed=11, device="cuda")
+    psi = psi_t.cpu().numpy().astype(np.float32)
+    pi = pi_t.cpu().numpy().astype(np.float32)
+    del psi_t, pi_t
+    coef = djb.stepper_coefficients(cl, "fastpm", 0.02, 1.0, 40)
+    opts = dict(worder=3, antialias=1, grad_order=4, lap_order=4)
+    with djb.PMSolver(djb.PMConfig(res_pm=res, n_part=n, boxsize=L, **opts)) as S:
+        S.set_state(psi, pi)
+        S.run(coef["ddrift1"], coef["alpha"], coef["beta"], coef["ddrift2"])
+        Pg, Mg = S.get_state()
+        k, pk, nm = S.state_power_spectrum(bins=32)
+    C = cpm.CPUPM(opm.PMConfig(res_pm=res, n_part=n, boxsize=L, **opts), dtype=np.float64)
+    p64, m64 = _port_run(C, psi.astype(np.float64), pi.astype(np.float64), coef, 0, 40)
+    # P(k) of the float64 final state: CIC deposit (the C port), δ, float64 shell sums
+    X = onb.add_q(p64, L)
+    mesh = np.zeros(res ** 3)
+    Xb = np.ascontiguousarray(np.moveaxis(X, -1, 0).transpose(0, 3, 2, 1))  # [c][k][j][i]
+    cpm.lib().cpm_scatter_f64(cpm._ptr(Xb), n ** 3, res, float(L), 2, cpm._ptr(mesh))
+    field = mesh.reshape(res, res, res).T                                    # [ix,iy,iz]
+    kr, pkr, nmr = opw.evaluate_power_spectrum(opw.density_contrast(field, n), L, bins=32)
+    dx = np.abs(Pg.astype(np.float64) - p64)
+    errs = dict(psi=rel(Pg, p64), mom=rel(Mg, m64), dX_over_L=float(dx.max()) / L,
+                pk=float(np.max(np.abs(pk[nmr > 0] / pkr[nmr > 0] - 1))))
+    _report(capsys, "C2 40-step FastPM vs float64", **errs)
+    assert np.array_equal(nm, nmr)
+    assert errs["dX_over_L"] < 1e-5
+    assert errs["pk"] < 1e-4
+    assert errs["psi"] < 2e-4 and errs["mom"] < 5e-4
+
+
+@pytest.mark.slow
+def test_c3_bullfrog_steps_vs_float64_port(djb, cosmo_pair, capsys):
+    """512³ particles on the 1024³ mesh, L = 1000, 3LPT ICs at a = 0.02, PCS,
+    interlacing, order-6 gradient, BullFrog (20-step schedule): the first two steps,
+    float32 on the GPU against the float64 C port from the same float32 ICs. The
+    momentum after the first step isolates one force evaluation (Mom₁ = α Mom₀ + β F)."""
+    import psutil
+
+    from oracle import cpm
+    from oracle import pm as opm
+    if psutil.virtual_memory().available < 160 * 2 ** 30:
+        pytest.skip("the float64 port at 1024³ needs about 80 GB of host memory (160 GB free asked)")
+    cl, co = cosmo_pair
+    n, res, L = 512, 1024, 1000.0
+    psi_t, pi_t = _ics(djb, cl, n, L, 3, seed=5, device="cuda")
+    psi = psi_t.cpu().numpy().astype(np.float32)
+    pi = pi_t.cpu().numpy().astype(np.float32)
+    del psi_t, pi_t
+    coef = djb.stepper_coefficients(cl, "bullfrog", 0.02, 1.0, 20)
+    opts = dict(worder=4, antialias=1, grad_order=6)
+    got = []
+    with djb.PMSolver(djb.PMConfig(res_pm=res, n_part=n, boxsize=L, **opts)) as S:
+        S.set_state(psi, pi)
+        for k in range(2):
+            S.step(coef["ddrift1"][k], coef["alpha"][k], coef["beta"][k], coef["ddrift2"][k])
+            got.append(S.get_state())
+    C = cpm.CPUPM(opm.PMConfig(res_pm=res, n_part=n, boxsize=L, **opts), dtype=np.float64)
+    p64, m64 = psi.astype(np.float64), pi.astype(np.float64)
+    del psi, pi
+    errs = {}
+    for k in range(2):
+        p64, m64 = _port_run(C, p64, m64, coef, k, k + 1)
+        Pg, Mg = got[k]
+        errs[f"psi{k + 1}"] = rel(Pg, p64)
+        errs[f"mom{k + 1}"] = rel(Mg, m64)
+        errs[f"dX{k + 1}_over_L"] = float(np.max(np.abs(Pg.astype(np.float64) - p64))) / L
+    _report(capsys, "C3 BullFrog steps vs float64", **errs)
+    for k in (1, 2):
+        assert errs[f"psi{k}"] < 2e-5
+        assert errs[f"mom{k}"] < 2e-5
+        assert errs[f"dX{k}_over_L"] < 1e-5
 
 
 @pytest.mark.parametrize("stepper,nsteps", [("bullfrog", 1), ("bullfrog", 16), ("fastpm", 16), ("symplectic", 64)])
