@@ -8,12 +8,25 @@ the particle state resident on the GPU. Host arrays (`Array{Float32,4}`) and dev
 arrays (`CuArray{Float32,4}`, via their pointers) of shape (n,n,n,3) are both
 accepted, exactly as laid out by the reference (`pm.jl:15-17`).
 
+Differentiation: `pm_acceleration_b200`, `pm_step_b200`, `run_states_b200` and
+`state_power_spectrum_b200` are pure functions with ChainRulesCore `rrule`s over the
+library's hand-written adjoints (djb_pm_acceleration_vjp, djb_step_vjp,
+djb_state_power_spectrum_vjp), following the pattern of the reference's
+`rrule(cic_deposit)` (src/field/sheet_deposit.jl:118-132); `run_states_b200`
+checkpoints the state every `checkpoint_every` steps and re-runs each segment once on
+the way back. Zygote picks these rules up, so a loss written with them
+differentiates through the B200 step.
+
+Force correction: `ForceNetB200` wraps the `djb_nn_*` network and
+`attach_nn!(S, net, scales)` adds its correction to every force of a solver.
+
 Load with `include("DiscoDJB200.jl")` after `using DiscoDJNative`; set
 `ENV["DJB200_LIB"]` to the library path if it is not next to this file.
 """
 module DiscoDJB200
 
 using DiscoDJNative: PMConfig, Cosmology, stepper_coefficients, Fplus
+using ChainRulesCore: ChainRulesCore, NoTangent, unthunk
 
 const LIB = get(ENV, "DJB200_LIB", joinpath(@__DIR__, "..", "lib", "libdjb200.so"))
 
@@ -109,5 +122,167 @@ function run_nbody_b200(c::Cosmology, psi_ini::AbstractArray{Float32,4}, pi_ini:
                  S.handle, _ptr(X), _ptr(P), return_displacement ? 0 : 1, pdiv, F, _mem(X)))
     return X, P, a_end
 end
+
+# ── differentiable forms (ChainRulesCore rrules over the library's adjoints) ──────
+"""    pm_acceleration_b200(S, psi) -> acc   (pure form of pm_acceleration!, pm.jl:507-521)"""
+pm_acceleration_b200(S::PMSolverB200, psi::AbstractArray{Float32,4}) = pm_acceleration!(similar(psi), S, psi)
+
+function ChainRulesCore.rrule(::typeof(pm_acceleration_b200), S::PMSolverB200, psi::AbstractArray{Float32,4})
+    acc = pm_acceleration_b200(S, psi)
+    function pm_acceleration_pullback(Δ)
+        ā = convert(typeof(psi), unthunk(Δ))
+        ψ̄ = similar(psi)
+        _check(ccall((:djb_pm_acceleration_vjp, LIB), Cint,
+                     (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Ptr{Float32}, Int32),
+                     S.handle, _ptr(psi), _ptr(ā), _ptr(ψ̄), _mem(psi)))
+        return (NoTangent(), NoTangent(), ψ̄)
+    end
+    return acc, pm_acceleration_pullback
+end
+
+"""
+    pm_step_b200(S, psi, mom, dd1, alpha, beta, dd2) -> (psi', mom')
+
+One drift-kick-drift step (run_nbody.jl:156-158) on copies of the state.
+"""
+function pm_step_b200(S::PMSolverB200, psi::AbstractArray{Float32,4}, mom::AbstractArray{Float32,4},
+                      dd1::Real, alpha::Real, beta::Real, dd2::Real)
+    _check(ccall((:djb_set_state, LIB), Cint, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Float64, Int32),
+                 S.handle, _ptr(psi), _ptr(mom), 1.0, _mem(psi)))
+    _check(ccall((:djb_step, LIB), Cint, (Ptr{Cvoid}, Float64, Float64, Float64, Float64),
+                 S.handle, dd1, alpha, beta, dd2))
+    p = similar(psi); m = similar(mom)
+    _check(ccall((:djb_get_state, LIB), Cint, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Int32),
+                 S.handle, _ptr(p), _ptr(m), _mem(p)))
+    return p, m
+end
+
+# (ψ̄, M̄) of the state before one step from those after it (djb_step_vjp).
+function _step_vjp!(S::PMSolverB200, psi0, mom0, ψ̄, M̄, dd1, alpha, beta, dd2)
+    _check(ccall((:djb_step_vjp, LIB), Cint,
+                 (Ptr{Cvoid}, Float64, Float64, Float64, Float64, Ptr{Float32}, Ptr{Float32}, Ptr{Float32},
+                  Ptr{Float32}, Int32),
+                 S.handle, dd1, alpha, beta, dd2, _ptr(psi0), _ptr(mom0), _ptr(ψ̄), _ptr(M̄), _mem(psi0)))
+    return ψ̄, M̄
+end
+
+_tangent_or_zero(Δ, like) = Δ isa ChainRulesCore.AbstractZero ? fill!(similar(like), 0f0) :
+                            convert(typeof(like), copy(unthunk(Δ)))
+
+function ChainRulesCore.rrule(::typeof(pm_step_b200), S::PMSolverB200, psi, mom, dd1, alpha, beta, dd2)
+    out = pm_step_b200(S, psi, mom, dd1, alpha, beta, dd2)
+    function pm_step_pullback(Δ)
+        Δp, Δm = unthunk(Δ)
+        ψ̄, M̄ = _step_vjp!(S, psi, mom, _tangent_or_zero(Δp, psi), _tangent_or_zero(Δm, mom), dd1, alpha, beta, dd2)
+        return (NoTangent(), NoTangent(), ψ̄, M̄, NoTangent(), NoTangent(), NoTangent(), NoTangent())
+    end
+    return out, pm_step_pullback
+end
+
+"""
+    run_states_b200(S, psi0, mom0, co; checkpoint_every=5) -> (psi, mom)
+
+The DKD loop of run_nbody.jl:155-163 over the coefficients `co` (a NamedTuple of
+`stepper_coefficients`), returning the final state. Its rrule saves the state every
+`checkpoint_every` steps and re-runs each segment once while taking its steps back.
+"""
+function run_states_b200(S::PMSolverB200, psi0::AbstractArray{Float32,4}, mom0::AbstractArray{Float32,4}, co;
+                         checkpoint_every::Int=5)
+    p, m = psi0, mom0
+    for k in eachindex(co.alpha)
+        p, m = pm_step_b200(S, p, m, co.ddrift1[k], co.alpha[k], co.beta[k], co.ddrift2[k])
+    end
+    return p, m
+end
+
+function ChainRulesCore.rrule(::typeof(run_states_b200), S::PMSolverB200, psi0, mom0, co; checkpoint_every::Int=5)
+    nsteps = length(co.alpha)
+    ckpt = Dict(0 => (copy(psi0), copy(mom0)))
+    p, m = psi0, mom0
+    for k in 1:nsteps
+        p, m = pm_step_b200(S, p, m, co.ddrift1[k], co.alpha[k], co.beta[k], co.ddrift2[k])
+        k % checkpoint_every == 0 && k < nsteps && (ckpt[k] = (copy(p), copy(m)))
+    end
+    function run_states_pullback(Δ)
+        Δp, Δm = unthunk(Δ)
+        ψ̄ = _tangent_or_zero(Δp, psi0); M̄ = _tangent_or_zero(Δm, mom0)
+        starts = sort(collect(keys(ckpt)))
+        for (i, c0) in Iterators.reverse(enumerate(starts))
+            c1 = i < length(starts) ? starts[i + 1] : nsteps
+            states = [ckpt[c0]]
+            for k in c0 + 1:c1 - 1
+                push!(states, pm_step_b200(S, states[end]..., co.ddrift1[k], co.alpha[k], co.beta[k], co.ddrift2[k]))
+            end
+            for k in c1:-1:c0 + 1
+                p_k, m_k = states[k - c0]
+                ψ̄, M̄ = _step_vjp!(S, p_k, m_k, ψ̄, M̄, co.ddrift1[k], co.alpha[k], co.beta[k], co.ddrift2[k])
+            end
+        end
+        return (NoTangent(), NoTangent(), ψ̄, M̄, NoTangent())
+    end
+    return (p, m), run_states_pullback
+end
+
+"""    state_power_spectrum_b200(S, psi; bins=32, logarithmic=true) -> P(k) (Vector{Float64})
+
+P(k) of the particles X = q + psi: CIC deposit on the solver's mesh and the float64
+shell sums of `evaluate_power_spectrum` (power_spectrum.jl:25-79).
+"""
+function state_power_spectrum_b200(S::PMSolverB200, psi::AbstractArray{Float32,4}; bins::Int=32,
+                                   logarithmic::Bool=true)
+    _check(ccall((:djb_set_state, LIB), Cint, (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Float64, Int32),
+                 S.handle, _ptr(psi), _ptr(psi), 1.0, _mem(psi)))
+    k = zeros(Float64, bins); pk = zeros(Float64, bins); nm = zeros(Int64, bins)
+    _check(ccall((:djb_state_power_spectrum, LIB), Cint,
+                 (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Int64}),
+                 S.handle, bins, logarithmic, k, pk, nm))
+    return pk
+end
+
+function ChainRulesCore.rrule(::typeof(state_power_spectrum_b200), S::PMSolverB200, psi; bins::Int=32,
+                              logarithmic::Bool=true)
+    pk = state_power_spectrum_b200(S, psi; bins=bins, logarithmic=logarithmic)
+    function state_power_spectrum_pullback(Δ)
+        p̄ = Float64.(collect(unthunk(Δ)))
+        ψ̄ = similar(psi)
+        _check(ccall((:djb_state_power_spectrum_vjp, LIB), Cint,
+                     (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}, Ptr{Float32}, Int32),
+                     S.handle, bins, logarithmic, p̄, _ptr(ψ̄), _mem(ψ̄)))
+        return (NoTangent(), NoTangent(), ψ̄)
+    end
+    return pk, state_power_spectrum_pullback
+end
+
+# ── force-correction network ──────────────────────────────────────────────────────
+"""    ForceNetB200(; layers=4, cin=4, hidden=32, cout=3, seed=0, device=0)"""
+mutable struct ForceNetB200
+    handle::Ptr{Cvoid}
+    function ForceNetB200(; layers::Integer=4, cin::Integer=4, hidden::Integer=32, cout::Integer=3,
+                          seed::Integer=0, device::Integer=0)
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        _check(ccall((:djb_nn_create, LIB), Cint, (Int32, Int32, Int32, Int32, UInt64, Int32, Ref{Ptr{Cvoid}}),
+                     layers, cin, hidden, cout, seed, device, h))
+        net = new(h[])
+        finalizer(x -> ccall((:djb_nn_destroy, LIB), Cint, (Ptr{Cvoid},), x.handle), net)
+        return net
+    end
+end
+
+"""    load_params!(net, params::Vector{Float32})   (djb_nn_load)"""
+load_params!(net::ForceNetB200, params::Vector{Float32}) =
+    _check(ccall((:djb_nn_load, LIB), Cint, (Ptr{Cvoid}, Ptr{Float32}), net.handle, params))
+
+"""
+    attach_nn!(S, net, (delta_scale, force_scale, out_scale))
+
+Every force of S then adds out_scale·interp(net([delta_scale·δ, force_scale·F])) at the
+particles (djb_solver_attach_nn); `attach_nn!(S, nothing)` detaches.
+"""
+attach_nn!(S::PMSolverB200, net::ForceNetB200, scales) =
+    _check(ccall((:djb_solver_attach_nn, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Float64, Float64, Float64),
+                 S.handle, net.handle, scales[1], scales[2], scales[3]))
+attach_nn!(S::PMSolverB200, ::Nothing) =
+    _check(ccall((:djb_solver_attach_nn, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Float64, Float64, Float64),
+                 S.handle, C_NULL, 1.0, 1.0, 1.0))
 
 end # module

@@ -138,3 +138,60 @@ def test_pk_loss_gradient_through_a_run_vs_finite_differences(djb):
             fd = (loss(psi, pi + eps * v) - loss(psi, pi - eps * v)) / (2 * eps)
         an = float(np.sum(grad.astype(np.float64) * v))
         assert abs(an - fd) < 2e-2 * abs(fd), (which, an, fd)
+
+
+def _mode(n, m, phase, device):
+    """A real Fourier mode of unit variance per voxel: √2 cos(2π m·x/n + phase)."""
+    import torch
+    i = torch.arange(n, device=device, dtype=torch.float64)
+    arg = (2 * np.pi / n) * (m[0] * i[:, None, None] + m[1] * i[None, :, None] + m[2] * i[None, None, :]) + phase
+    return (np.sqrt(2.0) * torch.cos(arg)).float()
+
+
+def _white_noise_fd_check(djb, n, res, L, n_modes, capsys, label, eps=1e-3, seed=21):
+    """∂loss/∂(white noise) through 2LPT ICs and a checkpointed BullFrog run (CIC, grad 2,
+    20 steps, checkpoints every 5) against central differences (ε = 1e-3) along random
+    low-k Fourier modes of the white noise (|m| < n/8, random phases)."""
+    import torch
+
+    from djb200 import adjoint as dad
+    from djb200 import ics
+    cl = djb.Cosmology(**COSMO)
+    kw = dict(boxsize=L, a_ini=0.02, a_end=1.0, n_steps=20, res_pm=res, stepper="bullfrog", worder=2,
+              grad_kernel_order=2, antialias=0, checkpoint_every=5, bins=32)
+    w = ics.white_noise(seed, n, device="cuda", dtype=torch.float32)
+    _, pk0 = dad.white_noise_loss(cl, w, np.ones(32), **dict(kw))
+    target = 0.9 * pk0
+    loss, gw = dad.white_noise_loss_and_gradient(cl, w, target, **dict(kw))
+    rng = np.random.default_rng(seed)
+    an, fd = [], []
+    for _ in range(n_modes):
+        while True:
+            m = rng.integers(-(n // 8) + 1, n // 8, size=3)
+            if 0 < np.sum(m * m) < (n // 8) ** 2:
+                break
+        v = _mode(n, m, rng.uniform(0, 2 * np.pi), "cuda")
+        an.append(float((gw.double() * v.double()).sum()))
+        lp, _ = dad.white_noise_loss(cl, w + eps * v, target, **dict(kw))
+        lm, _ = dad.white_noise_loss(cl, w - eps * v, target, **dict(kw))
+        fd.append((lp - lm) / (2 * eps))
+    an, fd = np.array(an), np.array(fd)
+    err = np.abs(an - fd) / np.maximum(np.abs(fd), 1e-3 * np.max(np.abs(fd)))
+    with capsys.disabled():
+        print(f"\n[{label}] loss {loss:.4e}; {n_modes} modes: median rel err {np.median(err):.2e}, "
+              f"max {np.max(err):.2e}, corr {np.corrcoef(an, fd)[0, 1]:.6f}")
+    return an, fd, err
+
+
+def test_white_noise_gradient_small_vs_finite_differences(djb, capsys):
+    an, fd, err = _white_noise_fd_check(djb, 32, 64, 62.5, 8, capsys, "white-noise gradient 32^3/64^3")
+    assert np.median(err) < 5e-2
+    assert np.corrcoef(an, fd)[0, 1] > 0.99
+
+
+@pytest.mark.slow
+def test_white_noise_gradient_c5_vs_finite_differences(djb, capsys):
+    """The differentiable-run configuration: 128³ particles on a 256³ mesh, L = 250."""
+    an, fd, err = _white_noise_fd_check(djb, 128, 256, 250.0, 64, capsys, "white-noise gradient C5 128^3/256^3")
+    assert np.median(err) < 5e-2
+    assert np.corrcoef(an, fd)[0, 1] > 0.99
