@@ -20,6 +20,7 @@ using djb::fail;
 struct djb_solver;
 namespace djb {
 int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cudaStream_t* st);
+int solver_res(const djb_solver* s);
 int64_t solver_np(const djb_solver* s);
 cufftHandle solver_r2c(const djb_solver* s);
 cufftHandle solver_c2r(const djb_solver* s);
@@ -256,6 +257,43 @@ int noalloc_scratch(int device, unsigned char** out) {
     return DJB_OK;
 }
 
+// Density-contrast Fourier modes δ̂(m)/res³ / W_CIC(m) of a CIC mesh's half spectrum
+// (in place, rows of nh = res/2 + 1 complex, [kz][ky][kx]); m = (mx, my, mz) in
+// (−res/2, res/2], modes with mx < 0 read the conjugate of −m. `f` = res³/n³ scales the
+// mesh to 1 + δ; the m = 0 mode is δ's mean, 0. W_CIC = Π_d sinc²(π m_d / res).
+__global__ void k_density_modes(const float2* __restrict__ spec, int res, const int* __restrict__ modes, int nm,
+                                double f, double2* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nm) return;
+    int mx = modes[3 * i], my = modes[3 * i + 1], mz = modes[3 * i + 2];
+    if (mx == 0 && my == 0 && mz == 0) {
+        out[i] = make_double2(0.0, 0.0);
+        return;
+    }
+    const bool conj = mx < 0;
+    if (conj) {
+        mx = -mx;
+        my = -my;
+        mz = -mz;
+    }
+    const int nh = res / 2 + 1;
+    const int ky = (my % res + res) % res, kz = (mz % res + res) % res;
+    const float2 v = spec[(int64_t(kz) * res + ky) * nh + mx];
+    double w = 1.0;
+    const int md[3] = {mx, my, mz};
+    for (int d = 0; d < 3; ++d) {
+        if (md[d] == 0) continue;
+        const double x = M_PI * double(md[d]) / double(res);
+        const double sc = sin(x) / x;
+        w *= sc * sc;
+    }
+    const double r3 = double(res) * res * res;
+    const double sc = f / (r3 * w);
+    out[i] = make_double2(double(v.x) * sc, (conj ? -double(v.y) : double(v.y)) * sc);
+}
+
+int res_limit(const djb_solver* s) { return djb::solver_res(s) / 2; }
+
 // Makes a device current for the guard's lifetime and gives the calling thread its
 // previous current device back on every return path.
 struct DeviceGuard {
@@ -400,6 +438,47 @@ int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logarithmic, d
     const double f = double(res) * res * res / double(djb::solver_np(s));
     return shells(reinterpret_cast<const float2*>(mesh), res, djb::solver_boxsize(s), f * f, bins,
                   logarithmic != 0, k, pk, nmodes, st);
+}
+
+int djb_state_density_modes(djb_solver* s, int32_t nmodes, const int32_t* modes, double* out) {
+    djb::clear_error();
+    if (!s || (nmodes > 0 && (!modes || !out))) return fail(DJB_ERR_INVALID, "null argument");
+    if (nmodes < 0) return fail(DJB_ERR_INVALID, "nmodes must be >= 0");
+    float* mesh = nullptr;
+    int res = 0, pitch = 0;
+    cudaStream_t st = nullptr;
+    for (int32_t i = 0; i < 3 * nmodes; ++i)
+        if (modes[i] <= -res_limit(s) || modes[i] > res_limit(s))
+            return fail(DJB_ERR_INVALID, "mode component %d outside (-res/2, res/2]", int(modes[i]));
+    int rc = djb::solver_deposit_cic(s, &mesh, &res, &pitch, &st);
+    if (rc != DJB_OK) return rc;
+    if (nmodes == 0) return djb::solver_check_err(s);
+    CUFFT_TRY(cufftExecR2C(djb::solver_r2c(s), mesh, reinterpret_cast<cufftComplex*>(mesh)));
+    int* d_modes = nullptr;
+    double2* d_out = nullptr;
+    auto cleanup = [&]() {
+        if (d_modes) cudaFreeAsync(d_modes, st);
+        if (d_out) cudaFreeAsync(d_out, st);
+    };
+    if (cudaMallocAsync(reinterpret_cast<void**>(&d_modes), sizeof(int) * 3 * size_t(nmodes), st) != cudaSuccess ||
+        cudaMallocAsync(reinterpret_cast<void**>(&d_out), sizeof(double2) * size_t(nmodes), st) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        return fail(DJB_ERR_ALLOC, "mode buffers allocation failed");
+    }
+    const double f = double(res) * res * res / double(djb::solver_np(s));
+    cudaError_t e = cudaMemcpyAsync(d_modes, modes, sizeof(int) * 3 * size_t(nmodes), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        k_density_modes<<<(nmodes + 127) / 128, 128, 0, st>>>(reinterpret_cast<const float2*>(mesh), res, d_modes,
+                                                              nmodes, f, d_out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, d_out, sizeof(double2) * size_t(nmodes), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cleanup();
+    if (e != cudaSuccess) return fail(DJB_ERR_CUDA, "density modes failed: %s", cudaGetErrorString(e));
+    return djb::solver_check_err(s);
 }
 
 // Ψ̄ of Σ_b P̄_b·P_b for the solver's particle state, P as djb_state_power_spectrum.

@@ -2320,4 +2320,5 @@ int solver_deposit_cic(djb_solver* s, float** mesh_out, int* res, int* pitch, cu
     return DJB_OK;
 }
 int64_t solver_np(const djb_solver* s) { return s->np; }
+int solver_res(const djb_solver* s) { return s->res; }
 }  // namespace djb

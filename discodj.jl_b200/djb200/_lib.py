@@ -109,6 +109,7 @@ SIGNATURES = {
     "djb_solver_attach_nn": [_P, _P, _D, _D, _D],
     "djb_mesh_interp3": [_P, _P, _P, _P, _I],
     "djb_mesh_deposit3": [_P, _P, _P, _P, _I],
+    "djb_state_density_modes": [_P, _I, _IP, _DP],
 }
 _RESTYPES = {"djb_version": C.c_char_p, "djb_last_error": C.c_char_p}
 

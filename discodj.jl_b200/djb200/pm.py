@@ -302,6 +302,14 @@ class PMSolver:
                                  float(p_div), float(p_mul), MEM_HOST))
         return xo, po
 
+    def state_density_modes(self, modes) -> np.ndarray:
+        """Complex δ(m)/res³ / W_CIC(m) of the resident state at integer modes (k, 3)
+        (`djb_state_density_modes`; measure.jl:80-91 `density_modes`)."""
+        m = np.ascontiguousarray(np.asarray(modes, dtype=np.int32).reshape(-1, 3))
+        out = np.empty(2 * len(m), dtype=np.float64)
+        check(lib.djb_state_density_modes(self._h, len(m), m.ctypes.data_as(C.POINTER(C.c_int32)), _lib.dptr(out)))
+        return out[0::2] + 1j * out[1::2]
+
     def state_power_spectrum(self, bins: int = 32, logarithmic: bool = True):
         k = np.empty(bins)
         pk = np.empty(bins)

@@ -188,6 +188,15 @@ DJB_API int djb_power_spectrum(const float* field, int32_t res, double boxsize, 
 DJB_API int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logarithmic, double* k,
                              double* pk, int64_t* nmodes);
 
+/* CIC density-contrast Fourier modes of the solver's particle state, the snapshot
+ * measurement `density_modes` of studies/eft_shell_crossing/src/measure.jl:80-91: CIC
+ * deposit of X = q + Psi on the solver's mesh, delta = mesh*res^3/n^3 - 1, R2C, and per
+ * mode m = modes[3i..3i+2] (integers in (-res/2, res/2], x, y, z) the coefficient
+ * delta(m)/res^3 divided by the CIC window prod_d sinc^2(pi m_d/res), with
+ * delta(m) = sum_x delta(x) exp(-2 pi i m.x/res). out: host double[2*nmodes] (re, im).
+ * The particle state stays on the device. */
+DJB_API int djb_state_density_modes(djb_solver* s, int32_t nmodes, const int32_t* modes, double* out);
+
 /* ── adjoints (vector-Jacobian products) ────────────────────────────────────
  * No counterpart in the reference, which has no adjoint; these are the transposes
  * of the forward operators above, checked against finite differences of float64

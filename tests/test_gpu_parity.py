@@ -212,3 +212,29 @@ def test_dense_clump_vs_oracle(djb, W, n, res, clump, aa):
     ref = opm.pm_acceleration(cfg_o, psi.astype(np.float64))
     got = djb.pm_acceleration(psi, cfg_d)
     assert rel(got, ref) < ACC_TOL
+
+
+def test_state_density_modes_vs_oracle(djb):
+    """measure.jl:80-91 `density_modes`: CIC δ of the particle state, Fourier modes / res³,
+    CIC window divided out; against the float64 oracle's deposit and numpy's FFT."""
+    from oracle import nbody as onb
+    from oracle import pm as opm
+    n, res, L = 32, 32, 100.0
+    rng = np.random.default_rng(17)
+    psi = (1.5 * rng.standard_normal((n, n, n, 3))).astype(np.float32)
+    modes = rng.integers(-res // 2 + 1, res // 2 + 1, size=(40, 3))
+    modes[0] = (0, 0, 0)
+    modes[1] = (1, 0, 0)
+    modes[2] = (-3, 2, -1)
+    with djb.PMSolver(djb.PMConfig(res_pm=res, n_part=n, boxsize=L)) as S:
+        S.set_state(psi, psi)
+        got = S.state_density_modes(modes)
+    X = onb.add_q(psi.astype(np.float64), L).reshape(-1, 3)
+    mesh = opm.pm_scatter(np.zeros((res, res, res)), X, res, L, 2)       # [ix,iy,iz]
+    delta = mesh * (res ** 3 / n ** 3) - 1.0
+    dk = np.fft.fftn(delta) / res ** 3
+    ref = np.array([dk[m[0] % res, m[1] % res, m[2] % res] for m in modes])
+    W = np.prod(np.sinc(modes / res) ** 2, axis=1)
+    ref = ref / W
+    ref[0] = 0.0
+    assert np.max(np.abs(got - ref)) < 1e-5 * np.max(np.abs(ref))
