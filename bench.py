@@ -324,6 +324,33 @@ def nn_timing(dev, stream, world):
     return out
 
 
+def nn_corrected(world):
+    """NN-corrected 1x-mesh PM against the plain 2x-mesh PM, 512³ particles in L = 1000
+    (1x mesh 512³, 2x mesh 1024³ with this workload's options), one held-out seed, with
+    the network trained by `python -m djb200.correction` and shipped with the package:
+    P(k) at a = 1 against the 2x run for k < k_Nyq/2 of the 1x mesh, and device ms per
+    step (CUDA events, after 2 steps) of the corrected 1x and the plain 2x runs."""
+    import djb200
+    from djb200 import correction
+    path = os.path.join(ROOT, "discodj.jl_b200", "djb200", "data", "force_correction.npz")
+    if not os.path.exists(path):
+        return None
+    net, scales, info = correction.load(path)
+    cosmo = djb200.Cosmology(**correction.COSMO)
+    ev = correction.evaluate(cosmo, net, scales, n=512, boxsize=1000.0, seeds=[1000], timing=True,
+                             opts_lo=info.get("opts_lo", correction.OPTS_LO), opts_hi=info.get("opts_hi", correction.OPTS))
+    net.close()
+    ms = ev["ms_per_step"]
+    return dict(pk_max_err_lt_kNyq2=ev["pk_max_err_corrected"], pk_max_err_plain_1x=ev["pk_max_err_plain"],
+                speedup_vs_2x=ev["speedup_vs_2x"], ms_per_step=ms,
+                value=world * 512 ** 3 / (ms["corrected"] / 1e3), unit=UNIT,
+                held_out={k: {kk: info[k][kk] for kk in ("n_part", "seeds", "pk_max_err_plain", "pk_max_err_corrected",
+                                                     "speedup_vs_2x") if kk in info[k]}
+                          for k in ("eval_small", "eval_large") if k in info},
+                note="1x: " + json.dumps(info.get("opts_lo")) + " + network; 2x: " + json.dumps(info.get("opts_hi")) +
+                     "; trained on 64 seeds x 20 states of 128^3 particles (L=250) by this library's kernels")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -390,6 +417,7 @@ def main():
     clk = clocks.stop()
     S.synchronize()
     ms = allmax(world, ms_local)
+    device_bytes = S.device_bytes
     Np = n ** 3
     value = aggregate_value(world, n, args.steps, ms)
 
@@ -453,6 +481,11 @@ def main():
     nn = None
     if not args.no_nn:
         nn = nn_timing(dev, stream, world)
+    nnc = None
+    if not args.no_nn and args.size == "c3":
+        S.close()      # the corrected and 2x runs hold their own meshes
+        torch.cuda.empty_cache()
+        nnc = nn_corrected(world)
 
     # roofline of the dominant kernel of this library (CUDA-event time per launch)
     ab = algorithmic_bytes(n, res)
@@ -487,9 +520,9 @@ def main():
                     data="synthetic (seeded white noise -> EH P(k) -> 3LPT)",
                     config=config_block(args.size, n, res, L, lpt, world), roofline=roof,
                     step_roofline=step_roof, phases=phases, cpu_baseline=cpu, e2e=e2e, adjoint=adjoint, nn=nn,
-                    clocks=clk,
+                    nn_corrected=nnc, clocks=clk,
                     gpu_launches=int(sum(v[1] for v in prof.values())),
-                    device_bytes=S.device_bytes)
+                    device_bytes=device_bytes)
         print(json.dumps(line), flush=True)
     S.close()
     if world > 1:

@@ -849,6 +849,11 @@ struct djb_solver {
     // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
     bool zpass = false;
     float2* wN = nullptr;
+    // the z pass fed by bulk tensor copies: 2-D maps of each spectrum (8-byte complex
+    // elements, x = ky·nh + kx, y = kz); DJB_ZPASS_TMA=0 selects the register-fed form
+    CUtensorMap zmap[kMaxGroup];
+    bool ztma = false;
+    int zplanes = 0;   // z planes per 2-D transform call
     float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
     float* scr[10] = {};    // staging and work buffers of the adjoint entry points, kept between calls
     size_t scr_n[10] = {};
@@ -1064,6 +1069,11 @@ size_t gather_smem(const djb_solver* s) { return size_t(s->gsx) * s->gS * s->gS 
 // Dynamic shared memory of a brick kernel, 2 CTAs per SM: 228 KB of shared memory
 // less 1 KB per CTA reserved by the runtime and the kernel's static barrier.
 constexpr int kBrickSmemMax = 113 * 1024;
+// z planes per 2-D transform call of the 1024^3 path (DJB_FFT_PLANES overrides)
+#ifndef DJB_FFT_PLANES_DEFAULT
+#define DJB_FFT_PLANES_DEFAULT 1024
+#endif
+constexpr int kFftPlanes = DJB_FFT_PLANES_DEFAULT;
 
 // Tensor map of a dense [res]^3 float mesh with boxes of sx x S x S elements.
 int make_tmap(CUtensorMap* m, const float* base, int res, int sx, int S) {
@@ -1083,6 +1093,29 @@ int make_tmap(CUtensorMap* m, const float* base, int res, int sx, int S) {
                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+    return DJB_OK;
+}
+
+// 2-D tensor map of a res x res x (res/2+1) complex spectrum as 8-byte elements: x = the
+// flat index ky·nh + kx within a z plane, y = kz; boxes of kZTBox x 256 elements.
+int make_zmap(CUtensorMap* m, const void* base, int res) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const int64_t nh = res / 2 + 1;
+    const cuuint64_t dims[2] = {cuuint64_t(int64_t(res) * nh), cuuint64_t(res)};
+    const cuuint64_t strides[1] = {cuuint64_t(int64_t(res) * nh * 8)};
+    const cuuint32_t box[2] = {cuuint32_t(djb::kZTBox), 256};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_INT64, 2, const_cast<void*>(base), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled (spectrum) failed (%d)", int(r));
     return DJB_OK;
 }
 
@@ -1274,10 +1307,40 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
 // Force evaluation for all shifts; if `step`, fused with the drift/kick/drift.
 // Reads s->psi (and s->mom). Output: s->acc (step == 0) or updated psi/mom.
 // The fused z pass of the 1024³ Poisson solve on the half spectrum in `mesh`.
+// The dense-mesh transforms: 3-D, or with the fused z pass the 2-D transforms of the z
+// planes in calls of s->zplanes planes.
+int exec_r2c_d(djb_solver* s, float* in, cufftComplex* out) {
+    if (!s->zpass || s->zplanes >= s->res) {
+        CUFFT_TRY(cufftExecR2C(s->r2c_d, in, out));
+        return DJB_OK;
+    }
+    const int64_t nh = s->res / 2 + 1;
+    for (int z = 0; z < s->res; z += s->zplanes)
+        CUFFT_TRY(cufftExecR2C(s->r2c_d, in + int64_t(z) * s->res * s->res, out + int64_t(z) * s->res * nh));
+    return DJB_OK;
+}
+int exec_c2r_d(djb_solver* s, cufftComplex* in, float* out) {
+    if (!s->zpass || s->zplanes >= s->res) {
+        CUFFT_TRY(cufftExecC2R(s->c2r_d, in, out));
+        return DJB_OK;
+    }
+    const int64_t nh = s->res / 2 + 1;
+    for (int z = 0; z < s->res; z += s->zplanes)
+        CUFFT_TRY(cufftExecC2R(s->c2r_d, in + int64_t(z) * s->res * nh, out + int64_t(z) * s->res * s->res));
+    return DJB_OK;
+}
+
 void launch_zpass(djb_solver* s, float* mesh, int nh) {
     const dim3 grid(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res));
     const djb::KPhiFn kp{s->lapT, s->makT, s->s0};
-    if (DJB_ZPASS_PAIR)
+    int m = -1;
+    for (int i = 0; i < s->group; ++i)
+        if (mesh == s->mesh[i]) m = i;
+    if (s->ztma && m >= 0) {
+        const int tiles = int(grid.x * grid.y);
+        djb::k_zpencil_tma<<<std::min(tiles, s->nsm), djb::kZPairThreads, djb::kZTSmem, s->stream>>>(
+            reinterpret_cast<float2*>(mesh), nh, s->wN, kp, s->zmap[m], s->err);
+    } else if (DJB_ZPASS_PAIR)
         djb::k_zpencil_pair<<<grid, djb::kZPairThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh,
                                                                                   s->wN, kp);
     else
@@ -1340,7 +1403,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             float* mesh = s->mesh[m];
             cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
             s->prof.begin(s->stream, PH_R2C);
-            if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
+            if (s->phi[m]) TRY(exec_r2c_d(s, s->phi[m], spec));
             else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
             s->prof.end(s->stream, PH_R2C, 0);
             // network input, δ: the unshifted density is still in phi[0] after the R2C
@@ -1356,7 +1419,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
                 launch_zpass(s, mesh, nh);
                 s->prof.end(s->stream, PH_KSPACE, 1);
                 s->prof.begin(s->stream, PH_C2R);
-                CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+                TRY(exec_c2r_d(s, spec, s->phi[m]));
                 s->prof.end(s->stream, PH_C2R, 0);
             } else if (!ik) {
                 s->prof.begin(s->stream, PH_KSPACE);
@@ -1365,7 +1428,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
                     reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
                 s->prof.end(s->stream, PH_KSPACE, 1);
                 s->prof.begin(s->stream, PH_C2R);
-                if (s->phi[m]) CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+                if (s->phi[m]) TRY(exec_c2r_d(s, spec, s->phi[m]));
                 else CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
                 s->prof.end(s->stream, PH_C2R, 0);
             } else {
@@ -1436,16 +1499,16 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
 int poisson(djb_solver* s, int m) {
     float* mesh = s->mesh[m];
     cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
-    if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
+    if (s->phi[m]) TRY(exec_r2c_d(s, s->phi[m], spec));
     else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
     const int nh = s->res / 2 + 1;
     if (s->zpass) {
         launch_zpass(s, mesh, nh);
-        CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+        TRY(exec_c2r_d(s, spec, s->phi[m]));
     } else {
         djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)), kThreads,
                             0, s->stream>>>(reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
-        if (s->phi[m]) CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
+        if (s->phi[m]) TRY(exec_c2r_d(s, spec, s->phi[m]));
         else CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
     }
     CUDA_TRY(cudaGetLastError());
@@ -1783,7 +1846,16 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         }
         // 3-D transforms, or with the fused z pass 2-D transforms batched over the z planes
         const int rank = s->zpass ? 2 : 3;
-        const long long batch = s->zpass ? res : 1;
+        if (s->zpass) {
+            // z planes per 2-D transform call (DJB_FFT_PLANES, a divisor of res): small
+            // batches keep a call's intermediate (its x-stage output) resident in L2 for
+            // its y stage
+            const char* zb = std::getenv("DJB_FFT_PLANES");
+            int b = zb ? std::atoi(zb) : kFftPlanes;
+            if (b < 1 || b > res || res % b) b = res;
+            s->zplanes = b;
+        }
+        const long long batch = s->zpass ? s->zplanes : 1;
         long long dims[3] = {res, res, res};
         long long cembed[3] = {res, res, res / 2 + 1};
         long long dembed[3] = {res, res, res};
@@ -1817,6 +1889,13 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
             CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
+            const char* zt = std::getenv("DJB_ZPASS_TMA");
+            if (!(zt && std::strcmp(zt, "0") == 0)) {
+                CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_tma<djb::KPhiFn>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZTSmem));
+                for (int m = 0; m < s->group; ++m) TRY(make_zmap(&s->zmap[m], s->mesh[m], res));
+                s->ztma = true;
+            }
         }
         if (s->sorted && s->gsx <= res) {
             for (int m = 0; m < s->group; ++m) {

@@ -36,7 +36,10 @@ from .nn import ForceNet
 from .pm import PMConfig, PMSolver, native_view
 
 COSMO = dict(Omega_c=0.31 - 0.049, Omega_b=0.049, h=0.677, n_s=0.965, sigma8=0.81)
+# the 2x mesh runs the throughput configuration's options; the 1x mesh the cheapest PM
+# (one CIC deposit, no interlacing, order-2 gradient), whose error the network corrects
 OPTS = dict(worder=4, antialias=1, grad_order=6)
+OPTS_LO = dict(worder=2, antialias=0, grad_order=2)
 A_INI = 0.02
 
 
@@ -95,10 +98,12 @@ def state_pk(psi, *, res: int, boxsize: float, bins: int = 32, device: int = 0):
 class CorrectionTrainer:
     """Training of a ForceNet on (2× − 1×) PM force residuals of n³ particles."""
 
-    def __init__(self, cosmo, *, n: int = 128, boxsize: float = 250.0, opts=OPTS, device: int = 0, seed: int = 0):
-        self.cosmo, self.n, self.L, self.opts, self.device = cosmo, n, boxsize, dict(opts), device
-        self.lo = PMSolver(PMConfig(res_pm=n, n_part=n, boxsize=boxsize, **opts), device=device)
-        self.hi = PMSolver(PMConfig(res_pm=2 * n, n_part=n, boxsize=boxsize, **opts), device=device)
+    def __init__(self, cosmo, *, n: int = 128, boxsize: float = 250.0, opts_lo=OPTS_LO, opts_hi=OPTS, device: int = 0,
+                 seed: int = 0):
+        self.cosmo, self.n, self.L, self.device = cosmo, n, boxsize, device
+        self.opts_lo, self.opts_hi = dict(opts_lo), dict(opts_hi)
+        self.lo = PMSolver(PMConfig(res_pm=n, n_part=n, boxsize=boxsize, **opts_lo), device=device)
+        self.hi = PMSolver(PMConfig(res_pm=2 * n, n_part=n, boxsize=boxsize, **opts_hi), device=device)
         self.net = ForceNet(layers=4, cin=4, hidden=32, cout=3, seed=seed, device=device)
         self.scales = (1.0, 1.0, 1.0)
 
@@ -159,15 +164,15 @@ class CorrectionTrainer:
 
 
 def train(cosmo, *, n=128, boxsize=250.0, seeds=range(64), snapshots=20, epochs=4, lr=1e-3, lr_end=1e-4,
-          device=0, log=print):
+          opts_lo=OPTS_LO, opts_hi=OPTS, device=0, log=print):
     """Trains a ForceNet on `snapshots` states of each training seed; returns the trainer."""
     import torch
-    T = CorrectionTrainer(cosmo, n=n, boxsize=boxsize, device=device)
+    T = CorrectionTrainer(cosmo, n=n, boxsize=boxsize, opts_lo=opts_lo, opts_hi=opts_hi, device=device)
     states = []
     t0 = time.perf_counter()
     for s in seeds:
         p0, m0 = initial_state(cosmo, n, boxsize, s, device)
-        _, _, st, _ = run(cosmo, p0, m0, res=2 * n, boxsize=boxsize, n_steps=snapshots, device=device,
+        _, _, st, _ = run(cosmo, p0, m0, res=2 * n, boxsize=boxsize, n_steps=snapshots, opts=opts_hi, device=device,
                           keep_states=True)
         states += st
     t_data = time.perf_counter() - t0
@@ -187,11 +192,13 @@ def train(cosmo, *, n=128, boxsize=250.0, seeds=range(64), snapshots=20, epochs=
         log(f"epoch {e}: mean relative loss {hist[-1]:.4f}")
     torch.cuda.synchronize(device)
     T.info = dict(n_states=len(states), data_s=t_data, train_s=time.perf_counter() - t0, loss_history=hist,
-                  scales=list(T.scales), epochs=epochs, lr=lr, lr_end=lr_end)
+                  scales=list(T.scales), epochs=epochs, lr=lr, lr_end=lr_end, opts_lo=dict(opts_lo),
+                  opts_hi=dict(opts_hi))
     return T
 
 
-def evaluate(cosmo, net, scales, *, n, boxsize, seeds, n_steps=20, device=0, bins=32, timing=False):
+def evaluate(cosmo, net, scales, *, n, boxsize, seeds, n_steps=20, opts_lo=OPTS_LO, opts_hi=OPTS, device=0,
+             bins=32, timing=False):
     """Plain 1×, corrected 1× and plain 2× runs from each held-out seed. Returns per-bin
     P(k) ratios to the 2× run (mean over seeds) for k < k_Nyq/2 of the 1× mesh, their
     largest deviations, and (timing) device ms per step of the corrected 1× and plain 2×."""
@@ -200,10 +207,12 @@ def evaluate(cosmo, net, scales, *, n, boxsize, seeds, n_steps=20, device=0, bin
     k = None
     for s in seeds:
         p0, m0 = initial_state(cosmo, n, boxsize, s, device)
-        p2, _, _, t2 = run(cosmo, p0, m0, res=2 * n, boxsize=boxsize, n_steps=n_steps, device=device, timing=timing)
-        p1, _, _, t1 = run(cosmo, p0, m0, res=n, boxsize=boxsize, n_steps=n_steps, device=device, timing=timing)
-        pc, _, _, tc = run(cosmo, p0, m0, res=n, boxsize=boxsize, n_steps=n_steps, device=device, net=net,
-                           scales=scales, timing=timing)
+        p2, _, _, t2 = run(cosmo, p0, m0, res=2 * n, boxsize=boxsize, n_steps=n_steps, opts=opts_hi, device=device,
+                           timing=timing)
+        p1, _, _, t1 = run(cosmo, p0, m0, res=n, boxsize=boxsize, n_steps=n_steps, opts=opts_lo, device=device,
+                           timing=timing)
+        pc, _, _, tc = run(cosmo, p0, m0, res=n, boxsize=boxsize, n_steps=n_steps, opts=opts_lo, device=device,
+                           net=net, scales=scales, timing=timing)
         k, P2, nm = state_pk(p2, res=n, boxsize=boxsize, bins=bins, device=device)
         _, P1, _ = state_pk(p1, res=n, boxsize=boxsize, bins=bins, device=device)
         _, Pc, _ = state_pk(pc, res=n, boxsize=boxsize, bins=bins, device=device)
