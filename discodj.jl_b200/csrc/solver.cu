@@ -849,11 +849,13 @@ struct djb_solver {
     // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
     bool zpass = false;
     float2* wN = nullptr;
-    // the z pass fed by bulk tensor copies: 2-D maps of each spectrum (8-byte complex
-    // elements, x = ky·nh + kx, y = kz); DJB_ZPASS_TMA=0 selects the register-fed form
-    CUtensorMap zmap[kMaxGroup];
-    bool ztma = false;
-    int zplanes = 0;   // z planes per 2-D transform call
+    // shift pipelining (DJB_OVERLAP=1): the second shift's deposit and the first shift's
+    // interpolation run on the solver's stream while the other shift's transform chain runs
+    // on `stream2` (higher priority), with its own cuFFT plans
+    bool overlap = false;
+    cudaStream_t stream2 = nullptr;
+    cufftHandle r2c_d2 = 0, c2r_d2 = 0;
+    cudaEvent_t ev[4] = {};
     float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
     float* scr[10] = {};    // staging and work buffers of the adjoint entry points, kept between calls
     size_t scr_n[10] = {};
@@ -1069,11 +1071,6 @@ size_t gather_smem(const djb_solver* s) { return size_t(s->gsx) * s->gS * s->gS 
 // Dynamic shared memory of a brick kernel, 2 CTAs per SM: 228 KB of shared memory
 // less 1 KB per CTA reserved by the runtime and the kernel's static barrier.
 constexpr int kBrickSmemMax = 113 * 1024;
-// z planes per 2-D transform call of the 1024^3 path (DJB_FFT_PLANES overrides)
-#ifndef DJB_FFT_PLANES_DEFAULT
-#define DJB_FFT_PLANES_DEFAULT 1024
-#endif
-constexpr int kFftPlanes = DJB_FFT_PLANES_DEFAULT;
 
 // Tensor map of a dense [res]^3 float mesh with boxes of sx x S x S elements.
 int make_tmap(CUtensorMap* m, const float* base, int res, int sx, int S) {
@@ -1093,29 +1090,6 @@ int make_tmap(CUtensorMap* m, const float* base, int res, int sx, int S) {
                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
-    return DJB_OK;
-}
-
-// 2-D tensor map of a res x res x (res/2+1) complex spectrum as 8-byte elements: x = the
-// flat index ky·nh + kx within a z plane, y = kz; boxes of kZTBox x 256 elements.
-int make_zmap(CUtensorMap* m, const void* base, int res) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-        if (q != cudaDriverEntryPointSuccess || !fn) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
-    const int64_t nh = res / 2 + 1;
-    const cuuint64_t dims[2] = {cuuint64_t(int64_t(res) * nh), cuuint64_t(res)};
-    const cuuint64_t strides[1] = {cuuint64_t(int64_t(res) * nh * 8)};
-    const cuuint32_t box[2] = {cuuint32_t(djb::kZTBox), 256};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_INT64, 2, const_cast<void*>(base), dims, strides, box, estr,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(DJB_ERR_CUDA, "cuTensorMapEncodeTiled (spectrum) failed (%d)", int(r));
     return DJB_OK;
 }
 
@@ -1307,40 +1281,10 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
 // Force evaluation for all shifts; if `step`, fused with the drift/kick/drift.
 // Reads s->psi (and s->mom). Output: s->acc (step == 0) or updated psi/mom.
 // The fused z pass of the 1024³ Poisson solve on the half spectrum in `mesh`.
-// The dense-mesh transforms: 3-D, or with the fused z pass the 2-D transforms of the z
-// planes in calls of s->zplanes planes.
-int exec_r2c_d(djb_solver* s, float* in, cufftComplex* out) {
-    if (!s->zpass || s->zplanes >= s->res) {
-        CUFFT_TRY(cufftExecR2C(s->r2c_d, in, out));
-        return DJB_OK;
-    }
-    const int64_t nh = s->res / 2 + 1;
-    for (int z = 0; z < s->res; z += s->zplanes)
-        CUFFT_TRY(cufftExecR2C(s->r2c_d, in + int64_t(z) * s->res * s->res, out + int64_t(z) * s->res * nh));
-    return DJB_OK;
-}
-int exec_c2r_d(djb_solver* s, cufftComplex* in, float* out) {
-    if (!s->zpass || s->zplanes >= s->res) {
-        CUFFT_TRY(cufftExecC2R(s->c2r_d, in, out));
-        return DJB_OK;
-    }
-    const int64_t nh = s->res / 2 + 1;
-    for (int z = 0; z < s->res; z += s->zplanes)
-        CUFFT_TRY(cufftExecC2R(s->c2r_d, in + int64_t(z) * s->res * nh, out + int64_t(z) * s->res * s->res));
-    return DJB_OK;
-}
-
 void launch_zpass(djb_solver* s, float* mesh, int nh) {
     const dim3 grid(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res));
     const djb::KPhiFn kp{s->lapT, s->makT, s->s0};
-    int m = -1;
-    for (int i = 0; i < s->group; ++i)
-        if (mesh == s->mesh[i]) m = i;
-    if (s->ztma && m >= 0) {
-        const int tiles = int(grid.x * grid.y);
-        djb::k_zpencil_tma<<<std::min(tiles, s->nsm), djb::kZPairThreads, djb::kZTSmem, s->stream>>>(
-            reinterpret_cast<float2*>(mesh), nh, s->wN, kp, s->zmap[m], s->err);
-    } else if (DJB_ZPASS_PAIR)
+    if (DJB_ZPASS_PAIR)
         djb::k_zpencil_pair<<<grid, djb::kZPairThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh,
                                                                                   s->wN, kp);
     else
@@ -1365,6 +1309,98 @@ int sort_particles(djb_solver* s, const float* mom, float dd1) {
 dim3 fd_grid(int res);
 int nn_correction(djb_solver* s);
 
+// The transform chain of mesh m (R2C, k-space multiplier or fused z pass, C2R) on
+// stream2 with its own plans.
+int transform_chain2(djb_solver* s, int m) {
+    float* mesh = s->mesh[m];
+    cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
+    const int64_t nh = s->res / 2 + 1;
+    CUFFT_TRY(cufftExecR2C(s->r2c_d2, s->phi[m], spec));
+    cudaStream_t keep = s->stream;
+    s->stream = s->stream2;  // the launchers run on s->stream
+    if (s->zpass) {
+        launch_zpass(s, mesh, int(nh));
+    } else {
+        djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)), kThreads,
+                            0, s->stream>>>(reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
+    }
+    s->stream = keep;
+    CUFFT_TRY(cufftExecC2R(s->c2r_d2, spec, s->phi[m]));
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+// The two-shift force with the shifts pipelined over two streams (DJB_OVERLAP=1, dense
+// finite-difference path, brick-sorted particles, no resampling, no network):
+//   stream  : sort | deposit 0 | deposit 1 | (wait T0) interpolate 0 | (wait T1) interpolate 1 + kick/drift
+//   stream2 :      (wait D0) transforms 0 = T0 | (wait D1) transforms 1 = T1
+// so that deposit 1 overlaps transforms 0 and interpolation 0 overlaps transforms 1.
+// The interpolation is split per shift (first/last sums in acc), as for larger shift sets.
+template <int W, int RR>
+int force_overlap_w(djb_solver* s, bool step, double alpha, double beta, double dd2) {
+    const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
+    const size_t cells = size_t(s->res) * s->res * s->res;
+    const GroupShifts both = group_shifts(s, 0, 2);
+    for (int m = 0; m < 2; ++m) CUDA_TRY(cudaMemsetAsync(s->phi[m], 0, cells * sizeof(float), s->stream));
+    for (int m = 0; m < 2; ++m) {
+        GroupShifts g{};
+        g.s[0] = both.s[m];
+        s->prof.begin(s->stream, PH_SCATTER);
+        djb::k_scatter_brick<W, 1><<<nbricks, djb::kTileThreads, scatter_smem(s), s->stream>>>(
+            s->psi, s->q1, s->n, s->np, s->Lf, s->res, s->res, g, s->phi[m], nullptr, s->err, brick_list(s),
+            s->tmap_s[m], s->tmap_s[m], s->tma ? 1 : 0);
+        s->prof.end(s->stream, PH_SCATTER, 1);
+        CUDA_TRY(cudaEventRecord(s->ev[m], s->stream));
+        CUDA_TRY(cudaStreamWaitEvent(s->stream2, s->ev[m], 0));
+        TRY(transform_chain2(s, m));
+        CUDA_TRY(cudaEventRecord(s->ev[2 + m], s->stream2));
+    }
+    for (int m = 0; m < 2; ++m) {
+        djb::GatherArgs a{};
+        a.psi = s->psi;
+        a.mom = s->mom;
+        a.acc = s->acc;
+        a.q1 = s->q1;
+        a.mesh[0] = s->phi[m];
+        a.sh.s[0] = both.s[m];
+        a.n = s->n;
+        a.np = s->np;
+        a.L = s->Lf;
+        a.res = s->res;
+        a.pitch = s->res;
+        a.c1 = s->c1;
+        a.c2 = s->c2;
+        a.c3 = s->c3;
+        a.first = (m == 0);
+        a.last = (m == 1);
+        a.divide = 1;
+        a.nshift_f = 2.0f;
+        a.step = step ? 1 : 0;
+        a.alpha = float(alpha);
+        a.beta = float(beta);
+        a.dd2 = float(dd2);
+        a.err = s->err;
+        a.perm = s->cur_perm;
+        a.extra = nullptr;
+        CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev[2 + m], 0));
+        s->prof.begin(s->stream, PH_GATHER);
+        djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, gather_smem(s), s->stream>>>(
+            a, brick_list(s), s->tmap[m], s->tmap[m], s->tma ? 1 : 0);
+        s->prof.end(s->stream, PH_GATHER, 1);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return DJB_OK;
+}
+
+int force_overlap(djb_solver* s, bool step, double alpha, double beta, double dd2) {
+#define DJB_FO(W_, R_) \
+    if (s->W == W_ && s->R == R_) return force_overlap_w<W_, R_>(s, step, alpha, beta, dd2);
+    DJB_FO(2, 1) DJB_FO(2, 2) DJB_FO(2, 3) DJB_FO(3, 1) DJB_FO(3, 2) DJB_FO(3, 3)
+    DJB_FO(4, 1) DJB_FO(4, 2) DJB_FO(4, 3)
+#undef DJB_FO
+    return fail(DJB_ERR_INVALID, "no overlapped force for this order");
+}
+
 int force(djb_solver* s, bool step, double dd1, double alpha, double beta, double dd2) {
     const int nh = s->res / 2 + 1;
     const int64_t nspec = int64_t(s->res) * s->res * nh;
@@ -1381,6 +1417,8 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         TRY(sort_particles(s, (step && dd1 != 0.0) ? s->mom : nullptr, float(dd1)));
         s->cur_perm = s->perm;
     }
+    if (s->overlap && s->cur_perm && !s->nn && s->nshift == 2 && s->phi[0] && s->phi[1] && s->R > 0)
+        return force_overlap(s, step, alpha, beta, dd2);
     for (int first = 0; first < s->nshift; first += s->group) {
         const int ns = std::min(s->group, s->nshift - first);
         const GroupShifts g = group_shifts(s, first, ns);
@@ -1403,7 +1441,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             float* mesh = s->mesh[m];
             cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
             s->prof.begin(s->stream, PH_R2C);
-            if (s->phi[m]) TRY(exec_r2c_d(s, s->phi[m], spec));
+            if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
             else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
             s->prof.end(s->stream, PH_R2C, 0);
             // network input, δ: the unshifted density is still in phi[0] after the R2C
@@ -1419,7 +1457,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
                 launch_zpass(s, mesh, nh);
                 s->prof.end(s->stream, PH_KSPACE, 1);
                 s->prof.begin(s->stream, PH_C2R);
-                TRY(exec_c2r_d(s, spec, s->phi[m]));
+                CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
                 s->prof.end(s->stream, PH_C2R, 0);
             } else if (!ik) {
                 s->prof.begin(s->stream, PH_KSPACE);
@@ -1428,7 +1466,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
                     reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
                 s->prof.end(s->stream, PH_KSPACE, 1);
                 s->prof.begin(s->stream, PH_C2R);
-                if (s->phi[m]) TRY(exec_c2r_d(s, spec, s->phi[m]));
+                if (s->phi[m]) CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
                 else CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
                 s->prof.end(s->stream, PH_C2R, 0);
             } else {
@@ -1499,16 +1537,16 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
 int poisson(djb_solver* s, int m) {
     float* mesh = s->mesh[m];
     cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
-    if (s->phi[m]) TRY(exec_r2c_d(s, s->phi[m], spec));
+    if (s->phi[m]) CUFFT_TRY(cufftExecR2C(s->r2c_d, s->phi[m], spec));
     else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
     const int nh = s->res / 2 + 1;
     if (s->zpass) {
         launch_zpass(s, mesh, nh);
-        TRY(exec_c2r_d(s, spec, s->phi[m]));
+        CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
     } else {
         djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)), kThreads,
                             0, s->stream>>>(reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
-        if (s->phi[m]) TRY(exec_c2r_d(s, spec, s->phi[m]));
+        if (s->phi[m]) CUFFT_TRY(cufftExecC2R(s->c2r_d, spec, s->phi[m]));
         else CUFFT_TRY(cufftExecC2R(s->c2r, spec, mesh));
     }
     CUDA_TRY(cudaGetLastError());
@@ -1696,6 +1734,13 @@ void release(djb_solver* s) {
     if (s->have_c2r_n) cufftDestroy(s->c2r_n);
     if (s->have_c2r_d) cufftDestroy(s->c2r_d);
     if (s->have_r2c_d) cufftDestroy(s->r2c_d);
+    if (s->overlap) {
+        cufftDestroy(s->r2c_d2);
+        cufftDestroy(s->c2r_d2);
+        for (cudaEvent_t e : s->ev)
+            if (e) cudaEventDestroy(e);
+        if (s->stream2) cudaStreamDestroy(s->stream2);
+    }
     for (void* p : s->allocs) cudaFree(p);
     for (float* p : s->scr)
         if (p) cudaFree(p);
@@ -1846,16 +1891,7 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         }
         // 3-D transforms, or with the fused z pass 2-D transforms batched over the z planes
         const int rank = s->zpass ? 2 : 3;
-        if (s->zpass) {
-            // z planes per 2-D transform call (DJB_FFT_PLANES, a divisor of res): small
-            // batches keep a call's intermediate (its x-stage output) resident in L2 for
-            // its y stage
-            const char* zb = std::getenv("DJB_FFT_PLANES");
-            int b = zb ? std::atoi(zb) : kFftPlanes;
-            if (b < 1 || b > res || res % b) b = res;
-            s->zplanes = b;
-        }
-        const long long batch = s->zpass ? s->zplanes : 1;
+        const long long batch = s->zpass ? res : 1;
         long long dims[3] = {res, res, res};
         long long cembed[3] = {res, res, res / 2 + 1};
         long long dembed[3] = {res, res, res};
@@ -1875,6 +1911,26 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                       CUFFT_R2C, batch, &work));
         CUFFT_TRY(cufftSetStream(s->r2c_d, s->stream));
         s->bytes += int64_t(work);
+        {
+            const char* ov = std::getenv("DJB_OVERLAP");
+            if (ov && std::strcmp(ov, "1") == 0 && s->group == 2 && s->sorted && !resample) {
+                int lo = 0, hi = 0;
+                CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+                CUDA_TRY(cudaStreamCreateWithPriority(&s->stream2, cudaStreamNonBlocking, hi));
+                for (cudaEvent_t& e : s->ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                CUFFT_TRY(cufftCreate(&s->c2r_d2));
+                CUFFT_TRY(cufftCreate(&s->r2c_d2));
+                s->overlap = true;
+                CUFFT_TRY(cufftMakePlanMany64(s->c2r_d2, rank, s->zpass ? dims + 1 : dims, cd, 1, cdist, dd, 1, ddist,
+                                              CUFFT_C2R, batch, &work));
+                s->bytes += int64_t(work);
+                CUFFT_TRY(cufftMakePlanMany64(s->r2c_d2, rank, s->zpass ? dims + 1 : dims, dd, 1, ddist, cd, 1, cdist,
+                                              CUFFT_R2C, batch, &work));
+                s->bytes += int64_t(work);
+                CUFFT_TRY(cufftSetStream(s->c2r_d2, s->stream2));
+                CUFFT_TRY(cufftSetStream(s->r2c_d2, s->stream2));
+            }
+        }
         if (s->zpass) {
             std::vector<float2> w(res);
             for (int j = 0; j < res; ++j)
@@ -1889,13 +1945,6 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
             CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
-            const char* zt = std::getenv("DJB_ZPASS_TMA");
-            if (!(zt && std::strcmp(zt, "0") == 0)) {
-                CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_tma<djb::KPhiFn>,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZTSmem));
-                for (int m = 0; m < s->group; ++m) TRY(make_zmap(&s->zmap[m], s->mesh[m], res));
-                s->ztma = true;
-            }
         }
         if (s->sorted && s->gsx <= res) {
             for (int m = 0; m < s->group; ++m) {

@@ -44,17 +44,6 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// 2-D box at global element coordinates (x, y) of `map` into shared memory at `dst`
-// (128-byte aligned); completion on `bar` as transaction bytes. x times the element size
-// must be a multiple of 16 bytes.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
 // Element-wise float add of the shared-memory box at `src` (16-byte aligned, laid out
 // as the map's box) into global memory at box coordinates (x, y, z) of `map`; the
 // coordinates are non-negative and the box lies inside the tensor.

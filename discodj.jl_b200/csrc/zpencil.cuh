@@ -25,8 +25,6 @@
 
 #include <cstdint>
 
-#include "tma.cuh"
-
 namespace djb {
 
 #ifndef DJB_ZPASS_BLOCKS
@@ -309,119 +307,6 @@ __global__ void __launch_bounds__(kZPairThreads, 2) k_zpencil_pair(float2* __res
     if (active) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) __stcs(col + int64_t(t + 32 * brev5(16 * h + i)) * zstride, conjf2(b[i]));
-    }
-}
-
-// ── the pair form fed by bulk tensor copies ─────────────────────────────────
-// The forms above stall on their strided loads (load latency, 26% of HBM bandwidth). This
-// persistent form (one CTA of 512 threads per SM) stages each tile (8 kx of one ky, all
-// 1024 kz) in shared memory with bulk tensor copies and requests the next tile's copies
-// before it transforms the current one, so that a tile is always in flight per SM.
-// The spectrum is described as a 2-D tensor of 8-byte complex elements: x = ky·nh + kx
-// (one z plane, flat) and y = kz. A tile's copy starts at the even x at or below
-// ky·nh + 8g (16-byte aligned start) and spans kZTBox = 10 elements, which covers the 8
-// wanted ones at offset o = 0 or 1; 4 copies of 256 kz rows fill the 1024 rows. Elements
-// past the tensor's end are filled with zeros by the copy; they belong to inactive
-// pencils (kx >= nh), whose results are not stored. Results leave by ordinary stores,
-// 8 kx of a kz row per 64 bytes. After step A has read the tile, its buffer holds the
-// transpose blocks (8 × 1058 complex < 1024 × 10).
-constexpr int kZTBox = 10;
-constexpr int kZTileBytes = kZRes * kZTBox * 8;        // 81,920
-constexpr int kZTSmem = 2 * kZTileBytes + 128;         // two tiles + two mbarriers
-static_assert(kZPencils * kZPlane <= kZRes * kZTBox, "transpose blocks fit a tile buffer");
-static_assert(kZPencils == 8, "tiles of 8 kx");
-
-template <class KPhi>
-__global__ void __launch_bounds__(kZPairThreads, 1) k_zpencil_tma(float2* __restrict__ f, int nh,
-                                                                  const float2* __restrict__ wN, KPhi kphi,
-                                                                  const __grid_constant__ CUtensorMap tm, int* err) {
-    extern __shared__ __align__(128) unsigned char zsm[];
-    float2* const buf0 = reinterpret_cast<float2*>(zsm);
-    float2* const buf1 = reinterpret_cast<float2*>(zsm + kZTileBytes);
-    uint64_t* const full = reinterpret_cast<uint64_t*>(zsm + 2 * kZTileBytes);
-    const int tid = threadIdx.x;
-    const int q = tid & 7;
-    const int h = (tid >> 3) & 1;
-    const int t = tid >> 4;
-    const int ngx = (nh + kZPencils - 1) / kZPencils;
-    const int ntiles = ngx * kZRes;
-    const int64_t zstride = int64_t(kZRes) * nh;
-    if (tid == 0) {
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
-    }
-    __syncthreads();
-    // one thread arms the barrier and issues the tile's four copies
-    auto issue = [&](int tile, int which) {
-        const int g = tile % ngx, ky = tile / ngx;
-        const int x0 = (ky * nh + g * kZPencils) & ~1;
-        float2* dst = which ? buf1 : buf0;
-        fence_proxy_async_smem();  // earlier generic accesses of the buffer precede the copies
-        mbar_arrive_expect_tx(&full[which], unsigned(kZTileBytes));
-#pragma unroll
-        for (int j = 0; j < 4; ++j) tma_load_2d(dst + j * 256 * kZTBox, &tm, x0, 256 * j, &full[which]);
-    };
-    int tile = blockIdx.x;
-    if (tid == 0 && tile < ntiles) issue(tile, 0);
-    unsigned parity0 = 0, parity1 = 0;
-    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-        const int which = it & 1;
-        const int next = tile + gridDim.x;
-        if (tid == 0 && next < ntiles) issue(next, which ^ 1);
-        const bool ok = mbar_wait(&full[which], which ? parity1 : parity0);
-        if (which) parity1 ^= 1u;
-        else parity0 ^= 1u;
-        if (__syncthreads_or(!ok)) {  // a copy never completed: report, let the other one land, stop
-            if (tid == 0) {
-                atomicOr(err, 8);
-                if (next < ntiles) mbar_wait(&full[which ^ 1], which ? parity0 : parity1);
-            }
-            __syncthreads();
-            return;
-        }
-        const int g = tile % ngx, ky = tile / ngx;
-        const int o = (ky * nh + g * kZPencils) & 1;
-        const int kx = g * kZPencils + q;
-        const bool active = kx < nh;
-        float2* const tb = which ? buf1 : buf0;
-        float2 b[16];
-        // A: x[t + 32 n1], n1 = 16 h + i, from the staged rows
-#pragma unroll
-        for (int i = 0; i < 16; ++i) b[i] = tb[(t + 32 * (16 * h + i)) * kZTBox + o + q];
-        __syncthreads();  // the tile is read: its buffer now holds the transpose blocks
-        float2* const sq = tb + q * kZPlane;
-        dft32_dif_pair(b, h);  // b[i] = Y[k1 = brev(16h + i)]
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const int k1 = brev5(16 * h + i);
-            sq[k1 * kZRow + t] = (k1 == 0) ? b[i] : cmul(b[i], __ldg(wN + ((t * k1) & (kZRes - 1))));
-        }
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) b[i] = sq[t * kZRow + 16 * h + i];
-        dft32_dif_pair(b, h);  // b[i] = X[t + 32 brev(16h + i)]
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const float K = active ? kphi.fast(kx, ky, t + 32 * brev5(16 * h + i)) : 0.0f;
-            b[i] = make_float2(b[i].x * K, -(b[i].y * K));
-        }
-        dft32_dit_pair(b, h);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const int n2 = 16 * h + i;
-            const float2 z = conjf2(b[i]);
-            sq[t * kZRow + n2] = (t == 0 || n2 == 0) ? z : cmul(z, conjf2(__ldg(wN + ((n2 * t) & (kZRes - 1)))));
-        }
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) b[i] = conjf2(sq[(16 * h + i) * kZRow + t]);
-        dft32_dif_pair(b, h);  // b[i] = conj(x[t + 32 brev(16h + i)])
-        if (active) {
-            float2* const col = f + int64_t(ky) * nh + kx;
-#pragma unroll
-            for (int i = 0; i < 16; ++i) __stcs(col + int64_t(t + 32 * brev5(16 * h + i)) * zstride, conjf2(b[i]));
-        }
-        __syncthreads();  // the buffer's transpose blocks are read before it is refilled
     }
 }
 

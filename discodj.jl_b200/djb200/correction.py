@@ -260,19 +260,24 @@ def _main(argv=None):
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-seeds", type=int, default=8)
+    ap.add_argument("--lr-end", type=float, default=1e-4)
     ap.add_argument("--eval-large", type=int, default=512, help="particles per side of the large evaluation (0: skip)")
+    ap.add_argument("--opts-lo", default=json.dumps(OPTS_LO), help="PMConfig options of the 1x mesh (JSON)")
+    ap.add_argument("--opts-hi", default=json.dumps(OPTS), help="PMConfig options of the 2x mesh (JSON)")
     args = ap.parse_args(argv)
+    opts_lo, opts_hi = json.loads(args.opts_lo), json.loads(args.opts_hi)
     os.makedirs(args.out, exist_ok=True)
     cosmo = Cosmology(**COSMO)
     T = train(cosmo, n=args.n, boxsize=args.boxsize, seeds=range(args.seeds), snapshots=args.snapshots,
-              epochs=args.epochs, lr=args.lr)
+              epochs=args.epochs, lr=args.lr, lr_end=args.lr_end, opts_lo=opts_lo, opts_hi=opts_hi)
     info = dict(T.info, n=args.n, boxsize=args.boxsize, train_seeds=args.seeds, snapshots=args.snapshots)
     held = range(1000, 1000 + args.eval_seeds)
-    info["eval_small"] = evaluate(cosmo, T.net, T.scales, n=args.n, boxsize=args.boxsize, seeds=held)
+    info["eval_small"] = evaluate(cosmo, T.net, T.scales, n=args.n, boxsize=args.boxsize, seeds=held,
+                                  opts_lo=opts_lo, opts_hi=opts_hi)
     if args.eval_large:
         nl = args.eval_large
         info["eval_large"] = evaluate(cosmo, T.net, T.scales, n=nl, boxsize=args.boxsize * nl / args.n,
-                                      seeds=held, timing=True)
+                                      seeds=held, timing=True, opts_lo=opts_lo, opts_hi=opts_hi)
     save(os.path.join(args.out, "force_correction.npz"), T.net, T.scales, info)
     with open(os.path.join(args.out, "force_correction.json"), "w") as f:
         json.dump(info, f, indent=1)
