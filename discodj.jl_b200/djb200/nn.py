@@ -153,6 +153,20 @@ class ForceNet:
         check(lib.djb_nn_adam_step(self._h, float(lr)))
 
 
+def allreduce_gradients(net, group=None):
+    """Data-parallel training over seeds, one replica per GPU: every replica's gradient
+    buffer is replaced by the mean over the replicas (djb_nn_grads, all_reduce,
+    djb_nn_set_grads) before its Adam step, so that the replicas' weights stay equal."""
+    import torch
+    import torch.distributed as dist
+    g = torch.from_numpy(net.grads())
+    if dist.get_backend(group) == "nccl":
+        g = g.cuda()
+    dist.all_reduce(g, group=group)
+    g /= dist.get_world_size(group)
+    net.set_grads(g.cpu().numpy())
+
+
 def force_correction_pair(cosmo, *, n=64, boxsize=250.0, res=128, a=1.0, seed=0, worder=4, grad_order=6,
                           device=0):
     """One training pair for the force-correction network on device tensors.

@@ -57,3 +57,48 @@ def test_reference_arm_other_ranks_do_nothing(capsys):
     args = argparse.Namespace(size="small", steps=1, warmup=3, gpus=2)
     bench.run_reference(args, world=2, rank=1)   # returns at once, prints nothing
     assert capsys.readouterr().out == ""
+
+
+class _HostGrads:
+    """Stands in for a ForceNet's gradient buffer on a CPU-only host."""
+
+    def __init__(self, g):
+        self.g = g
+
+    def grads(self):
+        return self.g.copy()
+
+    def set_grads(self, g):
+        self.g = g.copy()
+
+
+def _nn_worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
+                      LOCAL_RANK=str(rank))
+    import numpy as np
+    import torch.distributed as dist
+
+    import bench
+    from djb200.nn import allreduce_gradients
+    bench.dist_setup("gloo")
+    net = _HostGrads(np.arange(6, dtype=np.float32) * (rank + 1))
+    allreduce_gradients(net)
+    dist.destroy_process_group()
+    out.put((rank, net.g.tolist()))
+
+
+def test_nn_gradient_allreduce_gloo_world_size_2():
+    """djb_nn_grads -> all_reduce -> djb_nn_set_grads: both replicas end with the mean."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_nn_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    expect = [1.5 * i for i in range(6)]
+    assert res[0][1] == pytest.approx(expect) and res[1][1] == pytest.approx(expect)
