@@ -68,9 +68,9 @@ __device__ __forceinline__ void red_add_v4(float* dst, float a, float b, float c
                  : "memory");
 }
 
-// Waits for the barrier phase with the given parity; false when about 2^31 SM clock
-// cycles (about a second) pass without completion.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// Waits for the barrier phase with the given parity; false when `limit` SM clock cycles
+// pass without completion (by default 2^31, about a second).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long limit = (1LL << 31)) {
     const long long t0 = clock64();
     for (unsigned it = 0;; ++it) {
         unsigned ok;
@@ -80,7 +80,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
             : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (ok) return true;
-        if ((it & 255u) == 255u && clock64() - t0 > (1LL << 31)) return false;
+        if ((it & 255u) == 255u && clock64() - t0 > limit) return false;
     }
 }
 

@@ -110,6 +110,7 @@ SIGNATURES = {
     "djb_mesh_interp3": [_P, _P, _P, _P, _I],
     "djb_mesh_deposit3": [_P, _P, _P, _P, _I],
     "djb_state_density_modes": [_P, _I, _IP, _DP],
+    "djb_selftest_bounded_wait": [_I, _I, C.c_int64, _IP],
 }
 _RESTYPES = {"djb_version": C.c_char_p, "djb_last_error": C.c_char_p}
 

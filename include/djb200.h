@@ -300,6 +300,14 @@ DJB_API int djb_mesh_interp3(djb_solver* s, const float* psi, const float* mesh3
 /* The transpose of djb_mesh_interp3: mesh3[c](node) = sum_p W(X_p - node) vec_c(p). */
 DJB_API int djb_mesh_deposit3(djb_solver* s, const float* psi, const float* vec, float* mesh3, int32_t mem);
 
+/* ── self-test ───────────────────────────────────────────────────────────────
+ * No counterpart in the reference. Runs the bounded mbarrier wait that the library's
+ * bulk-copy kernels use on a barrier of its own: with arrive = 1 the barrier completes
+ * and *err_word = 0; with arrive = 0 nothing arrives, the wait gives up after
+ * limit_cycles SM cycles (at most 2^31, the kernels' own limit) and *err_word has bit 8
+ * set, the kernels' "a wait ran out" flag. No copy is in flight; the device stays usable. */
+DJB_API int djb_selftest_bounded_wait(int32_t device, int32_t arrive, int64_t limit_cycles, int32_t* err_word);
+
 /* ── non-allocating shell sums ──────────────────────────────────────────────
  * No counterpart in the reference. For callers that cannot allocate device
  * memory at the point of the call: applications whose device memory is owned by

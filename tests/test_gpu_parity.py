@@ -245,3 +245,21 @@ def test_state_density_modes_vs_oracle(djb):
     ref = ref / W
     ref[0] = 0.0
     assert np.max(np.abs(got - ref)) < 1e-5 * np.max(np.abs(ref))
+
+
+def test_bounded_wait_runs_out_and_reports(djb):
+    """The bulk-copy kernels' mbarrier wait is bounded: made to run out (a barrier that
+    nothing completes), it sets error bit 8 and returns; the device stays usable."""
+    import ctypes as C
+
+    from djb200 import _lib
+    err = C.c_int32(-1)
+    _lib.check(_lib.lib.djb_selftest_bounded_wait(0, 1, 1 << 20, C.byref(err)))
+    assert err.value == 0                      # the barrier completed
+    _lib.check(_lib.lib.djb_selftest_bounded_wait(0, 0, 1 << 20, C.byref(err)))
+    assert err.value & 8                       # the wait ran out and said so
+    # the context is intact: an ordinary force call still works
+    rng = np.random.default_rng(2)
+    psi = rng.standard_normal((16, 16, 16, 3)).astype(np.float32)
+    acc = djb.pm_acceleration(psi, djb.PMConfig(res_pm=32, n_part=16, boxsize=100.0, worder=4, grad_order=4))
+    assert np.all(np.isfinite(acc))
