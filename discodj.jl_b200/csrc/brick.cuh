@@ -176,15 +176,18 @@ constexpr int kScatterBoxes = DJB_SCATTER_BOXES;
 // Fixed-point unit of a brick of `cnt` particles. A node sum is at most
 // cnt * (MaxW3 * up + 1) (each rounded weight is below its value + 1), which must stay
 // below 2^32. Sparse bricks keep FixScale<W>::up; denser ones take the largest power of
-// two that keeps the bound, down to 2^20 (unit ~1e-6 of a particle's weight sum). Below
-// that the brick accumulates in float with shared float atomics (returns 0).
+// two that keeps the bound. The rounding error of a fixed-point sum is at most half a unit
+// per particle whatever the sum's size, while a float sum of many equal weights (a
+// collapsed clump) drifts by a fraction of its own ulp per addition; so fixed point stays
+// the more accurate form down to units of 2^8 (bricks of ~5.6e7 particles), below which
+// the brick accumulates in float with shared float atomics (returns 0).
 template <int W>
 __device__ __forceinline__ float brick_fixed_unit(unsigned cnt) {
     const float room = 4294967296.0f / float(cnt) - 1.0f;  // MaxW3 * up must stay below this
     if (room >= MaxW3<W>::v * FixScale<W>::up) return FixScale<W>::up;
     int e;
     frexpf(room / MaxW3<W>::v, &e);  // room / MaxW3 in [2^(e-1), 2^e)
-    return (e - 1 >= 20) ? ldexpf(1.0f, e - 1) : 0.0f;
+    return (e - 1 >= 8) ? ldexpf(1.0f, e - 1) : 0.0f;
 }
 
 template <int W, int NS>

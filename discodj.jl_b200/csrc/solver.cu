@@ -849,13 +849,6 @@ struct djb_solver {
     // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
     bool zpass = false;
     float2* wN = nullptr;
-    // shift pipelining (DJB_OVERLAP=1): the second shift's deposit and the first shift's
-    // interpolation run on the solver's stream while the other shift's transform chain runs
-    // on `stream2` (higher priority), with its own cuFFT plans
-    bool overlap = false;
-    cudaStream_t stream2 = nullptr;
-    cufftHandle r2c_d2 = 0, c2r_d2 = 0;
-    cudaEvent_t ev[4] = {};
     float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
     float* scr[10] = {};    // staging and work buffers of the adjoint entry points, kept between calls
     size_t scr_n[10] = {};
@@ -1309,98 +1302,6 @@ int sort_particles(djb_solver* s, const float* mom, float dd1) {
 dim3 fd_grid(int res);
 int nn_correction(djb_solver* s);
 
-// The transform chain of mesh m (R2C, k-space multiplier or fused z pass, C2R) on
-// stream2 with its own plans.
-int transform_chain2(djb_solver* s, int m) {
-    float* mesh = s->mesh[m];
-    cufftComplex* spec = reinterpret_cast<cufftComplex*>(mesh);
-    const int64_t nh = s->res / 2 + 1;
-    CUFFT_TRY(cufftExecR2C(s->r2c_d2, s->phi[m], spec));
-    cudaStream_t keep = s->stream;
-    s->stream = s->stream2;  // the launchers run on s->stream
-    if (s->zpass) {
-        launch_zpass(s, mesh, int(nh));
-    } else {
-        djb::k_kspace_mul<<<dim3(unsigned((s->res + djb::kSpecRows - 1) / djb::kSpecRows), unsigned(s->res)), kThreads,
-                            0, s->stream>>>(reinterpret_cast<float2*>(mesh), s->res, s->lapT, s->makT, s->s0);
-    }
-    s->stream = keep;
-    CUFFT_TRY(cufftExecC2R(s->c2r_d2, spec, s->phi[m]));
-    CUDA_TRY(cudaGetLastError());
-    return DJB_OK;
-}
-
-// The two-shift force with the shifts pipelined over two streams (DJB_OVERLAP=1, dense
-// finite-difference path, brick-sorted particles, no resampling, no network):
-//   stream  : sort | deposit 0 | deposit 1 | (wait T0) interpolate 0 | (wait T1) interpolate 1 + kick/drift
-//   stream2 :      (wait D0) transforms 0 = T0 | (wait D1) transforms 1 = T1
-// so that deposit 1 overlaps transforms 0 and interpolation 0 overlaps transforms 1.
-// The interpolation is split per shift (first/last sums in acc), as for larger shift sets.
-template <int W, int RR>
-int force_overlap_w(djb_solver* s, bool step, double alpha, double beta, double dd2) {
-    const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
-    const size_t cells = size_t(s->res) * s->res * s->res;
-    const GroupShifts both = group_shifts(s, 0, 2);
-    for (int m = 0; m < 2; ++m) CUDA_TRY(cudaMemsetAsync(s->phi[m], 0, cells * sizeof(float), s->stream));
-    for (int m = 0; m < 2; ++m) {
-        GroupShifts g{};
-        g.s[0] = both.s[m];
-        s->prof.begin(s->stream, PH_SCATTER);
-        djb::k_scatter_brick<W, 1><<<nbricks, djb::kTileThreads, scatter_smem(s), s->stream>>>(
-            s->psi, s->q1, s->n, s->np, s->Lf, s->res, s->res, g, s->phi[m], nullptr, s->err, brick_list(s),
-            s->tmap_s[m], s->tmap_s[m], s->tma ? 1 : 0);
-        s->prof.end(s->stream, PH_SCATTER, 1);
-        CUDA_TRY(cudaEventRecord(s->ev[m], s->stream));
-        CUDA_TRY(cudaStreamWaitEvent(s->stream2, s->ev[m], 0));
-        TRY(transform_chain2(s, m));
-        CUDA_TRY(cudaEventRecord(s->ev[2 + m], s->stream2));
-    }
-    for (int m = 0; m < 2; ++m) {
-        djb::GatherArgs a{};
-        a.psi = s->psi;
-        a.mom = s->mom;
-        a.acc = s->acc;
-        a.q1 = s->q1;
-        a.mesh[0] = s->phi[m];
-        a.sh.s[0] = both.s[m];
-        a.n = s->n;
-        a.np = s->np;
-        a.L = s->Lf;
-        a.res = s->res;
-        a.pitch = s->res;
-        a.c1 = s->c1;
-        a.c2 = s->c2;
-        a.c3 = s->c3;
-        a.first = (m == 0);
-        a.last = (m == 1);
-        a.divide = 1;
-        a.nshift_f = 2.0f;
-        a.step = step ? 1 : 0;
-        a.alpha = float(alpha);
-        a.beta = float(beta);
-        a.dd2 = float(dd2);
-        a.err = s->err;
-        a.perm = s->cur_perm;
-        a.extra = nullptr;
-        CUDA_TRY(cudaStreamWaitEvent(s->stream, s->ev[2 + m], 0));
-        s->prof.begin(s->stream, PH_GATHER);
-        djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, gather_smem(s), s->stream>>>(
-            a, brick_list(s), s->tmap[m], s->tmap[m], s->tma ? 1 : 0);
-        s->prof.end(s->stream, PH_GATHER, 1);
-    }
-    CUDA_TRY(cudaGetLastError());
-    return DJB_OK;
-}
-
-int force_overlap(djb_solver* s, bool step, double alpha, double beta, double dd2) {
-#define DJB_FO(W_, R_) \
-    if (s->W == W_ && s->R == R_) return force_overlap_w<W_, R_>(s, step, alpha, beta, dd2);
-    DJB_FO(2, 1) DJB_FO(2, 2) DJB_FO(2, 3) DJB_FO(3, 1) DJB_FO(3, 2) DJB_FO(3, 3)
-    DJB_FO(4, 1) DJB_FO(4, 2) DJB_FO(4, 3)
-#undef DJB_FO
-    return fail(DJB_ERR_INVALID, "no overlapped force for this order");
-}
-
 int force(djb_solver* s, bool step, double dd1, double alpha, double beta, double dd2) {
     const int nh = s->res / 2 + 1;
     const int64_t nspec = int64_t(s->res) * s->res * nh;
@@ -1417,8 +1318,6 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         TRY(sort_particles(s, (step && dd1 != 0.0) ? s->mom : nullptr, float(dd1)));
         s->cur_perm = s->perm;
     }
-    if (s->overlap && s->cur_perm && !s->nn && s->nshift == 2 && s->phi[0] && s->phi[1] && s->R > 0)
-        return force_overlap(s, step, alpha, beta, dd2);
     for (int first = 0; first < s->nshift; first += s->group) {
         const int ns = std::min(s->group, s->nshift - first);
         const GroupShifts g = group_shifts(s, first, ns);
@@ -1734,13 +1633,6 @@ void release(djb_solver* s) {
     if (s->have_c2r_n) cufftDestroy(s->c2r_n);
     if (s->have_c2r_d) cufftDestroy(s->c2r_d);
     if (s->have_r2c_d) cufftDestroy(s->r2c_d);
-    if (s->overlap) {
-        cufftDestroy(s->r2c_d2);
-        cufftDestroy(s->c2r_d2);
-        for (cudaEvent_t e : s->ev)
-            if (e) cudaEventDestroy(e);
-        if (s->stream2) cudaStreamDestroy(s->stream2);
-    }
     for (void* p : s->allocs) cudaFree(p);
     for (float* p : s->scr)
         if (p) cudaFree(p);
@@ -1911,26 +1803,6 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                       CUFFT_R2C, batch, &work));
         CUFFT_TRY(cufftSetStream(s->r2c_d, s->stream));
         s->bytes += int64_t(work);
-        {
-            const char* ov = std::getenv("DJB_OVERLAP");
-            if (ov && std::strcmp(ov, "1") == 0 && s->group == 2 && s->sorted && !resample) {
-                int lo = 0, hi = 0;
-                CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-                CUDA_TRY(cudaStreamCreateWithPriority(&s->stream2, cudaStreamNonBlocking, hi));
-                for (cudaEvent_t& e : s->ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-                CUFFT_TRY(cufftCreate(&s->c2r_d2));
-                CUFFT_TRY(cufftCreate(&s->r2c_d2));
-                s->overlap = true;
-                CUFFT_TRY(cufftMakePlanMany64(s->c2r_d2, rank, s->zpass ? dims + 1 : dims, cd, 1, cdist, dd, 1, ddist,
-                                              CUFFT_C2R, batch, &work));
-                s->bytes += int64_t(work);
-                CUFFT_TRY(cufftMakePlanMany64(s->r2c_d2, rank, s->zpass ? dims + 1 : dims, dd, 1, ddist, cd, 1, cdist,
-                                              CUFFT_R2C, batch, &work));
-                s->bytes += int64_t(work);
-                CUFFT_TRY(cufftSetStream(s->c2r_d2, s->stream2));
-                CUFFT_TRY(cufftSetStream(s->r2c_d2, s->stream2));
-            }
-        }
         if (s->zpass) {
             std::vector<float2> w(res);
             for (int j = 0; j < res; ++j)

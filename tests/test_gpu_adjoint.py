@@ -148,7 +148,7 @@ def _mode(n, m, phase, device):
     return (np.sqrt(2.0) * torch.cos(arg)).float()
 
 
-def _white_noise_fd_check(djb, n, res, L, n_modes, capsys, label, eps=1e-3, seed=21):
+def _white_noise_fd_check(djb, n, res, L, n_modes, capsys, label, eps=1e-3, seed=21, worder=2):
     """∂loss/∂(white noise) through 2LPT ICs and a checkpointed BullFrog run (CIC, grad 2,
     20 steps, checkpoints every 5), float32 on the GPU, against central differences
     (ε = 1e-3) of the same loss through the float64 oracle (2LPT ICs in float64, the
@@ -167,14 +167,14 @@ def _white_noise_fd_check(djb, n, res, L, n_modes, capsys, label, eps=1e-3, seed
     cl = djb.Cosmology(**COSMO)
     co = cz.compute_timetables(cz.Cosmology(**COSMO))
     steps, bins = 20, 32
-    kw = dict(boxsize=L, a_ini=0.02, a_end=1.0, n_steps=steps, res_pm=res, stepper="bullfrog", worder=2,
+    kw = dict(boxsize=L, a_ini=0.02, a_end=1.0, n_steps=steps, res_pm=res, stepper="bullfrog", worder=worder,
               grad_kernel_order=2, antialias=0, checkpoint_every=5, bins=bins)
     w = ics.white_noise(seed, n, device="cuda", dtype=torch.float32)
     _, pk0 = dad.white_noise_loss(cl, w, np.ones(bins), **dict(kw))
     target = 0.9 * pk0
     loss, gw = dad.white_noise_loss_and_gradient(cl, w, target, **dict(kw))
     coef = onb.stepper_coefficients(co, "bullfrog", 0.02, 1.0, steps)
-    port = cpm.CPUPM(opm.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=2, grad_order=2), dtype=np.float64)
+    port = cpm.CPUPM(opm.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=worder, grad_order=2), dtype=np.float64)
     w64 = w.double().cpu()
 
     def loss64(white):

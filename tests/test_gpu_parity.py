@@ -192,9 +192,8 @@ def test_state_calls_need_state(djb, golden):
 def test_dense_clump_vs_oracle(djb, W, n, res, clump, aa):
     """Thousands of particles on one node (a collapsed halo core): the brick deposit's
     32-bit fixed point must not wrap. `clump` particles sit on one mesh node and the
-    rest stay near their lattice sites. The cases cover a reduced fixed-point unit
-    (PCS with 3000, TSC with 6000 in one brick) and float accumulation (CIC with 5000,
-    PCS with 20000 in one brick, beyond what 32-bit fixed point holds at a 2^-20 unit)."""
+    rest stay near their lattice sites. The bricks holding the clump take reduced
+    fixed-point units: 2^21 (PCS, 3000), 2^20 (TSC, 6000), 2^19 (CIC, 5000; PCS, 20000)."""
     from oracle import nbody as onb
     from oracle import pm as opm
     L = 120.0
