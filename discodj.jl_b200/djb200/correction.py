@@ -36,10 +36,11 @@ from .nn import ForceNet
 from .pm import PMConfig, PMSolver, native_view
 
 COSMO = dict(Omega_c=0.31 - 0.049, Omega_b=0.049, h=0.677, n_s=0.965, sigma8=0.81)
-# the 2x mesh runs the throughput configuration's options; the 1x mesh the cheapest PM
-# (one CIC deposit, no interlacing, order-2 gradient), whose error the network corrects
+# the 2x mesh runs the throughput configuration's options; the 1x mesh a cheaper PM (TSC,
+# no interlacing, order-4 gradient, the assignment window divided out), whose remaining
+# error the network corrects
 OPTS = dict(worder=4, antialias=1, grad_order=6)
-OPTS_LO = dict(worder=2, antialias=0, grad_order=2)
+OPTS_LO = dict(worder=3, antialias=0, grad_order=4, deconvolve=True)
 A_INI = 0.02
 
 
@@ -163,7 +164,7 @@ class CorrectionTrainer:
         return loss
 
 
-def train(cosmo, *, n=128, boxsize=250.0, seeds=range(64), snapshots=20, epochs=4, lr=1e-3, lr_end=1e-4,
+def train(cosmo, *, n=128, boxsize=250.0, seeds=range(64), snapshots=20, epochs=8, lr=1e-3, lr_end=1e-4,
           opts_lo=OPTS_LO, opts_hi=OPTS, device=0, log=print):
     """Trains a ForceNet on `snapshots` states of each training seed; returns the trainer."""
     import torch
@@ -257,7 +258,7 @@ def _main(argv=None):
     ap.add_argument("--boxsize", type=float, default=250.0)
     ap.add_argument("--seeds", type=int, default=64)
     ap.add_argument("--snapshots", type=int, default=20)
-    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-seeds", type=int, default=8)
     ap.add_argument("--lr-end", type=float, default=1e-4)

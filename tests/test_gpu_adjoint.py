@@ -209,19 +209,30 @@ def _white_noise_fd_check(djb, n, res, L, n_modes, capsys, label, eps=1e-3, seed
 
 
 def test_white_noise_gradient_small_vs_finite_differences(djb, capsys):
-    an, fd, err = _white_noise_fd_check(djb, 32, 64, 62.5, 8, capsys, "white-noise gradient 32^3/64^3")
-    assert np.median(err) < 5e-2
-    assert np.corrcoef(an, fd)[0, 1] > 0.99
+    """32³/64³. The CIC weights are piecewise linear, so the loss has kinks wherever a
+    particle crosses a cell face: a difference over ±ε averages the derivative's jumps
+    of every crossing the step causes. The difference converges to the adjoint as ε
+    shrinks (measured: median relative error 7.2e-2 at ε = 1e-3, 1.8e-2 at 1e-4, 2.3e-3
+    at 1e-5); the check uses ε = 1e-5 (float64 differences) and reports ε = 1e-3."""
+    an, fd, err = _white_noise_fd_check(djb, 32, 64, 62.5, 8, capsys, "white-noise gradient 32^3/64^3, eps 1e-5",
+                                        eps=1e-5)
+    assert np.median(err) < 1e-2
+    assert np.corrcoef(an, fd)[0, 1] > 0.9999
+    an3, fd3, _ = _white_noise_fd_check(djb, 32, 64, 62.5, 8, capsys, "white-noise gradient 32^3/64^3, eps 1e-3")
+    assert np.corrcoef(an3, fd3)[0, 1] > 0.99
 
 
 @pytest.mark.slow
 def test_white_noise_gradient_c5_vs_finite_differences(djb, capsys):
-    """The differentiable-run configuration: 128³ particles on a 256³ mesh, L = 250. The
-    float64 differences take ~10 s per run on 16 cores, so the default checks 16 modes;
-    DJB_C5_MODES=64 runs the full set of the configuration."""
+    """The differentiable-run configuration: 128³ particles on a 256³ mesh, L = 250, at
+    ε = 1e-5 (see above; at the configuration's ε = 1e-3 the CIC kinks leave a median
+    relative error of 1.2e-1, correlation 0.82, over 16 modes). The float64 differences
+    take ~10 s per run on 16 cores, so the default checks 8 modes; DJB_C5_MODES=64 and
+    DJB_C5_EPS choose the configuration's full set and step."""
     import os
-    modes = int(os.environ.get("DJB_C5_MODES", "16"))
+    modes = int(os.environ.get("DJB_C5_MODES", "8"))
+    eps = float(os.environ.get("DJB_C5_EPS", "1e-5"))
     an, fd, err = _white_noise_fd_check(djb, 128, 256, 250.0, modes, capsys,
-                                        "white-noise gradient C5 128^3/256^3")
-    assert np.median(err) < 5e-2
-    assert np.corrcoef(an, fd)[0, 1] > 0.99
+                                        f"white-noise gradient C5 128^3/256^3, eps {eps:g}", eps=eps)
+    assert np.median(err) < 3e-2
+    assert np.corrcoef(an, fd)[0, 1] > 0.9999
