@@ -362,12 +362,19 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-nn", action="store_true")
+    ap.add_argument("--only-nn-corrected", action="store_true",
+                    help="run only the NN-corrected comparison at 512^3 and print it (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("warm-up must be >= 3 steps")
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.only_nn_corrected:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps(nn_corrected(world)), flush=True)
         return
     import numpy as np
     import torch

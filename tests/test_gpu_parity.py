@@ -262,3 +262,20 @@ def test_bounded_wait_runs_out_and_reports(djb):
     psi = rng.standard_normal((16, 16, 16, 3)).astype(np.float32)
     acc = djb.pm_acceleration(psi, djb.PMConfig(res_pm=32, n_part=16, boxsize=100.0, worder=4, grad_order=4))
     assert np.all(np.isfinite(acc))
+
+
+def test_lpt_ics_on_the_gpu_match_the_pinned_cpu_path(djb):
+    """The initial conditions run the same torch restatement on the GPU in float32 as on
+    the CPU in float64, where 2LPT is pinned to the fixture at 1e-12: white noise → φ →
+    2LPT / 3LPT shapes → (Ψ, Π) at a = 0.02, 32³ particles, L = 62.5."""
+    import torch
+
+    from djb200 import ics
+    c = djb.Cosmology("Planck18EEBAOSN")
+    w = ics.white_noise(5, 32, device="cpu", dtype=torch.float64)
+    for order in (2, 3):
+        p64, m64 = ics.lpt_ics(c, 32, 62.5, 0.02, n_order=order, white=w)
+        p32, m32 = ics.lpt_ics(c, 32, 62.5, 0.02, n_order=order, device="cuda", dtype=torch.float32,
+                               white=w.float().cuda())
+        assert rel(p32.cpu().numpy(), p64.numpy()) < 1e-5
+        assert rel(m32.cpu().numpy(), m64.numpy()) < 1e-5
