@@ -158,6 +158,61 @@ __device__ __forceinline__ void for_box_wrapped(const TileBox& box, int res, int
     }
 }
 
+// ── lanes assigned by shared-memory bank ────────────────────────────────────
+// A warp's loads (or atomics) of one stencil element hit shared memory at (the stencil
+// origin of each lane's particle) + (the element's constant offset), so two lanes
+// conflict exactly when their origins agree modulo the 32 banks; with particles in
+// sort order the origins are effectively random and an access costs about 3 wavefronts.
+// bank_assign gives the lanes of a CTA round of 256 particles by origin bank: the r-th
+// particle of bank b goes to lane b of warp r (r < 8), and the particles beyond 8 per
+// bank fill the lanes left empty, in order. Every thread of the CTA calls it; `has`:
+// the thread owns a particle of origin bank `bank`. Returns whether the thread got a
+// particle and, in `owner`, the thread that owns it.
+struct BankTable {
+    unsigned cnt[32];                  // particles per origin bank
+    unsigned full[kTileThreads / 32];  // lanes of tab filled by their own bank
+    unsigned wempty[kTileThreads / 32];
+    unsigned novf;
+    unsigned char tab[kTileThreads];   // [warp][lane] -> owner thread
+    unsigned char ovf[kTileThreads];   // owners beyond 8 per bank
+};
+
+__device__ __forceinline__ bool bank_assign(BankTable& T, bool has, unsigned bank, unsigned& owner) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __syncthreads();  // the previous round's table has been read
+    if (tid < 32) T.cnt[tid] = 0u;
+    if (tid < kTileThreads / 32) T.full[tid] = 0u;
+    if (tid == 0) T.novf = 0u;
+    __syncthreads();
+    if (has) {
+        const unsigned r = atomicAdd(&T.cnt[bank], 1u);
+        if (r < unsigned(kTileThreads / 32)) {
+            T.tab[r * 32 + bank] = (unsigned char)tid;
+            atomicOr(&T.full[r], 1u << bank);
+        } else {
+            T.ovf[atomicAdd(&T.novf, 1u)] = (unsigned char)tid;
+        }
+    }
+    __syncthreads();
+    bool valid = (T.full[warp] >> lane) & 1u;
+    const unsigned nov = T.novf;
+    if (nov) {  // uniform: read after the barrier
+        const unsigned m = __ballot_sync(0xffffffffu, !valid);
+        if (lane == 0) T.wempty[warp] = __popc(m);
+        __syncthreads();
+        unsigned before = 0;
+        for (int w2 = 0; w2 < warp; ++w2) before += T.wempty[w2];
+        const unsigned idx = before + __popc(m & ((1u << lane) - 1u));
+        if (!valid && idx < nov) {
+            T.tab[tid] = T.ovf[idx];
+            valid = true;
+        }
+        __syncthreads();
+    }
+    owner = T.tab[tid];
+    return valid;
+}
+
 // ── mass assignment ───────────────────────────────────────────────────────────
 // Box: the deposit box (BrickList::ssx, sSs, sos); kScatterBoxes shifts of the group
 // are filled per pass over the brick's particles, one box each. One box per pass (45 KB
@@ -194,9 +249,10 @@ template <int W, int NS>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scatter_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     GroupShifts sh, float* __restrict__ mesh0, float* __restrict__ mesh1, int* err, BrickList bl,
-    const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1, int tma) {
+    const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1, int tma, int banked) {
     constexpr int NB = kScatterBoxes < NS ? kScatterBoxes : NS;  // boxes per particle pass
     extern __shared__ __align__(128) unsigned int sacc[];
+    __shared__ BankTable s_bt;
     const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
@@ -221,10 +277,37 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
             *reinterpret_cast<uint4*>(sacc + t) = make_uint4(0u, 0u, 0u, 0u);
         __syncthreads();
         for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
-            // lanes 8 slots apart: particles of one cell land in different warps, which
-            // keeps same-address shared atomics out of a single instruction
-            const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
-            if (slot >= cnt) continue;
+            unsigned slot;
+            if (NB == 1 && banked) {
+                // lanes by the shared-memory bank of the deposit origin (bank_assign); the
+                // particles of one cell share a bank and so land in different warps
+                const unsigned own_slot = r0 + tid;
+                unsigned bank = 0;
+                if (own_slot < cnt) {
+                    const int64_t po = bl.perm[start + own_slot];
+                    int io, jo, ko;
+                    ld.ijk(po, io, jo, ko);
+                    const float Xo[3] = {psi[po] + q1[io], psi[po + np] + q1[jo], psi[po + 2 * np] + q1[ko]};
+                    const Shift3 so = (g0 == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
+                    int dd[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float s = (a == 0) ? so.x : (a == 1) ? so.y : so.z;
+                        const int bb = wbase<W>(grid_coord(Xo[a] + s, L, resf, nullptr));
+                        const int v = box_rel(bb + WLo<W>::v, box.o[a], res);
+                        dd[a] = v < 0 ? 0 : (v > box.S[a] - W ? box.S[a] - W : v);
+                    }
+                    bank = unsigned(((dd[2] * box.S[1] + dd[1]) * box.P + dd[0]) & 31);
+                }
+                unsigned own;
+                if (!bank_assign(s_bt, own_slot < cnt, bank, own)) continue;
+                slot = r0 + own;
+            } else {
+                // lanes 8 slots apart: particles of one cell land in different warps, which
+                // keeps same-address shared atomics out of a single instruction
+                slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
+                if (slot >= cnt) continue;
+            }
             const int64_t p = bl.perm[start + slot];
             int i, j, k;
             ld.ijk(p, i, j, k);
@@ -538,18 +621,13 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
     int tma) {
     extern __shared__ __align__(128) float sbox[];
     __shared__ __align__(8) uint64_t s_bar;
-    __shared__ unsigned s_cnt[32];                  // particles per origin bank
-    __shared__ unsigned char s_tab[kTileThreads];   // [warp][lane] -> owner thread
-    __shared__ unsigned s_full[kTileWarps];         // lanes of s_tab filled by their bank
-    __shared__ unsigned char s_ovf[kTileThreads];   // owners beyond 8 per bank
-    __shared__ unsigned s_novf;
-    __shared__ unsigned s_wempty[kTileWarps];
+    __shared__ BankTable s_bt;
     constexpr int E = W + 2 * R;
     const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
     if (cnt == 0) return;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int n = A.n;
     const int64_t np = A.np;
     const int res = A.res;
@@ -587,12 +665,9 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
         const bool finish = A.last && g == NS - 1;       // mean, correction, kick-drift
 #pragma unroll 1
         for (unsigned sr = 0; sr < cnt; sr += kTileThreads) {
-            if (tid < 32) s_cnt[tid] = 0u;
-            if (tid < kTileWarps) s_full[tid] = 0u;
-            if (tid == 0) s_novf = 0u;
-            __syncthreads();
-            // owners: the origin bank of this shift's stencil, counted per bank
+            // owners: the origin bank of this shift's stencil
             const unsigned slot = sr + tid;
+            unsigned bank = 0;
             if (slot < cnt) {
                 const int64_t p = bl.perm[start + slot];
                 int i, j, k;
@@ -600,34 +675,10 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
                 const float X[3] = {A.psi[p] + A.q1[i], A.psi[p + np] + A.q1[j], A.psi[p + 2 * np] + A.q1[k]};
                 int d[3];
                 stencil_origin<W, R>(X, sgs, box, A.L, resf, res, d);
-                const unsigned bank = unsigned((d[2] * box.plane + d[1] * box.P + d[0]) & 31);
-                const unsigned r = atomicAdd(&s_cnt[bank], 1u);
-                if (r < unsigned(kTileWarps)) {
-                    s_tab[r * 32 + bank] = (unsigned char)tid;
-                    atomicOr(&s_full[r], 1u << bank);
-                } else {
-                    s_ovf[atomicAdd(&s_novf, 1u)] = (unsigned char)tid;
-                }
+                bank = unsigned((d[2] * box.plane + d[1] * box.P + d[0]) & 31);
             }
-            __syncthreads();
-            bool valid = (s_full[warp] >> lane) & 1u;
-            // the particles beyond 8 per bank fill the empty lanes, in order
-            const unsigned nov = s_novf;
-            if (nov) {
-                const unsigned m = __ballot_sync(0xffffffffu, !valid);
-                if (lane == 0) s_wempty[warp] = __popc(m);
-                __syncthreads();
-                unsigned before = 0;
-                for (int w2 = 0; w2 < warp; ++w2) before += s_wempty[w2];
-                const unsigned idx = before + __popc(m & ((1u << lane) - 1u));
-                if (!valid && idx < nov) {
-                    s_tab[tid] = s_ovf[idx];
-                    valid = true;
-                }
-                __syncthreads();
-            }
-            if (valid) {
-                const unsigned own = s_tab[tid];
+            unsigned own;
+            if (bank_assign(s_bt, slot < cnt, bank, own)) {
                 const int64_t p = bl.perm[start + sr + own];
                 int i, j, k;
                 ld.ijk(p, i, j, k);
@@ -730,8 +781,8 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
                     A.acc[p + 2 * np] = a3[2];
                 }
             }
-            __syncthreads();  // the table and counters are reset for the next super-round
         }
+        __syncthreads();  // the box is read before the next shift's copy
     }
 }
 

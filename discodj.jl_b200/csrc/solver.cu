@@ -1097,7 +1097,7 @@ void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShi
         const int tma = (dense && s->tma) ? 1 : 0;
         djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, std::min(NS, djb::kScatterBoxes) * scatter_smem(s), s->stream>>>(
             s->psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, m0, m1, s->err, brick_list(s), s->tmap_s[0],
-            s->tmap_s[NS > 1 ? 1 : 0], tma);
+            s->tmap_s[NS > 1 ? 1 : 0], tma, s->banked ? 1 : 0);
         return;
     }
     if (s->tiled) {
@@ -1586,7 +1586,7 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
     if (s->W == W_)                                                                                            \
         djb::k_scatter_brick<W_, 1><<<nbricks, djb::kTileThreads, scatter_smem(s), s->stream>>>(                \
             psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, brick_list(s), s->tmap_s[0], \
-            s->tmap_s[0], tma);
+            s->tmap_s[0], tma, s->banked ? 1 : 0);
             DJB_VS(2) DJB_VS(3) DJB_VS(4)
 #undef DJB_VS
         } else {
