@@ -462,13 +462,17 @@ __global__ void __launch_bounds__(kThreads) k_gather(GatherArgs A) {
 // out_c(p) = Σ_n W(X_p − n) f_c(n) over the W-order stencil of X_p = q + Ψ_p, for three
 // dense res³ meshes f_c = f + c·res³ ([z][y][x]); the interpolation of pm.jl:344-364
 // applied to given node values, without shifts.
+// perm (or null): the particles are visited in that order (the brick sort: neighbouring
+// threads then read neighbouring nodes).
 template <int W>
 __global__ void __launch_bounds__(kThreads) k_interp3(const float* __restrict__ psi, const float* __restrict__ q1,
                                                       int n, int64_t np, float L, int res,
                                                       const float* __restrict__ f, float scale,
-                                                      float* __restrict__ out, int* err) {
-    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= np) return;
+                                                      float* __restrict__ out, int* err,
+                                                      const int* __restrict__ perm = nullptr) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int64_t p = perm ? int64_t(perm[t]) : t;
     LatticeDiv ld;
     ld.init(n);
     int i, j, k;
@@ -1483,7 +1487,8 @@ int nn_correction(djb_solver* s) {
 #define DJB_INTERP(W_)                                                                                          \
     if (s->W == W_)                                                                                             \
         djb::k_interp3<W_><<<blocks(s->np), kThreads, 0, s->stream>>>(s->psi, s->q1, s->n, s->np, s->Lf, s->res, \
-                                                                      s->nnd, s->nn_out, s->nnacc, s->err);
+                                                                      s->nnd, s->nn_out, s->nnacc, s->err,   \
+                                                                      s->cur_perm);
     DJB_INTERP(2)
     DJB_INTERP(3)
     DJB_INTERP(4)
