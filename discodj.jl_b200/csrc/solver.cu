@@ -1329,12 +1329,8 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
     const bool ik = (s->cfg.grad_order == 0);
     const bool resample = (s->cfg.n_resample > 1);
     s->cur_perm = nullptr;
-    if (s->nn && step && dd1 != 0.0) {
-        // the correction is evaluated at the drifted positions: drift first, then run
-        // the force pipeline without its fused first drift
-        djb::k_drift<<<grid_for(3 * s->np), kThreads, 0, s->stream>>>(s->psi, s->mom, float(dd1), 3 * s->np);
-        dd1 = 0.0;
-    }
+    // the first drift is applied by the binning pass (or the first deposit without the
+    // sort), before the network correction reads the positions
     if (s->tiled && s->sorted) {
         TRY(sort_particles(s, (step && dd1 != 0.0) ? s->mom : nullptr, float(dd1)));
         s->cur_perm = s->perm;

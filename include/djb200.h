@@ -287,8 +287,8 @@ DJB_API int djb_nn_info(const djb_nn* h, int32_t* layers, int32_t* cin, int32_t*
  *   out_scale * interp(net([delta_scale * delta, force_scale * F]))(X_p)
  * to the PM acceleration of pm.jl:507-521, where delta and F are the unshifted density
  * contrast and finite-difference force on the mesh (as djb_mesh_fields computes them) and
- * interp is the solver's W-order interpolation at X = q + Psi (djb_mesh_interp3). The
- * drift before the force is then a separate pass. Needs a finite-difference gradient
+ * interp is the solver's W-order interpolation at X = q + Psi (djb_mesh_interp3), at
+ * the positions the force sees (after the step's first drift). Needs a finite-difference gradient
  * (2/4/6), no resampling, a non-lean solver with res divisible by 4 and antialias 0 or 1;
  * net = NULL detaches. The solver keeps 4 + 3 meshes and 3*n^3 floats for it. The
  * network runs on the solver's stream (its stream is set to the solver's at every force). */
