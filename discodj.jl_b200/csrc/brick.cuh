@@ -158,61 +158,6 @@ __device__ __forceinline__ void for_box_wrapped(const TileBox& box, int res, int
     }
 }
 
-// ── lanes assigned by shared-memory bank ────────────────────────────────────
-// A warp's loads (or atomics) of one stencil element hit shared memory at (the stencil
-// origin of each lane's particle) + (the element's constant offset), so two lanes
-// conflict exactly when their origins agree modulo the 32 banks; with particles in
-// sort order the origins are effectively random and an access costs about 3 wavefronts.
-// bank_assign gives the lanes of a CTA round of 256 particles by origin bank: the r-th
-// particle of bank b goes to lane b of warp r (r < 8), and the particles beyond 8 per
-// bank fill the lanes left empty, in order. Every thread of the CTA calls it; `has`:
-// the thread owns a particle of origin bank `bank`. Returns whether the thread got a
-// particle and, in `owner`, the thread that owns it.
-struct BankTable {
-    unsigned cnt[32];                  // particles per origin bank
-    unsigned full[kTileThreads / 32];  // lanes of tab filled by their own bank
-    unsigned wempty[kTileThreads / 32];
-    unsigned novf;
-    unsigned char tab[kTileThreads];   // [warp][lane] -> owner thread
-    unsigned char ovf[kTileThreads];   // owners beyond 8 per bank
-};
-
-__device__ __forceinline__ bool bank_assign(BankTable& T, bool has, unsigned bank, unsigned& owner) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    __syncthreads();  // the previous round's table has been read
-    if (tid < 32) T.cnt[tid] = 0u;
-    if (tid < kTileThreads / 32) T.full[tid] = 0u;
-    if (tid == 0) T.novf = 0u;
-    __syncthreads();
-    if (has) {
-        const unsigned r = atomicAdd(&T.cnt[bank], 1u);
-        if (r < unsigned(kTileThreads / 32)) {
-            T.tab[r * 32 + bank] = (unsigned char)tid;
-            atomicOr(&T.full[r], 1u << bank);
-        } else {
-            T.ovf[atomicAdd(&T.novf, 1u)] = (unsigned char)tid;
-        }
-    }
-    __syncthreads();
-    bool valid = (T.full[warp] >> lane) & 1u;
-    const unsigned nov = T.novf;
-    if (nov) {  // uniform: read after the barrier
-        const unsigned m = __ballot_sync(0xffffffffu, !valid);
-        if (lane == 0) T.wempty[warp] = __popc(m);
-        __syncthreads();
-        unsigned before = 0;
-        for (int w2 = 0; w2 < warp; ++w2) before += T.wempty[w2];
-        const unsigned idx = before + __popc(m & ((1u << lane) - 1u));
-        if (!valid && idx < nov) {
-            T.tab[tid] = T.ovf[idx];
-            valid = true;
-        }
-        __syncthreads();
-    }
-    owner = T.tab[tid];
-    return valid;
-}
-
 // ── mass assignment ───────────────────────────────────────────────────────────
 // Box: the deposit box (BrickList::ssx, sSs, sos); kScatterBoxes shifts of the group
 // are filled per pass over the brick's particles, one box each. One box per pass (45 KB
@@ -249,10 +194,9 @@ template <int W, int NS>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scatter_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     GroupShifts sh, float* __restrict__ mesh0, float* __restrict__ mesh1, int* err, BrickList bl,
-    const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1, int tma, int banked) {
+    const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1, int tma) {
     constexpr int NB = kScatterBoxes < NS ? kScatterBoxes : NS;  // boxes per particle pass
     extern __shared__ __align__(128) unsigned int sacc[];
-    __shared__ BankTable s_bt;
     const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
@@ -277,37 +221,10 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
             *reinterpret_cast<uint4*>(sacc + t) = make_uint4(0u, 0u, 0u, 0u);
         __syncthreads();
         for (unsigned r0 = 0; r0 < cnt; r0 += kTileThreads) {
-            unsigned slot;
-            if (NB == 1 && banked) {
-                // lanes by the shared-memory bank of the deposit origin (bank_assign); the
-                // particles of one cell share a bank and so land in different warps
-                const unsigned own_slot = r0 + tid;
-                unsigned bank = 0;
-                if (own_slot < cnt) {
-                    const int64_t po = bl.perm[start + own_slot];
-                    int io, jo, ko;
-                    ld.ijk(po, io, jo, ko);
-                    const float Xo[3] = {psi[po] + q1[io], psi[po + np] + q1[jo], psi[po + 2 * np] + q1[ko]};
-                    const Shift3 so = (g0 == 0) ? sh.s[0] : sh.s[NS > 1 ? 1 : 0];
-                    int dd[3];
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        const float s = (a == 0) ? so.x : (a == 1) ? so.y : so.z;
-                        const int bb = wbase<W>(grid_coord(Xo[a] + s, L, resf, nullptr));
-                        const int v = box_rel(bb + WLo<W>::v, box.o[a], res);
-                        dd[a] = v < 0 ? 0 : (v > box.S[a] - W ? box.S[a] - W : v);
-                    }
-                    bank = unsigned(((dd[2] * box.S[1] + dd[1]) * box.P + dd[0]) & 31);
-                }
-                unsigned own;
-                if (!bank_assign(s_bt, own_slot < cnt, bank, own)) continue;
-                slot = r0 + own;
-            } else {
-                // lanes 8 slots apart: particles of one cell land in different warps, which
-                // keeps same-address shared atomics out of a single instruction
-                slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
-                if (slot >= cnt) continue;
-            }
+            // lanes 8 slots apart: particles of one cell land in different warps, which
+            // keeps same-address shared atomics out of a single instruction
+            const unsigned slot = r0 + unsigned((tid & 31) * (kTileThreads / 32) + (tid >> 5));
+            if (slot >= cnt) continue;
             const int64_t p = bl.perm[start + slot];
             int i, j, k;
             ld.ijk(p, i, j, k);
@@ -585,204 +502,6 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
                 A.acc[p + 2 * np] = a3[2];
             }
         }
-    }
-}
-
-// ── interpolation with bank-sorted lanes ────────────────────────────────────
-// The loads of one stencil element by the 32 lanes of a warp hit shared memory at
-// (stencil origin of the lane's particle) + (the element's constant offset), so two
-// lanes conflict exactly when their origins agree modulo 32 banks; with particles in
-// sort order the 32 origins are effectively random and a load costs 2.8 wavefronts.
-// Here the lanes are assigned per shift by origin bank: each super-round of 256
-// particles is counted into the 32 banks (shared atomics), the r-th particle of bank b
-// goes to lane b of warp r (r < 8), and the particles beyond 8 in a bank fill the lanes
-// left empty. A warp then reads 32 distinct banks except for the filled-in lanes.
-// The lane that interpolates a particle is not its owner, so the partial sums across
-// the shifts go through the solver's acceleration array (A.acc) and the last shift's
-// lane applies the mean, the correction and the kick-drift. The potential box is staged
-// once per shift for all super-rounds of the brick.
-template <int W, int R>
-__device__ __forceinline__ void stencil_origin(const float X[3], const Shift3& sg, const TileBox& box, float L,
-                                               float resf, int res, int d[3]) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float s = (a == 0) ? sg.x : (a == 1) ? sg.y : sg.z;
-        const float gc = grid_coord(X[a] + s, L, resf, nullptr);
-        const int bb = wbase<W>(gc);
-        d[a] = box_rel(bb + WLo<W>::v - R, box.o[a], res);
-        constexpr int E = W + 2 * R;
-        d[a] = d[a] < 0 ? 0 : (d[a] > box.S[a] - E ? box.S[a] - E : d[a]);
-    }
-}
-
-template <int W, int R, int NS>
-__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gather_brick_banked(
-    GatherArgs A, BrickList bl, const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
-    int tma) {
-    extern __shared__ __align__(128) float sbox[];
-    __shared__ __align__(8) uint64_t s_bar;
-    __shared__ BankTable s_bt;
-    constexpr int E = W + 2 * R;
-    const int b = brick_of_block(bl, blockIdx.x);
-    unsigned start, cnt;
-    brick_range(bl, b, start, cnt);
-    if (cnt == 0) return;
-    const int tid = threadIdx.x;
-    const int n = A.n;
-    const int64_t np = A.np;
-    const int res = A.res;
-    const TileBox box = aligned_box(bl, b, bl.so, bl.sS, bl.sx);
-    const bool bulk = tma && box_inside(box, res) && (smem_u32(sbox) & 127u) == 0u;
-    const bool vec = ((A.pitch | res) & 3) == 0;
-    const unsigned box_bytes = unsigned(box.plane) * unsigned(box.S[2]) * 4u;
-    if (bulk && tid == 0) mbar_init(&s_bar, 1);
-    __syncthreads();
-    unsigned parity = 0;
-    const float resf = float(res);
-    const float cc[4] = {0.0f, A.c1, A.c2, A.c3};
-    LatticeDiv ld;
-    ld.init(n);
-#pragma unroll 1
-    for (int g = 0; g < NS; ++g) {
-        const Shift3 sgs = (g == 0) ? A.sh.s[0] : A.sh.s[NS > 1 ? 1 : 0];
-        if (bulk) {
-            if (tid == 0) {
-                fence_proxy_async_smem();  // the previous shift's reads precede the refill
-                mbar_arrive_expect_tx(&s_bar, box_bytes);
-                tma_load_3d(sbox, (g == 0) ? &tm0 : &tm1, box.o[0], box.o[1], box.o[2], &s_bar);
-            }
-            const bool ok = mbar_wait(&s_bar, parity);
-            parity ^= 1u;
-            if (__syncthreads_or(!ok)) {  // the copy never completed: report, do not spin
-                if (tid == 0) atomicOr(A.err, 8);
-                return;
-            }
-        } else {
-            stage_box_wrapped(sbox, (g == 0) ? A.mesh[0] : A.mesh[NS > 1 ? 1 : 0], box, res, A.pitch, vec);
-            __syncthreads();
-        }
-        const bool first_sum = A.first && g == 0;        // no partial sum to continue
-        const bool finish = A.last && g == NS - 1;       // mean, correction, kick-drift
-#pragma unroll 1
-        for (unsigned sr = 0; sr < cnt; sr += kTileThreads) {
-            // owners: the origin bank of this shift's stencil
-            const unsigned slot = sr + tid;
-            unsigned bank = 0;
-            if (slot < cnt) {
-                const int64_t p = bl.perm[start + slot];
-                int i, j, k;
-                ld.ijk(p, i, j, k);
-                const float X[3] = {A.psi[p] + A.q1[i], A.psi[p + np] + A.q1[j], A.psi[p + 2 * np] + A.q1[k]};
-                int d[3];
-                stencil_origin<W, R>(X, sgs, box, A.L, resf, res, d);
-                bank = unsigned((d[2] * box.plane + d[1] * box.P + d[0]) & 31);
-            }
-            unsigned own;
-            if (bank_assign(s_bt, slot < cnt, bank, own)) {
-                const int64_t p = bl.perm[start + sr + own];
-                int i, j, k;
-                ld.ijk(p, i, j, k);
-                const float ps[3] = {A.psi[p], A.psi[p + np], A.psi[p + 2 * np]};
-                const float X[3] = {ps[0] + A.q1[i], ps[1] + A.q1[j], ps[2] + A.q1[k]};
-                float w[3][W], u[3][E];
-                int d[3];
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    const float s = (a == 0) ? sgs.x : (a == 1) ? sgs.y : sgs.z;
-                    const float gc = grid_coord(X[a] + s, A.L, resf, A.err);
-                    const int bb = wbase<W>(gc);
-#pragma unroll
-                    for (int o = 0; o < W; ++o) w[a][o] = wk<W>(fabsf(gc - float(bb + WLo<W>::v + o)));
-#pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        float sacc = 0.0f;
-#pragma unroll
-                        for (int o = 0; o < W; ++o) {
-                            const int t = e - R - o;
-                            if (t > 0 && t <= R) sacc -= w[a][o] * cc[t > 0 ? t : 0];
-                            if (t < 0 && -t <= R) sacc += w[a][o] * cc[t < 0 ? -t : 0];
-                        }
-                        u[a][e] = sacc;
-                    }
-                    d[a] = box_rel(bb + WLo<W>::v - R, box.o[a], res);
-                    if (d[a] < 0 || d[a] > box.S[a] - E) {  // not binned consistently: report, stay in bounds
-                        atomicOr(A.err, 2);
-                        d[a] = d[a] < 0 ? 0 : box.S[a] - E;
-                    }
-                }
-                float sX = 0.0f, sY = 0.0f, sZ = 0.0f;
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const float* pl = sbox + (d[2] + e) * box.plane + d[0];
-                    if (e >= R && e < R + W) {
-                        const int c = e - R;
-#pragma unroll
-                        for (int bb = 0; bb < W; ++bb) {
-                            const float* row = pl + (d[1] + R + bb) * box.P;
-                            float rx = 0.0f, rc = 0.0f;
-#pragma unroll
-                            for (int x = 0; x < E; ++x) {
-                                const float v = row[x];
-                                rx += u[0][x] * v;
-                                if (x >= R && x < R + W) rc += w[0][x - R] * v;
-                            }
-                            sX += (w[1][bb] * w[2][c]) * rx;
-                            sY += (u[1][bb + R] * w[2][c]) * rc;
-                            sZ += (u[2][e] * w[1][bb]) * rc;
-                        }
-#pragma unroll
-                        for (int h = 0; h < 2 * R; ++h) {
-                            const int ey = (h < R) ? h : h + W;
-                            const float* row = pl + (d[1] + ey) * box.P + R;
-                            float rc = 0.0f;
-#pragma unroll
-                            for (int a = 0; a < W; ++a) rc += w[0][a] * row[a];
-                            sY += (u[1][ey] * w[2][c]) * rc;
-                        }
-                    } else {
-#pragma unroll
-                        for (int bb = 0; bb < W; ++bb) {
-                            const float* row = pl + (d[1] + R + bb) * box.P + R;
-                            float rc = 0.0f;
-#pragma unroll
-                            for (int a = 0; a < W; ++a) rc += w[0][a] * row[a];
-                            sZ += (u[2][e] * w[1][bb]) * rc;
-                        }
-                    }
-                }
-                float a3[3] = {sX, sY, sZ};
-                if (!first_sum) {
-                    a3[0] += A.acc[p];
-                    a3[1] += A.acc[p + np];
-                    a3[2] += A.acc[p + 2 * np];
-                }
-                if (finish) {
-                    if (A.divide) {
-                        a3[0] = a3[0] / A.nshift_f;
-                        a3[1] = a3[1] / A.nshift_f;
-                        a3[2] = a3[2] / A.nshift_f;
-                    }
-                    if (A.extra) {
-                        a3[0] += A.extra[p];
-                        a3[1] += A.extra[p + np];
-                        a3[2] += A.extra[p + 2 * np];
-                    }
-                }
-                if (finish && A.step) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const float m = A.alpha * A.mom[p + c * np] + A.beta * a3[c];
-                        A.mom[p + c * np] = m;
-                        A.psi[p + c * np] = ps[c] + A.dd2 * m;
-                    }
-                } else {
-                    A.acc[p] = a3[0];
-                    A.acc[p + np] = a3[1];
-                    A.acc[p + 2 * np] = a3[2];
-                }
-            }
-        }
-        __syncthreads();  // the box is read before the next shift's copy
     }
 }
 

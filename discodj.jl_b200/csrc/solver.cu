@@ -886,7 +886,6 @@ struct djb_solver {
     int* err = nullptr;
     bool have_state = false;
     bool tiled = true;  // shared-memory tiled scatter/gather (DJB_KERNELS=simple selects the per-particle ones)
-    bool banked = true; // brick interpolation with bank-sorted lanes (DJB_GATHER_BANKED=0: sort order)
     // force correction (djb_solver_attach_nn): network inputs [δ, F_x, F_y, F_z] scaled by
     // nn_in (δ) and nn_fin (F), its output scaled by nn_out, interpolated to the particles
     djb_nn* nn = nullptr;
@@ -1101,7 +1100,7 @@ void launch_scatter_t(djb_solver* s, const float* mom, float dd1, const GroupShi
         const int tma = (dense && s->tma) ? 1 : 0;
         djb::k_scatter_brick<W, NS><<<nbricks, djb::kTileThreads, std::min(NS, djb::kScatterBoxes) * scatter_smem(s), s->stream>>>(
             s->psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, m0, m1, s->err, brick_list(s), s->tmap_s[0],
-            s->tmap_s[NS > 1 ? 1 : 0], tma, s->banked ? 1 : 0);
+            s->tmap_s[NS > 1 ? 1 : 0], tma);
         return;
     }
     if (s->tiled) {
@@ -1144,20 +1143,12 @@ void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
         const size_t smem = gather_smem(s);
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const int tma = (s->tma && a.mesh[0] == s->phi[0]) ? 1 : 0;
-        if (s->banked) {
-            if (ns == 1)
-                djb::k_gather_brick_banked<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
-                    a, brick_list(s), s->tmap[0], s->tmap[0], tma);
-            else
-                djb::k_gather_brick_banked<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
-                    a, brick_list(s), s->tmap[0], s->tmap[1], tma);
-        } else if (ns == 1) {
+        if (ns == 1)
             djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 a, brick_list(s), s->tmap[0], s->tmap[0], tma);
-        } else {
+        else
             djb::k_gather_brick<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 a, brick_list(s), s->tmap[0], s->tmap[1], tma);
-        }
         return;
     }
     if (R > 0 && s->tiled) {
@@ -1189,14 +1180,6 @@ int tiled_attrs_wr() {
                                   int(cudaSharedmemCarveoutMaxShared)));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   int(cudaSharedmemCarveoutMaxShared)));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_banked<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kBrickSmemMax));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_banked<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kBrickSmemMax));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_banked<W, R, 1>,
-                                  cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_banked<W, R, 2>,
-                                  cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)));
     return DJB_OK;
 }
 
@@ -1587,7 +1570,7 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
     if (s->W == W_)                                                                                            \
         djb::k_scatter_brick<W_, 1><<<nbricks, djb::kTileThreads, scatter_smem(s), s->stream>>>(                \
             psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err, brick_list(s), s->tmap_s[0], \
-            s->tmap_s[0], tma, s->banked ? 1 : 0);
+            s->tmap_s[0], tma);
             DJB_VS(2) DJB_VS(3) DJB_VS(4)
 #undef DJB_VS
         } else {
@@ -1680,10 +1663,6 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         s->tiled = !(kind && std::strcmp(kind, "simple") == 0);
     }
     if (s->tiled) TRY(tiled_attrs(s->W, s->R));
-    {
-        const char* gb = std::getenv("DJB_GATHER_BANKED");
-        s->banked = !(gb && std::strcmp(gb, "0") == 0);
-    }
     {
         const char* srt = std::getenv("DJB_SORT");
         s->sorted = s->tiled && !(srt && std::strcmp(srt, "0") == 0);
