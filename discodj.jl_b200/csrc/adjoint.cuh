@@ -153,8 +153,10 @@ __global__ void __launch_bounds__(256) k_scatter_weighted(const float* __restric
 #endif
 constexpr int kFdTX = 32, kFdTY = DJB_FD_TY, kFdZ = DJB_FD_Z, kFdR = 3;
 
-// Periodic index of any integer (tiles and windows reach past 2·res on small meshes).
+// Periodic index of any integer (tiles and windows reach past 2·res on small meshes);
+// indices inside the mesh, the common case, take one unsigned comparison.
 __device__ __forceinline__ int fd_wrap(int v, int res) {
+    if (unsigned(v) < unsigned(res)) return v;
     v %= res;
     return v < 0 ? v + res : v;
 }

@@ -218,15 +218,18 @@ __device__ __forceinline__ void dit_stage16(float2 (&b)[16]) {
     }
 }
 
+// The partner of the pair is `P` lanes away (P pencils per CTA, P = 8 or 16).
+template <int P>
 __device__ __forceinline__ float2 shfl_pair(float2 v) {
-    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, 8), __shfl_xor_sync(0xffffffffu, v.y, 8));
+    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, P), __shfl_xor_sync(0xffffffffu, v.y, P));
 }
 
 // Forward DIF over the pair: natural order in, bit-reversed order out (position 16h + i).
+template <int P>
 __device__ __forceinline__ void dft32_dif_pair(float2 (&b)[16], int h) {
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        const float2 o = shfl_pair(b[j]);
+        const float2 o = shfl_pair<P>(b[j]);
         if (h == 0) {
             b[j] = make_float2(b[j].x + o.x, b[j].y + o.y);
         } else {
@@ -241,6 +244,7 @@ __device__ __forceinline__ void dft32_dif_pair(float2 (&b)[16], int h) {
 }
 
 // Forward DIT over the pair: bit-reversed order in, natural order out.
+template <int P>
 __device__ __forceinline__ void dft32_dit_pair(float2 (&b)[16], int h) {
     dit_stage16<2>(b);
     dit_stage16<4>(b);
@@ -249,22 +253,23 @@ __device__ __forceinline__ void dft32_dit_pair(float2 (&b)[16], int h) {
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const float2 m = (h == 1 && j > 0) ? cmul(b[j], c_w32[j]) : b[j];
-        const float2 o = shfl_pair(m);
+        const float2 o = shfl_pair<P>(m);
         b[j] = (h == 0) ? make_float2(m.x + o.x, m.y + o.y) : make_float2(o.x - m.x, o.y - m.y);
     }
 }
 
-// Thread (q, h, t) at threadIdx.x = q + 8 h + 16 t: pencil q, half h, and t = n2 (steps
-// A, B') or k1 (steps B, A'); a warp reads 4 kz rows of 8 consecutive kx per load.
-template <class KPhi>
-__global__ void __launch_bounds__(kZPairThreads, 2) k_zpencil_pair(float2* __restrict__ f, int nh,
-                                                                   const float2* __restrict__ wN, KPhi kphi) {
-    extern __shared__ __align__(16) float2 s[];  // kZPencils transpose blocks
-    const int q = threadIdx.x & 7;
-    const int h = (threadIdx.x >> 3) & 1;
-    const int t = threadIdx.x >> 4;
+// P pencils per CTA of 64·P threads. Thread (q, h, t) at threadIdx.x = q + P h + 2P t:
+// pencil q, half h, and t = n2 (steps A, B') or k1 (steps B, A'); a warp reads 32/P kz
+// row pairs of P consecutive kx (8·P bytes each) per load.
+template <class KPhi, int P = 8>
+__global__ void __launch_bounds__(64 * P, P == 8 ? 2 : 1) k_zpencil_pair(float2* __restrict__ f, int nh,
+                                                                         const float2* __restrict__ wN, KPhi kphi) {
+    extern __shared__ __align__(16) float2 s[];  // P transpose blocks
+    const int q = threadIdx.x & (P - 1);
+    const int h = (threadIdx.x / P) & 1;
+    const int t = threadIdx.x / (2 * P);
     const int ky = blockIdx.y;
-    const int kx = blockIdx.x * kZPencils + q;
+    const int kx = blockIdx.x * P + q;
     const bool active = kx < nh;
     const int64_t zstride = int64_t(kZRes) * nh;
     float2* __restrict__ col = f + int64_t(ky) * nh + (active ? kx : 0);
@@ -274,7 +279,7 @@ __global__ void __launch_bounds__(kZPairThreads, 2) k_zpencil_pair(float2* __res
 #pragma unroll
     for (int i = 0; i < 16; ++i)
         b[i] = active ? __ldcs(col + int64_t(t + 32 * (16 * h + i)) * zstride) : make_float2(0.f, 0.f);
-    dft32_dif_pair(b, h);  // b[i] = Y[k1 = brev(16h + i)]
+    dft32_dif_pair<P>(b, h);  // b[i] = Y[k1 = brev(16h + i)]
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         const int k1 = brev5(16 * h + i);
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(kZPairThreads, 2) k_zpencil_pair(float2* __res
     // B: thread pair k1 = t: DFT over n2 (this thread: n2 = 16 h + i)
 #pragma unroll
     for (int i = 0; i < 16; ++i) b[i] = sq[t * kZRow + 16 * h + i];
-    dft32_dif_pair(b, h);  // b[i] = X[t + 32 brev(16h + i)]
+    dft32_dif_pair<P>(b, h);  // b[i] = X[t + 32 brev(16h + i)]
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         const float K = kphi.fast(kx, ky, t + 32 * brev5(16 * h + i));
@@ -292,7 +297,7 @@ __global__ void __launch_bounds__(kZPairThreads, 2) k_zpencil_pair(float2* __res
     }
     // A': inverse DFT over k2 -> Z[k1 = t][n2 = 16 h + i]; this thread reads and writes
     // only its half of row t
-    dft32_dit_pair(b, h);
+    dft32_dit_pair<P>(b, h);
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         const int n2 = 16 * h + i;
@@ -303,7 +308,7 @@ __global__ void __launch_bounds__(kZPairThreads, 2) k_zpencil_pair(float2* __res
     // B': thread pair n2 = t: inverse DFT over k1 (this thread: k1 = 16 h + i)
 #pragma unroll
     for (int i = 0; i < 16; ++i) b[i] = conjf2(sq[(16 * h + i) * kZRow + t]);
-    dft32_dif_pair(b, h);  // b[i] = conj(x[t + 32 brev(16h + i)])
+    dft32_dif_pair<P>(b, h);  // b[i] = conj(x[t + 32 brev(16h + i)])
     if (active) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) __stcs(col + int64_t(t + 32 * brev5(16 * h + i)) * zstride, conjf2(b[i]));
