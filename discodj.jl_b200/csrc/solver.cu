@@ -852,7 +852,6 @@ struct djb_solver {
     // res == 1024: the dense transforms are batched 2-D transforms of the z planes and
     // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
     bool zpass = false;
-    bool zp16 = false;   // z pass with 16 pencils per CTA (DJB_ZPASS_P16=1)
     float2* wN = nullptr;
     float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
     float* scr[10] = {};    // staging and work buffers of the adjoint entry points, kept between calls
@@ -1282,11 +1281,7 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
 void launch_zpass(djb_solver* s, float* mesh, int nh) {
     const dim3 grid(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res));
     const djb::KPhiFn kp{s->lapT, s->makT, s->s0};
-    if (s->zp16) {
-        const dim3 grid16(unsigned((nh + 15) / 16), unsigned(s->res));
-        djb::k_zpencil_pair<djb::KPhiFn, 16><<<grid16, 16 * 64, 16 * djb::kZPlane * 8, s->stream>>>(
-            reinterpret_cast<float2*>(mesh), nh, s->wN, kp);
-    } else if (DJB_ZPASS_PAIR)
+    if (DJB_ZPASS_PAIR)
         djb::k_zpencil_pair<<<grid, djb::kZPairThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh,
                                                                                   s->wN, kp);
     else
@@ -1823,12 +1818,6 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
             CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
-            CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn, 16>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * djb::kZPlane * 8));
-            {
-                const char* z16 = std::getenv("DJB_ZPASS_P16");
-                s->zp16 = z16 && std::strcmp(z16, "1") == 0;
-            }
         }
         if (s->sorted && s->gsx <= res) {
             for (int m = 0; m < s->group; ++m) {
