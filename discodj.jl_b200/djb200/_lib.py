@@ -111,6 +111,7 @@ SIGNATURES = {
     "djb_mesh_deposit3": [_P, _P, _P, _P, _I],
     "djb_state_density_modes": [_P, _I, _IP, _DP],
     "djb_selftest_bounded_wait": [_I, _I, C.c_int64, _IP],
+    "djb_lpt2_ics": [_P, _I, _D, _DP, _DP, _I, _D, _P, _P, _I, _P],
 }
 _RESTYPES = {"djb_version": C.c_char_p, "djb_last_error": C.c_char_p}
 

@@ -306,3 +306,27 @@ def lpt_ics(cosmo, n: int, boxsize: float, a: float, *, n_order: int = 2, seed: 
         Psi += (D ** m) * shapes[f"psi_{m}"]
         Pi += (m * D ** (m - 1)) * shapes[f"psi_{m}"]
     return Psi, Pi
+
+
+def lpt2_ics_native(cosmo, n: int, boxsize: float, a: float, *, seed: int = 42, white=None, device: int = 0):
+    """2LPT (Ψ, Π = dΨ/dD) at scale factor a from the library's CUDA kernels
+    (`djb_lpt2_ics`): the same white noise → φ → ψ₁, ψ₂ chain as `lpt_ics(n_order=2)`,
+    with the fields and products in float32 on the GPU. `white`: (n,n,n) [i,j,k] tensor
+    (default: `white_noise(seed, n)` on the device). Returns native (3,n,n,n) float32
+    device tensors (the library's particle layout, `pm.native_view`)."""
+    import ctypes as C
+
+    from . import _lib
+    dev = f"cuda:{device}"
+    w = white if white is not None else white_noise(seed, n, device=dev, dtype=torch.float32)
+    w_native = w.to(dev, torch.float32).permute(2, 1, 0).contiguous()   # x fastest
+    k_tab, p_tab = linear_power_spectrum(cosmo.params)
+    k_tab = np.ascontiguousarray(k_tab, dtype=np.float64)
+    p_tab = np.ascontiguousarray(p_tab, dtype=np.float64)
+    psi = torch.empty((3, n, n, n), dtype=torch.float32, device=dev)
+    pi = torch.empty_like(psi)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    _lib.check(_lib.lib.djb_lpt2_ics(C.c_void_p(w_native.data_ptr()), int(n), float(boxsize), _lib.dptr(k_tab),
+                                     _lib.dptr(p_tab), len(k_tab), float(cosmo.Dplus(a)), C.c_void_p(psi.data_ptr()),
+                                     C.c_void_p(pi.data_ptr()), int(device), C.c_void_p(stream)))
+    return psi, pi

@@ -197,6 +197,20 @@ DJB_API int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logari
  * The particle state stays on the device. */
 DJB_API int djb_state_density_modes(djb_solver* s, int32_t nmodes, const int32_t* modes, double* out);
 
+/* ── initial conditions (2LPT) ───────────────────────────────────────────────
+ * Replaces the GPU path of `nbody_ics_lpt` at n_order = 2 (src/ics/grf.jl:118-144,
+ * src/lpt/nlpt_core.jl:44-311, src/nbody/run_nbody.jl:180-208): white noise w (device, n^3
+ * float32, x fastest) -> phi(k) = rfft(w) * (-sqrt(P(|k|) (n/L)^3) / k^2) with P linearly
+ * interpolated in the host table (k_tab, p_tab, npk points, clamped at its ends) ->
+ * psi_1 = -D phi and the second-order shape from the 3/2-padded source
+ * mu2 = sum_{a<b} (psi_aa psi_bb - psi_ab^2) -> Psi = D psi_1 + D^2 psi_2 and
+ * Pi = dPsi/dD = psi_1 + 2 D psi_2 at growth factor D, written to psi and pi (device,
+ * (n,n,n,3) float32). n a multiple of 4. Runs on `stream` (a cudaStream_t, NULL = legacy
+ * default) and waits for it; allocates its work areas (about 6 (3n/2)^3 + 6 n^3 floats)
+ * for the call. */
+DJB_API int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab,
+                         int32_t npk, double D, float* psi, float* pi, int32_t device, void* stream);
+
 /* ── adjoints (vector-Jacobian products) ────────────────────────────────────
  * No counterpart in the reference, which has no adjoint; these are the transposes
  * of the forward operators above, checked against finite differences of float64
