@@ -23,6 +23,9 @@
 
 #include <cmath>
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "common.h"
@@ -95,7 +98,7 @@ __global__ void k_fphi(float2* __restrict__ spec, int n, double dk, double amp, 
     }
 }
 
-// The ext-grid spectrum of psi_ab = D_b D_a (-phi)... as (i k_b)(-(i k_a) phi) = k_a k_b phi
+// The ext-grid spectrum of psi_ab = D_b psi_a = (i k_b)(-(i k_a) phi) = k_a k_b phi
 // (Nyquist-zeroed factors), embedded from the n grid (index h = n/2 dropped on every axis,
 // the upper half of the full axes moved to the top of the ext axes) and scaled by
 // (ext/n)^3 / ext^3 = 1/n^3, the inverse transform's normalisation folded in.
@@ -185,6 +188,27 @@ __global__ void k_lpt_combine(const float* __restrict__ p1, const float* __restr
     }
 }
 
+// cuFFT plans kept per (device, size, kind) for the life of the library: creating a 768^3
+// plan takes longer than the whole 512^3 computation.
+std::mutex g_plan_mu;
+std::map<std::tuple<int, int, int>, cufftHandle> g_plans;
+
+cufftResult cached_plan(int device, int size, cufftType kind, cufftHandle* out) {
+    std::lock_guard<std::mutex> lock(g_plan_mu);
+    const auto key = std::make_tuple(device, size, int(kind));
+    auto it = g_plans.find(key);
+    if (it != g_plans.end()) {
+        *out = it->second;
+        return CUFFT_SUCCESS;
+    }
+    cufftHandle h = 0;
+    const cufftResult r = cufftPlan3d(&h, size, size, size, kind);
+    if (r != CUFFT_SUCCESS) return r;
+    g_plans[key] = h;
+    *out = h;
+    return CUFFT_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab,
@@ -205,7 +229,6 @@ extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const
     const double dk = 2 * M_PI / boxsize;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cufftHandle r2c_n = 0, c2r_n = 0, r2c_e = 0, c2r_e = 0;
-    bool h1 = false, h2 = false, h3 = false, h4 = false;
     float2 *phi = nullptr, *spec = nullptr, *espec = nullptr, *s1 = nullptr, *s2 = nullptr;
     float *ediag = nullptr, *emu = nullptr, *eoff = nullptr, *f1 = nullptr, *f2 = nullptr;
     double *dkt = nullptr, *dpt = nullptr;
@@ -224,14 +247,10 @@ extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const
     f2 = f1 + N;
     ICS_CUDA(cudaMemcpyAsync(dkt, k_tab, sizeof(double) * npk, cudaMemcpyHostToDevice, st));
     ICS_CUDA(cudaMemcpyAsync(dpt, p_tab, sizeof(double) * npk, cudaMemcpyHostToDevice, st));
-    ICS_FFT(cufftPlan3d(&r2c_n, n, n, n, CUFFT_R2C));
-    h1 = true;
-    ICS_FFT(cufftPlan3d(&c2r_n, n, n, n, CUFFT_C2R));
-    h2 = true;
-    ICS_FFT(cufftPlan3d(&r2c_e, ext, ext, ext, CUFFT_R2C));
-    h3 = true;
-    ICS_FFT(cufftPlan3d(&c2r_e, ext, ext, ext, CUFFT_C2R));
-    h4 = true;
+    ICS_FFT(cached_plan(device, n, CUFFT_R2C, &r2c_n));
+    ICS_FFT(cached_plan(device, n, CUFFT_C2R, &c2r_n));
+    ICS_FFT(cached_plan(device, ext, CUFFT_R2C, &r2c_e));
+    ICS_FFT(cached_plan(device, ext, CUFFT_C2R, &c2r_e));
     ICS_FFT(cufftSetStream(r2c_n, st));
     ICS_FFT(cufftSetStream(c2r_n, st));
     ICS_FFT(cufftSetStream(r2c_e, st));
@@ -264,10 +283,6 @@ extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const
     ICS_CUDA(cudaGetLastError());
     ICS_CUDA(cudaStreamSynchronize(st));
 done:
-    if (h1) cufftDestroy(r2c_n);
-    if (h2) cufftDestroy(c2r_n);
-    if (h3) cufftDestroy(r2c_e);
-    if (h4) cufftDestroy(c2r_e);
     for (void* q : {static_cast<void*>(phi), static_cast<void*>(spec), static_cast<void*>(espec),
                     static_cast<void*>(ediag), static_cast<void*>(emu), static_cast<void*>(eoff),
                     static_cast<void*>(f1), static_cast<void*>(dkt), static_cast<void*>(dpt)})
