@@ -29,6 +29,7 @@
 
 #include "common.h"
 #include "pm_kernels.cuh"
+#include "snapshot.h"
 
 using djb::fail;
 
@@ -2269,6 +2270,74 @@ int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wrap, doub
     }
     if (rc != DJB_OK) return rc;
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return check_err(s);
+}
+
+int djb_state_write_snapshot(djb_solver* s, const char* path, double D, double L, double p_div, double p_mul) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    if (!s->have_state) return fail(DJB_ERR_STATE, "no particle state set");
+    if (!path || !*path) return fail(DJB_ERR_INVALID, "snapshot path is empty");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    const size_t count = size_t(3 * s->np);
+    float* stage = nullptr;
+    TRY(scratch(s, 3, 2 * count, &stage));
+    djb::k_output<<<grid_for(count), kThreads, 0, s->stream>>>(s->psi, s->mom, s->q1, s->n, s->np, s->Lf, 0, p_div,
+                                                               p_mul, stage, stage + count);
+    if (cudaGetLastError() != cudaSuccess) return fail(DJB_ERR_CUDA, "output kernel launch failed");
+
+    // two pinned pieces: the copy of piece k+1 runs while piece k goes to the file
+    constexpr size_t kPiece = size_t(16) << 20;
+    float* host[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int rc = DJB_OK;
+    for (int i = 0; i < 2 && rc == DJB_OK; ++i) {
+        if (cudaHostAlloc(reinterpret_cast<void**>(&host[i]), kPiece * sizeof(float), cudaHostAllocDefault) !=
+                cudaSuccess ||
+            cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(DJB_ERR_ALLOC, "pinned snapshot buffers could not be allocated");
+        }
+    }
+    if (rc == DJB_OK) {
+        const uint64_t nn = uint64_t(s->n);
+        const std::vector<uint64_t> dims = {3, nn, nn, nn};
+        rc = djb::h5_write_arrays(
+            path, {{"Psi", dims, 4}, {"Pi", dims, 4}}, {{"D", D}, {"L", L}}, [&](size_t a, FILE* fp) -> int {
+                const float* src = stage + a * count;
+                const size_t pieces = (count + kPiece - 1) / kPiece;
+                auto issue = [&](size_t k) -> int {
+                    const size_t off = k * kPiece;
+                    const size_t len = std::min(kPiece, count - off);
+                    if (cudaMemcpyAsync(host[k & 1], src + off, len * sizeof(float), cudaMemcpyDeviceToHost,
+                                        s->stream) != cudaSuccess ||
+                        cudaEventRecord(ev[k & 1], s->stream) != cudaSuccess) {
+                        cudaGetLastError();
+                        return fail(DJB_ERR_CUDA, "snapshot copy failed");
+                    }
+                    return DJB_OK;
+                };
+                int r = issue(0);
+                for (size_t k = 0; k < pieces && r == DJB_OK; ++k) {
+                    if (k + 1 < pieces) r = issue(k + 1);
+                    if (r != DJB_OK) break;
+                    if (cudaEventSynchronize(ev[k & 1]) != cudaSuccess) {
+                        cudaGetLastError();
+                        r = fail(DJB_ERR_CUDA, "snapshot copy failed");
+                        break;
+                    }
+                    r = djb::h5_write_floats(fp, host[k & 1], std::min(kPiece, count - k * kPiece));
+                }
+                return r;
+            });
+    }
+    cudaError_t e = cudaStreamSynchronize(s->stream);   // no copy into the pinned pieces is left in flight
+    for (int i = 0; i < 2; ++i) {
+        if (host[i]) cudaFreeHost(host[i]);
+        if (ev[i]) cudaEventDestroy(ev[i]);
+    }
+    if (rc != DJB_OK) return rc;
+    if (e != cudaSuccess) return fail(DJB_ERR_CUDA, "%s", cudaGetErrorString(e));
     return check_err(s);
 }
 

@@ -20,6 +20,7 @@ DJB_ERR_CUFFT = 3
 DJB_ERR_ALLOC = 4
 DJB_ERR_STATE = 5
 DJB_ERR_DEVICE = 6
+DJB_ERR_IO = 7
 MEM_HOST = 0
 MEM_DEVICE = 1
 
@@ -80,6 +81,8 @@ SIGNATURES = {
     "djb_step": [_P, _D, _D, _D, _D],
     "djb_run": [_P, _I, _DP, _DP, _DP, _DP],
     "djb_get_output": [_P, _P, _P, _I, _D, _D, _I],
+    "djb_write_snapshot_h5": [C.c_char_p, _P, _P, _I, _D, _D],
+    "djb_state_write_snapshot": [_P, C.c_char_p, _D, _D, _D, _D],
     "djb_synchronize": [_P],
     "djb_solver_profile": [_P, _I],
     "djb_solver_profile_read": [_P, _DP, _I64P, _I64P, _I],

@@ -10,6 +10,7 @@ indexed [c,k,j,i] (`native_view`/`logical_view` convert).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -301,6 +302,14 @@ class PMSolver:
                                  C.c_void_p(po.ctypes.data) if p else None, int(wrap),
                                  float(p_div), float(p_mul), MEM_HOST))
         return xo, po
+
+    def write_snapshot(self, path, D: float, L: float, p_div: float = 1.0, p_mul: float = 1.0):
+        """HDF5 snapshot of the resident state: "Psi" (the displacement) and
+        "Pi" = Mom / p_div * p_mul, root attributes "D" and "L" (the study driver's
+        `snap_writer`, run_jobs.jl:41-48; the reference passes Pi = P / Fplus(a)).
+        Streams from HBM through pinned buffers (`djb_state_write_snapshot`)."""
+        check(lib.djb_state_write_snapshot(self._h, os.fsencode(path), float(D), float(L), float(p_div),
+                                           float(p_mul)))
 
     def state_density_modes(self, modes) -> np.ndarray:
         """Complex δ(m)/res³ / W_CIC(m) of the resident state at integer modes (k, 3)

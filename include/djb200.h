@@ -43,6 +43,7 @@ extern "C" {
 #define DJB_ERR_ALLOC 4     /* device or host allocation failed */
 #define DJB_ERR_STATE 5     /* call made in the wrong state (e.g. no particle state set) */
 #define DJB_ERR_DEVICE 6    /* a device-side check failed (error word set by a kernel) */
+#define DJB_ERR_IO 7        /* a file could not be written */
 
 #define DJB_MEM_HOST 0
 #define DJB_MEM_DEVICE 1
@@ -160,6 +161,21 @@ DJB_API int djb_run(djb_solver* s, int32_t n_steps, const double* ddrift1, const
  * Either pointer may be NULL. */
 DJB_API int djb_get_output(djb_solver* s, float* x_out, float* p_out, int32_t wrap, double p_div,
                    double p_mul, int32_t mem);
+/* Snapshot file of the study driver's snapshot writer
+ * (studies/eft_shell_crossing/scripts/run_jobs.jl:41-48, called at
+ * studies/eft_shell_crossing/src/runners.jl:154-156): HDF5 with the datasets "Psi" and "Pi"
+ * ((n,n,n,3) Float32 column-major; HDF5 dimensions (3,n,n,n)) and the float64 root
+ * attributes "D" and "L". The oldest HDF5 file format (superblock 0), readable by every
+ * HDF5 library. psi and pi are host arrays. DJB_ERR_IO when the file cannot be written
+ * (a partial file is removed). */
+DJB_API int djb_write_snapshot_h5(const char* path, const float* psi, const float* pi, int32_t n, double D,
+                                  double L);
+/* The same file from the resident state, Psi = the displacement and
+ * Pi = float((double(Mom) / p_div) * p_mul) as in djb_get_output (the reference passes
+ * Pi = P / Fplus(a), p_div = Fplus(a), p_mul = 1); the arrays stream from HBM through
+ * pinned host buffers in 64 MiB pieces, so no host copy of the state is made. */
+DJB_API int djb_state_write_snapshot(djb_solver* s, const char* path, double D, double L, double p_div,
+                                     double p_mul);
 /* Per-phase timing with CUDA events on the solver's stream (enable = 1) and launch
  * counts of this library's kernels. Phases: 0 mesh clear, 1 mass assignment,
  * 2 sheet resampling, 3 R2C, 4 k-space multiply, 5 C2R, 6 force interpolation
