@@ -24,16 +24,12 @@
 
 namespace djb {
 
-// Interpolation: particles kept per thread across the shifts, and the resident CTAs per
-// SM its registers are sized for (3 x 256 threads at <= 85 registers; the 26^3-node
-// PCS box of 76 KB lets 3 CTAs share an SM's shared memory).
-#ifndef DJB_BRICK_ROUNDS
-#define DJB_BRICK_ROUNDS 1
-#endif
+// Interpolation: the resident CTAs per SM its registers are sized for (3 x 256 threads at
+// <= 85 registers; the 28 x 26 x 26-node PCS box of 76 KB lets 3 CTAs share an SM's
+// shared memory).
 #ifndef DJB_BRICK_GATHER_BLOCKS
 #define DJB_BRICK_GATHER_BLOCKS 3
 #endif
-constexpr int kBrickRounds = DJB_BRICK_ROUNDS;
 
 struct BrickList {
     const unsigned* offset;  // block-local exclusive scan of the key counts
@@ -327,191 +323,16 @@ __device__ __forceinline__ void stage_box_wrapped(float* sbox, const float* __re
     asm volatile("cp.async.wait_all;\n" ::);
 }
 
-// `tma` != 0: the potentials are dense [res]^3 meshes (pitch == res) described by tm0/tm1
-// (box sx x S x S); boxes that do not wrap are then fetched with one bulk tensor copy.
+// Force interpolation of one brick's particles: FD gradient of the staged potential,
+// interpolation with the mass-assignment weights, mean over the interlacing shifts, then
+// the kick and drift. The shifts are the outer loop: the brick's box is staged once per
+// shift for all of its particles, and the sums over the shifts go through the
+// acceleration array (the last shift applies the mean, the correction and the
+// kick-drift). `tma` != 0: the potentials are dense [res]^3 meshes (pitch == res)
+// described by tm0/tm1 (box sx x S x S); boxes that do not wrap are then fetched with one
+// bulk tensor copy.
 template <int W, int R, int NS>
-__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gather_brick(GatherArgs A, BrickList bl,
-                                                                  const __grid_constant__ CUtensorMap tm0,
-                                                                  const __grid_constant__ CUtensorMap tm1, int tma) {
-    extern __shared__ __align__(128) float sbox[];
-    __shared__ __align__(8) uint64_t s_bar;
-    constexpr int E = W + 2 * R;
-    const int b = brick_of_block(bl, blockIdx.x);
-    unsigned start, cnt;
-    brick_range(bl, b, start, cnt);
-    if (cnt == 0) return;
-    const int tid = threadIdx.x;
-    const int n = A.n;
-    const int64_t np = A.np;
-    const int res = A.res;
-    const TileBox box = aligned_box(bl, b, bl.so, bl.sS, bl.sx);
-    const bool bulk = tma && box_inside(box, res) && (smem_u32(sbox) & 127u) == 0u;
-    const bool vec = ((A.pitch | res) & 3) == 0;
-    const unsigned box_bytes = unsigned(box.plane) * unsigned(box.S[2]) * 4u;
-    if (bulk && tid == 0) mbar_init(&s_bar, 1);
-    __syncthreads();
-    unsigned parity = 0;
-    const float resf = float(res);
-    const float cc[4] = {0.0f, A.c1, A.c2, A.c3};
-    LatticeDiv ld;
-    ld.init(n);
-    for (unsigned sr = 0; sr < cnt; sr += kTileThreads * kBrickRounds) {
-        // the particles of this super-round stay in registers across the shifts
-        int64_t pr[kBrickRounds];
-        float ps[kBrickRounds][3], acc[kBrickRounds][3];
-#pragma unroll
-        for (int r = 0; r < kBrickRounds; ++r) {
-            const unsigned slot = sr + r * kTileThreads + tid;
-            pr[r] = (slot < cnt) ? int64_t(bl.perm[start + slot]) : -1;
-            acc[r][0] = acc[r][1] = acc[r][2] = 0.0f;
-            ps[r][0] = ps[r][1] = ps[r][2] = 0.0f;
-            if (pr[r] >= 0) {
-                const int64_t p = pr[r];
-                ps[r][0] = A.psi[p];
-                ps[r][1] = A.psi[p + np];
-                ps[r][2] = A.psi[p + 2 * np];
-                if (!A.first) {
-                    acc[r][0] = A.acc[p];
-                    acc[r][1] = A.acc[p + np];
-                    acc[r][2] = A.acc[p + 2 * np];
-                }
-            }
-        }
-#pragma unroll 1
-        for (int g = 0; g < NS; ++g) {
-            const Shift3 sgs = (g == 0) ? A.sh.s[0] : A.sh.s[NS > 1 ? 1 : 0];
-            if (bulk) {
-                if (tid == 0) {
-                    fence_proxy_async_smem();  // the previous shift's reads precede the refill
-                    mbar_arrive_expect_tx(&s_bar, box_bytes);
-                    tma_load_3d(sbox, (g == 0) ? &tm0 : &tm1, box.o[0], box.o[1], box.o[2], &s_bar);
-                }
-                const bool ok = mbar_wait(&s_bar, parity);
-                parity ^= 1u;
-                if (__syncthreads_or(!ok)) {  // the copy never completed: report, do not spin
-                    if (tid == 0) atomicOr(A.err, 8);
-                    return;
-                }
-            } else {
-                stage_box_wrapped(sbox, (g == 0) ? A.mesh[0] : A.mesh[NS > 1 ? 1 : 0], box, res, A.pitch, vec);
-                __syncthreads();
-            }
-#pragma unroll 1
-            for (int r = 0; r < kBrickRounds; ++r) {
-                if (pr[r] < 0) continue;
-                int i, j, k;
-                ld.ijk(pr[r], i, j, k);
-                const float X[3] = {ps[r][0] + A.q1[i], ps[r][1] + A.q1[j], ps[r][2] + A.q1[k]};
-                float w[3][W], u[3][E];
-                int d[3];
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    const float s = (a == 0) ? sgs.x : (a == 1) ? sgs.y : sgs.z;
-                    const float gc = grid_coord(X[a] + s, A.L, resf, A.err);
-                    const int bb = wbase<W>(gc);
-#pragma unroll
-                    for (int o = 0; o < W; ++o) w[a][o] = wk<W>(fabsf(gc - float(bb + WLo<W>::v + o)));
-#pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        float sacc = 0.0f;
-#pragma unroll
-                        for (int o = 0; o < W; ++o) {
-                            const int t = e - R - o;
-                            if (t > 0 && t <= R) sacc -= w[a][o] * cc[t > 0 ? t : 0];
-                            if (t < 0 && -t <= R) sacc += w[a][o] * cc[t < 0 ? -t : 0];
-                        }
-                        u[a][e] = sacc;
-                    }
-                    d[a] = box_rel(bb + WLo<W>::v - R, box.o[a], res);
-                    if (d[a] < 0 || d[a] > box.S[a] - E) {  // not binned consistently: report, stay in bounds
-                        atomicOr(A.err, 2);
-                        d[a] = d[a] < 0 ? 0 : box.S[a] - E;
-                    }
-                }
-                float sX = 0.0f, sY = 0.0f, sZ = 0.0f;
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const float* pl = sbox + (d[2] + e) * box.plane + d[0];
-                    if (e >= R && e < R + W) {
-                        const int c = e - R;
-#pragma unroll
-                        for (int bb = 0; bb < W; ++bb) {
-                            const float* row = pl + (d[1] + R + bb) * box.P;
-                            float rx = 0.0f, rc = 0.0f;
-#pragma unroll
-                            for (int x = 0; x < E; ++x) {
-                                const float v = row[x];
-                                rx += u[0][x] * v;
-                                if (x >= R && x < R + W) rc += w[0][x - R] * v;
-                            }
-                            sX += (w[1][bb] * w[2][c]) * rx;
-                            sY += (u[1][bb + R] * w[2][c]) * rc;
-                            sZ += (u[2][e] * w[1][bb]) * rc;
-                        }
-#pragma unroll
-                        for (int h = 0; h < 2 * R; ++h) {
-                            const int ey = (h < R) ? h : h + W;
-                            const float* row = pl + (d[1] + ey) * box.P + R;
-                            float rc = 0.0f;
-#pragma unroll
-                            for (int a = 0; a < W; ++a) rc += w[0][a] * row[a];
-                            sY += (u[1][ey] * w[2][c]) * rc;
-                        }
-                    } else {
-#pragma unroll
-                        for (int bb = 0; bb < W; ++bb) {
-                            const float* row = pl + (d[1] + R + bb) * box.P + R;
-                            float rc = 0.0f;
-#pragma unroll
-                            for (int a = 0; a < W; ++a) rc += w[0][a] * row[a];
-                            sZ += (u[2][e] * w[1][bb]) * rc;
-                        }
-                    }
-                }
-                acc[r][0] += sX;
-                acc[r][1] += sY;
-                acc[r][2] += sZ;
-            }
-            __syncthreads();
-        }
-#pragma unroll
-        for (int r = 0; r < kBrickRounds; ++r) {
-            if (pr[r] < 0) continue;
-            const int64_t p = pr[r];
-            float a3[3] = {acc[r][0], acc[r][1], acc[r][2]};
-            if (A.last && A.divide) {
-                a3[0] = a3[0] / A.nshift_f;
-                a3[1] = a3[1] / A.nshift_f;
-                a3[2] = a3[2] / A.nshift_f;
-            }
-            if (A.last && A.extra) {
-                a3[0] += A.extra[p];
-                a3[1] += A.extra[p + np];
-                a3[2] += A.extra[p + 2 * np];
-            }
-            if (A.last && A.step) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const float m = A.alpha * A.mom[p + c * np] + A.beta * a3[c];
-                    A.mom[p + c * np] = m;
-                    A.psi[p + c * np] = ps[r][c] + A.dd2 * m;
-                }
-            } else {
-                A.acc[p] = a3[0];
-                A.acc[p + np] = a3[1];
-                A.acc[p + 2 * np] = a3[2];
-            }
-        }
-    }
-}
-
-// The same interpolation with the shifts in the outer loop: the brick's box is staged once
-// per shift for all of its particles (the form above re-stages it for every round of 256
-// particles, since it keeps a round's particles in registers across the shifts). The sums
-// over the shifts go through the acceleration array; the last shift applies the mean, the
-// correction and the kick-drift.
-template <int W, int R, int NS>
-__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gather_brick_so(
+__global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gather_brick(
     GatherArgs A, BrickList bl, const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
     int tma) {
     extern __shared__ __align__(128) float sbox[];

@@ -887,7 +887,6 @@ struct djb_solver {
     int* err = nullptr;
     bool have_state = false;
     bool tiled = true;  // shared-memory tiled scatter/gather (DJB_KERNELS=simple selects the per-particle ones)
-    bool shift_outer = true;  // brick interpolation with the shifts in the outer loop (DJB_GATHER_SO=0: rounds outer)
     // force correction (djb_solver_attach_nn): network inputs [δ, F_x, F_y, F_z] scaled by
     // nn_in (δ) and nn_fin (F), its output scaled by nn_out, interpolated to the particles
     djb_nn* nn = nullptr;
@@ -1145,20 +1144,12 @@ void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
         const size_t smem = gather_smem(s);
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const int tma = (s->tma && a.mesh[0] == s->phi[0]) ? 1 : 0;
-        if (s->shift_outer) {
-            if (ns == 1)
-                djb::k_gather_brick_so<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
-                    a, brick_list(s), s->tmap[0], s->tmap[0], tma);
-            else
-                djb::k_gather_brick_so<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
-                    a, brick_list(s), s->tmap[0], s->tmap[1], tma);
-        } else if (ns == 1) {
+        if (ns == 1)
             djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 a, brick_list(s), s->tmap[0], s->tmap[0], tma);
-        } else {
+        else
             djb::k_gather_brick<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 a, brick_list(s), s->tmap[0], s->tmap[1], tma);
-        }
         return;
     }
     if (R > 0 && s->tiled) {
@@ -1189,14 +1180,6 @@ int tiled_attrs_wr() {
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   int(cudaSharedmemCarveoutMaxShared)));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick<W, R, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  int(cudaSharedmemCarveoutMaxShared)));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_so<W, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kBrickSmemMax));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_so<W, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kBrickSmemMax));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_so<W, R, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  int(cudaSharedmemCarveoutMaxShared)));
-    CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_brick_so<W, R, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   int(cudaSharedmemCarveoutMaxShared)));
     return DJB_OK;
 }
@@ -1681,10 +1664,6 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         s->tiled = !(kind && std::strcmp(kind, "simple") == 0);
     }
     if (s->tiled) TRY(tiled_attrs(s->W, s->R));
-    {
-        const char* so = std::getenv("DJB_GATHER_SO");
-        s->shift_outer = !(so && std::strcmp(so, "0") == 0);
-    }
     {
         const char* srt = std::getenv("DJB_SORT");
         s->sorted = s->tiled && !(srt && std::strcmp(srt, "0") == 0);
