@@ -142,16 +142,14 @@ __global__ void __launch_bounds__(256) k_scatter_weighted(const float* __restric
         }
 }
 
-// Both stencil kernels sweep a column of kFdTX × kFdTY cells along z over kFdZ planes:
-// the z stencil from a register window of 2·kFdR + 1 values of the thread's own column,
-// the x and y stencils from the plane's tile with its halo, staged in shared memory.
-#ifndef DJB_FD_TY
-#define DJB_FD_TY 8
-#endif
-#ifndef DJB_FD_Z
-#define DJB_FD_Z 32
-#endif
-constexpr int kFdTX = 32, kFdTY = DJB_FD_TY, kFdZ = DJB_FD_Z, kFdR = 3;
+// Both stencil kernels sweep a column of kFdTX × kFdTY cells along z over kFdZ planes,
+// 256 threads with two rows each. The planes come into shared memory by asynchronous
+// copies (16 bytes where the row pitch and the mesh width allow it, else 4 bytes),
+// four planes ahead of the plane being computed, so the loads of later planes overlap
+// the arithmetic of this one; the z stencil reads a ring of staged planes.
+constexpr int kFdTX = 32, kFdTY = 16, kFdZ = 64, kFdR = 3;
+constexpr int kFdThreads = 256;
+constexpr int kFdRing = 8;   // planes z − 3 .. z + 3 and the one in flight
 
 // Periodic index of any integer (tiles and windows reach past 2·res on small meshes);
 // indices inside the mesh, the common case, take one unsigned comparison.
@@ -161,95 +159,134 @@ __device__ __forceinline__ int fd_wrap(int v, int res) {
     return v < 0 ? v + res : v;
 }
 
-__device__ __forceinline__ float fd_at(const float* __restrict__ f, int x, int y, int z, int res, int pitch) {
-    return f[(int64_t(fd_wrap(z, res)) * res + fd_wrap(y, res)) * pitch + fd_wrap(x, res)];
-}
-
-// Tile of plane z: rows y0 − hy .. y0 + kFdTY − 1 + hy, columns x0 − hx .. x0 + kFdTX − 1 + hx.
-__device__ __forceinline__ void fd_stage(float* t, const float* __restrict__ f, int x0, int y0, int z, int hx, int hy,
-                                         int res, int pitch) {
-    const int w = kFdTX + 2 * hx, h = kFdTY + 2 * hy;
-    for (int i = threadIdx.x; i < w * h; i += blockDim.x) {
-        const int r = i / w, c = i - r * w;
-        t[i] = fd_at(f, x0 - hx + c, y0 - hy + r, z, res, pitch);
+// Copies rows ys .. ys + rows − 1, columns xs .. xs + NCOL − 1 of plane z (periodic) into
+// t[rows][NCOL]. vec: xs, res and pitch are multiples of 4 and f is 16-byte aligned.
+template <int NCOL>
+__device__ __forceinline__ void fd_issue(float* t, const float* __restrict__ f, int xs, int ys, int rows, int z,
+                                         int res, int pitch, bool vec) {
+    const int64_t pz = int64_t(fd_wrap(z, res)) * res;
+    if (vec) {
+        constexpr int N4 = NCOL / 4;
+        for (int i = threadIdx.x; i < rows * N4; i += kFdThreads) {
+            const int r = i / N4, c = i - r * N4;
+            const float* src = f + (pz + fd_wrap(ys + r, res)) * pitch + fd_wrap(xs + 4 * c, res);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(t + r * NCOL + 4 * c)), "l"(src)
+                         : "memory");
+        }
+    } else {
+        for (int i = threadIdx.x; i < rows * NCOL; i += kFdThreads) {
+            const int r = i / NCOL, c = i - r * NCOL;
+            const float* src = f + (pz + fd_wrap(ys + r, res)) * pitch + fd_wrap(xs + c, res);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(t + r * NCOL + c)), "l"(src)
+                         : "memory");
+        }
     }
 }
+__device__ __forceinline__ void fd_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most one copy group of this thread is still in flight.
+__device__ __forceinline__ void fd_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ int fd_slot(int z, int z0) { return (z - z0 + kFdR) & (kFdRing - 1); }
 
 // g_c = −D_c φ, (D_c f)(n) = Σ_t c_t (f(n + t e_c) − f(n − t e_c)) (pm.jl:330-342).
-__global__ void __launch_bounds__(kFdTX * kFdTY) k_fd_grad3(const float* __restrict__ phi, int res, int pitch,
-                                                             float c1, float c2, float c3, float* __restrict__ g0,
-                                                             float* __restrict__ g1, float* __restrict__ g2) {
-    __shared__ float tile[(kFdTY + 2 * kFdR) * (kFdTX + 2 * kFdR)];
+// Staged planes: rows y0 − 3 .. y0 + 18, columns x0 − 4 .. x0 + 35.
+__global__ void __launch_bounds__(kFdThreads) k_fd_grad3(const float* __restrict__ phi, int res, int pitch, float c1,
+                                                          float c2, float c3, float* __restrict__ g0,
+                                                          float* __restrict__ g1, float* __restrict__ g2, int vec) {
+    constexpr int NC = kFdTX + 8, NR = kFdTY + 2 * kFdR;
+    __shared__ __align__(16) float ring[kFdRing][NR * NC];
     const float cc[kFdR] = {c1, c2, c3};
     const int tx = threadIdx.x % kFdTX, ty = threadIdx.x / kFdTX;
     const int x0 = blockIdx.x * kFdTX, y0 = blockIdx.y * kFdTY, z0 = blockIdx.z * kFdZ;
-    const int x = x0 + tx, y = y0 + ty;
     const int z1 = min(z0 + kFdZ, res);
-    float win[2 * kFdR + 1];   // φ(x, y, z − R .. z + R)
-#pragma unroll
-    for (int k = 0; k < 2 * kFdR; ++k) win[k + 1] = fd_at(phi, x, y, z0 - kFdR + k, res, pitch);
-    constexpr int W2 = kFdTX + 2 * kFdR;
+    const int x = x0 + tx;
+    for (int z = z0 - kFdR; z <= z0 + kFdR; ++z) {   // one copy group per plane
+        fd_issue<NC>(ring[fd_slot(z, z0)], phi, x0 - 4, y0 - kFdR, NR, z, res, pitch, vec != 0);
+        fd_commit();
+    }
     for (int z = z0; z < z1; ++z) {
-#pragma unroll
-        for (int k = 0; k < 2 * kFdR; ++k) win[k] = win[k + 1];
-        win[2 * kFdR] = fd_at(phi, x, y, z + kFdR, res, pitch);
+        if (z + 1 < z1) fd_issue<NC>(ring[fd_slot(z + kFdR + 1, z0)], phi, x0 - 4, y0 - kFdR, NR, z + kFdR + 1, res,
+                                     pitch, vec != 0);
+        fd_commit();
+        fd_wait1();   // planes up to z + 3 have landed
         __syncthreads();
-        fd_stage(tile, phi, x0, y0, z, kFdR, kFdR, res, pitch);
-        __syncthreads();
-        if (x < res && y < res) {
-            const float* c0 = tile + (ty + kFdR) * W2 + tx + kFdR;
-            float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
+        const float* pc = ring[fd_slot(z, z0)];
 #pragma unroll
-            for (int k = 0; k < kFdR; ++k) {
-                const int t = k + 1;
-                d0 += cc[k] * (c0[t] - c0[-t]);
-                d1 += cc[k] * (c0[t * W2] - c0[-t * W2]);
-                d2 += cc[k] * (win[kFdR + t] - win[kFdR - t]);
+        for (int h = 0; h < 2; ++h) {
+            const int yy = ty + 8 * h, y = y0 + yy;
+            if (x < res && y < res) {
+                const int off = (yy + kFdR) * NC + tx + 4;
+                const float* c0 = pc + off;
+                float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
+#pragma unroll
+                for (int k = 0; k < kFdR; ++k) {
+                    const int t = k + 1;
+                    d0 += cc[k] * (c0[t] - c0[-t]);
+                    d1 += cc[k] * (c0[t * NC] - c0[-t * NC]);
+                    d2 += cc[k] * (ring[fd_slot(z + t, z0)][off] - ring[fd_slot(z - t, z0)][off]);
+                }
+                const int64_t o = (int64_t(z) * res + y) * pitch + x;
+                g0[o] = -d0;
+                g1[o] = -d1;
+                g2[o] = -d2;
             }
-            const int64_t o = (int64_t(z) * res + y) * pitch + x;
-            g0[o] = -d0;
-            g1[o] = -d1;
-            g2[o] = -d2;
         }
+        __syncthreads();   // the slot of plane z − 3 is refilled next
     }
 }
 
-// out = Σ_c D_c g_c.
-__global__ void __launch_bounds__(kFdTX * kFdTY) k_fd_div3(const float* __restrict__ g0, const float* __restrict__ g1,
-                                                            const float* __restrict__ g2, int res, int pitch, float c1,
-                                                            float c2, float c3, float* __restrict__ out) {
-    __shared__ float tx_tile[kFdTY * (kFdTX + 2 * kFdR)];     // g0 with its x halo
-    __shared__ float ty_tile[(kFdTY + 2 * kFdR) * kFdTX];     // g1 with its y halo
+// out = Σ_c D_c g_c. Staged: g0 rows y0 .. y0 + 15 with columns x0 − 4 .. x0 + 35 and g1
+// rows y0 − 3 .. y0 + 18 with columns x0 .. x0 + 31 (plane z and z + 1), g2 rows
+// y0 .. y0 + 15, columns x0 .. x0 + 31 in the ring of planes.
+__global__ void __launch_bounds__(kFdThreads) k_fd_div3(const float* __restrict__ g0, const float* __restrict__ g1,
+                                                         const float* __restrict__ g2, int res, int pitch, float c1,
+                                                         float c2, float c3, float* __restrict__ out, int vec) {
+    constexpr int NX = kFdTX + 8, NY = kFdTY + 2 * kFdR;
+    __shared__ __align__(16) float ring[kFdRing][kFdTY * kFdTX];
+    __shared__ __align__(16) float tx_tile[2][kFdTY * NX];
+    __shared__ __align__(16) float ty_tile[2][NY * kFdTX];
     const float cc[kFdR] = {c1, c2, c3};
     const int tx = threadIdx.x % kFdTX, ty = threadIdx.x / kFdTX;
     const int x0 = blockIdx.x * kFdTX, y0 = blockIdx.y * kFdTY, z0 = blockIdx.z * kFdZ;
-    const int x = x0 + tx, y = y0 + ty;
     const int z1 = min(z0 + kFdZ, res);
-    float win[2 * kFdR + 1];   // g2(x, y, z − R .. z + R)
-#pragma unroll
-    for (int k = 0; k < 2 * kFdR; ++k) win[k + 1] = fd_at(g2, x, y, z0 - kFdR + k, res, pitch);
-    constexpr int WX = kFdTX + 2 * kFdR;
-    for (int z = z0; z < z1; ++z) {
-#pragma unroll
-        for (int k = 0; k < 2 * kFdR; ++k) win[k] = win[k + 1];
-        win[2 * kFdR] = fd_at(g2, x, y, z + kFdR, res, pitch);
-        __syncthreads();
-        fd_stage(tx_tile, g0, x0, y0, z, kFdR, 0, res, pitch);
-        fd_stage(ty_tile, g1, x0, y0, z, 0, kFdR, res, pitch);
-        __syncthreads();
-        if (x < res && y < res) {
-            const float* a0 = tx_tile + ty * WX + tx + kFdR;
-            const float* a1 = ty_tile + (ty + kFdR) * kFdTX + tx;
-            float d = 0.0f;
-#pragma unroll
-            for (int k = 0; k < kFdR; ++k) {
-                const int t = k + 1;
-                d += cc[k] * (a0[t] - a0[-t]);
-                d += cc[k] * (a1[t * kFdTX] - a1[-t * kFdTX]);
-                d += cc[k] * (win[kFdR + t] - win[kFdR - t]);
-            }
-            out[(int64_t(z) * res + y) * pitch + x] = d;
+    const int x = x0 + tx;
+    const bool v4 = vec != 0;
+    for (int z = z0 - kFdR; z <= z0 + kFdR; ++z) {
+        fd_issue<kFdTX>(ring[fd_slot(z, z0)], g2, x0, y0, kFdTY, z, res, pitch, v4);
+        if (z == z0) {
+            fd_issue<NX>(tx_tile[0], g0, x0 - 4, y0, kFdTY, z0, res, pitch, v4);
+            fd_issue<kFdTX>(ty_tile[0], g1, x0, y0 - kFdR, NY, z0, res, pitch, v4);
         }
+        fd_commit();
+    }
+    for (int z = z0; z < z1; ++z) {
+        const int b = (z - z0) & 1;
+        if (z + 1 < z1) {
+            fd_issue<kFdTX>(ring[fd_slot(z + kFdR + 1, z0)], g2, x0, y0, kFdTY, z + kFdR + 1, res, pitch, v4);
+            fd_issue<NX>(tx_tile[b ^ 1], g0, x0 - 4, y0, kFdTY, z + 1, res, pitch, v4);
+            fd_issue<kFdTX>(ty_tile[b ^ 1], g1, x0, y0 - kFdR, NY, z + 1, res, pitch, v4);
+        }
+        fd_commit();
+        fd_wait1();   // g2 up to plane z + 3, g0 and g1 of plane z have landed
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int yy = ty + 8 * h, y = y0 + yy;
+            if (x < res && y < res) {
+                const float* a0 = tx_tile[b] + yy * NX + tx + 4;
+                const float* a1 = ty_tile[b] + (yy + kFdR) * kFdTX + tx;
+                const int zc = yy * kFdTX + tx;
+                float d = 0.0f;
+#pragma unroll
+                for (int k = 0; k < kFdR; ++k) {
+                    const int t = k + 1;
+                    d += cc[k] * (a0[t] - a0[-t]);
+                    d += cc[k] * (a1[t * kFdTX] - a1[-t * kFdTX]);
+                    d += cc[k] * (ring[fd_slot(z + t, z0)][zc] - ring[fd_slot(z - t, z0)][zc]);
+                }
+                out[(int64_t(z) * res + y) * pitch + x] = d;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -297,7 +334,8 @@ __global__ void k_mesh_affine(const float* __restrict__ in, int res, int pitch, 
 // with error bit 2 when the binning and this evaluation disagree).
 // p: the particle (its lattice site); io: where its Ψ lives in `psi` (p, or its slot in
 // brick order when the arrays were gathered into that order).
-template <int W>
+// DW = false: the weights only (dw is left unset).
+template <int W, bool DW = true>
 __device__ __forceinline__ void brick_stencil(const float* __restrict__ psi, const float* __restrict__ q1,
                                               const LatticeDiv& ld, int64_t np, int64_t p, int64_t io, float L,
                                               float resf, int res, const float sh[3], const TileBox& box, int* err,
@@ -314,7 +352,7 @@ __device__ __forceinline__ void brick_stencil(const float* __restrict__ psi, con
         for (int o = 0; o < W; ++o) {
             const float dd = g - float(bb + WLo<W>::v + o);
             w[a][o] = wk<W>(fabsf(dd));
-            dw[a][o] = dwk<W>(dd) * dgdx;
+            if constexpr (DW) dw[a][o] = dwk<W>(dd) * dgdx;
         }
         d[a] = box_rel(bb + WLo<W>::v, box.o[a], res);
         if (d[a] < 0 || d[a] > box.S[a] - W) {
@@ -390,7 +428,8 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
             const float av = scale * abar[io + comp * np] * up;
             float w[3][W], dw[3][W];
             int d[3];
-            brick_stencil<W>(psi, q1, ld, np, p, io, L, resf, res, sh, box, comp == 0 ? err : nullptr, w, dw, d);
+            brick_stencil<W, false>(psi, q1, ld, np, p, io, L, resf, res, sh, box, comp == 0 ? err : nullptr, w, dw,
+                                    d);
 #pragma unroll
             for (int c = 0; c < W; ++c)
 #pragma unroll
@@ -460,20 +499,29 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gath
             int d[3];
             brick_stencil<W>(psi, q1, ld, np, p, io, L, resf, res, sh, box, f == 0 ? err : nullptr, w, dw, d);
             const float af = scale * (f1 ? abar[io + f * np] : 1.0f);
+            // separable sums: rows along x (∂_x W and W), then y, then z
             float v[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-            for (int c = 0; c < W; ++c)
+            for (int c = 0; c < W; ++c) {
+                float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
 #pragma unroll
                 for (int bb = 0; bb < W; ++bb) {
                     const float* row = fbox + ((d[2] + c) * box.S[1] + d[1] + bb) * box.P + d[0];
+                    float r0 = 0.0f, r1 = 0.0f;
 #pragma unroll
                     for (int a = 0; a < W; ++a) {
                         const float fv = row[a];
-                        v[0] += dw[0][a] * w[1][bb] * w[2][c] * fv;
-                        v[1] += w[0][a] * dw[1][bb] * w[2][c] * fv;
-                        v[2] += w[0][a] * w[1][bb] * dw[2][c] * fv;
+                        r0 += dw[0][a] * fv;
+                        r1 += w[0][a] * fv;
                     }
+                    s0 += w[1][bb] * r0;
+                    s1 += dw[1][bb] * r1;
+                    s2 += w[1][bb] * r1;
                 }
+                v[0] += w[2][c] * s0;
+                v[1] += w[2][c] * s1;
+                v[2] += dw[2][c] * s2;
+            }
 #pragma unroll
             for (int a = 0; a < 3; ++a) psibar[io + a * np] += af * v[a];
         }

@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <new>
 #include <string>
 #include <vector>
@@ -875,6 +876,8 @@ struct djb_solver {
     float2* phase = nullptr;    // px, py, pz tables (n + n + n/2+1)
     // brick sort of the particles (sort.cuh)
     bool sorted = true;
+    bool zp4 = false;        // z pass with 4 pencils per CTA (DJB_ZPASS_P=4)
+    bool fd_scalar = false;  // stencil kernels with 4-byte copies only (DJB_FD_SCALAR=1; the 16-byte path is the default)
     djb::SortGeom sg{};
     int64_t nbins = 0;
     int nscan = 0;
@@ -1282,7 +1285,11 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
 void launch_zpass(djb_solver* s, float* mesh, int nh) {
     const dim3 grid(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res));
     const djb::KPhiFn kp{s->lapT, s->makT, s->s0};
-    if (DJB_ZPASS_PAIR)
+    if (DJB_ZPASS_PAIR && s->zp4) {
+        const dim3 grid4(unsigned((nh + 3) / 4), unsigned(s->res));
+        djb::k_zpencil_pair<djb::KPhiFn, 4><<<grid4, 4 * 64, 4 * djb::kZPlane * 8, s->stream>>>(
+            reinterpret_cast<float2*>(mesh), nh, s->wN, kp);
+    } else if (DJB_ZPASS_PAIR)
         djb::k_zpencil_pair<<<grid, djb::kZPairThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh,
                                                                                   s->wN, kp);
     else
@@ -1305,6 +1312,7 @@ int sort_particles(djb_solver* s, const float* mom, float dd1) {
 }
 
 dim3 fd_grid(int res);
+int fd_vec(const djb_solver* s, int res, int pitch, std::initializer_list<const void*> meshes);
 int nn_correction(djb_solver* s);
 
 int force(djb_solver* s, bool step, double dd1, double alpha, double beta, double dd2) {
@@ -1387,9 +1395,10 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
                 // the interpolation of its output to the particles
                 const int64_t cells = int64_t(s->res) * s->res * s->res;
                 s->prof.begin(s->stream, PH_NN);
-                djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(
+                djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdThreads, 0, s->stream>>>(
                     s->phi[0], s->res, s->res, s->c1 * s->nn_fin, s->c2 * s->nn_fin, s->c3 * s->nn_fin,
-                    s->nnf + cells, s->nnf + 2 * cells, s->nnf + 3 * cells);
+                    s->nnf + cells, s->nnf + 2 * cells, s->nnf + 3 * cells,
+                    fd_vec(s, s->res, s->res, {s->phi[0], s->nnf + cells, s->nnf + 2 * cells, s->nnf + 3 * cells}));
                 TRY(nn_correction(s));
                 s->prof.end(s->stream, PH_NN, 3);
             }
@@ -1457,6 +1466,15 @@ int poisson(djb_solver* s, int m) {
 dim3 fd_grid(int res) {
     return dim3(unsigned((res + djb::kFdTX - 1) / djb::kFdTX), unsigned((res + djb::kFdTY - 1) / djb::kFdTY),
                 unsigned((res + djb::kFdZ - 1) / djb::kFdZ));
+}
+
+// 1 when the stencil kernels may stage with 16-byte copies: rows and the mesh width are
+// multiples of 4 floats and every mesh is 16-byte aligned.
+int fd_vec(const djb_solver* s, int res, int pitch, std::initializer_list<const void*> meshes) {
+    if (s->fd_scalar || (res & 3) || (pitch & 3)) return 0;
+    for (const void* m : meshes)
+        if (reinterpret_cast<uintptr_t>(m) & 15u) return 0;
+    return 1;
 }
 
 // The attached network on its scaled inputs in s->nnf (filled by the force pipeline),
@@ -1583,13 +1601,15 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
                 psi, nullptr, 0.0f, s->q1, s->n, s->np, s->Lf, s->res, pitch, g, rho, nullptr, s->err);
         }
         TRY(poisson(s, 0));  // φ
-        djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(rho, s->res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
-                                                    s->adj[2]);
+        djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdThreads, 0, s->stream>>>(
+            rho, s->res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1], s->adj[2],
+            fd_vec(s, s->res, pitch, {rho, s->adj[0], s->adj[1], s->adj[2]}));
         vjp_kernels(s, 0, kpsi, kabar, kpb, sh, inv_ns, perm);  // interpolation weights
         for (int c = 0; c < 3; ++c) CUDA_TRY(cudaMemsetAsync(s->adj[c], 0, rho_floats * sizeof(float), s->stream));
         vjp_kernels(s, 1, kpsi, kabar, kpb, sh, inv_ns, perm);  // Ḡ
-        djb::k_fd_div3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(s->adj[0], s->adj[1], s->adj[2], s->res, pitch, s->c1, s->c2,
-                                                   s->c3, rho);  // φ̄
+        djb::k_fd_div3<<<fd_grid(s->res), djb::kFdThreads, 0, s->stream>>>(
+            s->adj[0], s->adj[1], s->adj[2], s->res, pitch, s->c1, s->c2, s->c3, rho,
+            fd_vec(s, s->res, pitch, {rho, s->adj[0], s->adj[1], s->adj[2]}));  // φ̄
         TRY(poisson(s, 0));                                    // ρ̄
         vjp_kernels(s, 2, kpsi, kabar, kpb, sh, 1.0f, perm);  // deposit weights
     }
@@ -1664,6 +1684,14 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         s->tiled = !(kind && std::strcmp(kind, "simple") == 0);
     }
     if (s->tiled) TRY(tiled_attrs(s->W, s->R));
+    {
+        const char* zp = std::getenv("DJB_ZPASS_P");
+        s->zp4 = zp && std::strcmp(zp, "4") == 0;
+    }
+    {
+        const char* fs = std::getenv("DJB_FD_SCALAR");
+        s->fd_scalar = fs && std::strcmp(fs, "1") == 0;
+    }
     {
         const char* srt = std::getenv("DJB_SORT");
         s->sorted = s->tiled && !(srt && std::strcmp(srt, "0") == 0);
@@ -1819,6 +1847,8 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
             CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
+            CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn, 4>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * djb::kZPlane * 8));
         }
         if (s->sorted && s->gsx <= res) {
             for (int m = 0; m < s->group; ++m) {
@@ -2028,8 +2058,9 @@ int djb_mesh_fields(djb_solver* s, const float* psi, float* out, int32_t mem) {
         djb::k_mesh_affine<<<cb, 256, 0, s->stream>>>(rho, res, pitch, f, 1.0f, o);  // δ
         rc = poisson(s, 0);
         if (rc == DJB_OK) {
-            djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdTX * djb::kFdTY, 0, s->stream>>>(rho, res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1],
-                                                        s->adj[2]);
+            djb::k_fd_grad3<<<fd_grid(s->res), djb::kFdThreads, 0, s->stream>>>(
+                rho, res, pitch, s->c1, s->c2, s->c3, s->adj[0], s->adj[1], s->adj[2],
+                fd_vec(s, res, pitch, {rho, s->adj[0], s->adj[1], s->adj[2]}));
             for (int c = 0; c < 3; ++c)
                 djb::k_mesh_affine<<<cb, 256, 0, s->stream>>>(s->adj[c], res, pitch, 1.0f, 0.0f, o + (c + 1) * cells);
             if (cudaGetLastError() != cudaSuccess) rc = fail(DJB_ERR_CUDA, "mesh field kernels failed");

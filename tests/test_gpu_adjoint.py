@@ -59,6 +59,27 @@ def test_force_vjp_device_arrays_and_ik_rejected(djb):
             S.acceleration_vjp(psi, abar)
 
 
+def test_stencils_16_byte_staging_at_1024_mesh(djb, monkeypatch):
+    """On the dense 1024³ meshes the FD stencil kernels (network inputs, VJP) stage
+    their planes with 16-byte copies; the 4-byte path (DJB_FD_SCALAR=1, the one the
+    padded meshes of the oracle comparisons take) must give the same fields."""
+    n, res, L = 32, 1024, 1000.0
+    psi = _clustered(n, L, 5, amp=8.0)
+    abar = np.random.default_rng(4).standard_normal((n, n, n, 3)).astype(np.float32)
+    cfg = djb.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=4, grad_order=6, antialias=1)
+    out = {}
+    for scalar in ("0", "1"):
+        monkeypatch.setenv("DJB_FD_SCALAR", scalar)
+        with djb.PMSolver(cfg) as S:
+            f = S.mesh_fields(psi)
+            out[scalar] = (f[1:].copy(), S.acceleration_vjp(psi, abar))
+        del f
+    (f16, g16), (f4, g4) = out["0"], out["1"]
+    assert np.isfinite(f16).all() and np.abs(f16).max() > 0
+    assert rel(f16, f4) < 1e-5        # float atomics of the deposit reorder only
+    assert rel(g16, g4) < 1e-5
+
+
 def test_step_vjp_vs_oracle(djb):
     from oracle import adjoint as oad
     from oracle import pm as opm
