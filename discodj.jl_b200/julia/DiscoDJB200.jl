@@ -285,4 +285,15 @@ attach_nn!(S::PMSolverB200, ::Nothing) =
     _check(ccall((:djb_solver_attach_nn, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Float64, Float64, Float64),
                  S.handle, C_NULL, 1.0, 1.0, 1.0))
 
+"""
+    write_snapshot_b200(S, path, D, L; p_div=1.0, p_mul=1.0)
+
+The study driver's snapshot file (scripts/run_jobs.jl:41-48) from the resident state:
+HDF5 "Psi", "Pi" = Mom / p_div · p_mul and root attributes "D", "L"
+(djb_state_write_snapshot; pass p_div = Fplus(c, a) as runners.jl:155 divides P).
+"""
+write_snapshot_b200(S::PMSolverB200, path::AbstractString, D::Real, L::Real; p_div::Real=1.0, p_mul::Real=1.0) =
+    _check(ccall((:djb_state_write_snapshot, LIB), Cint, (Ptr{Cvoid}, Cstring, Float64, Float64, Float64, Float64),
+                 S.handle, path, D, L, p_div, p_mul))
+
 end # module
