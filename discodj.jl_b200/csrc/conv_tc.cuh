@@ -58,6 +58,10 @@ constexpr int kAccTiles = 16;                          // tile accumulators in t
 constexpr int kMaxSegment = kAccTiles;                 // z segment length (tiles) at most
 constexpr int kOneCtaSmem = 116 * 1024;                // more than half an SM: one CTA per SM
 constexpr int kEpiGroups = 2;                          // epilogue groups of four warps, alternate tiles
+#ifndef DJB_CONV_OSTAGES
+#define DJB_CONV_OSTAGES 4
+#endif
+constexpr int kOutStages = DJB_CONV_OSTAGES;           // output staging buffers per epilogue group
 constexpr int kLoaderWarp = 4 * kEpiGroups, kMmaWarp = kLoaderWarp + 1;
 constexpr int kThreads = 32 * (kMmaWarp + 1);
 
@@ -90,7 +94,7 @@ __host__ __device__ constexpr uint32_t slot_bytes() {
 template <int KC, int N, bool PAIR = false>
 constexpr int smem_bytes() {
     const int w = PAIR ? 3 * 2 * 3 * N * 16 : 27 * KC * N * 16;
-    const int stage = kEpiGroups * 2 * 128 * N * 2;   // output staging: two tiles per epilogue group
+    const int stage = kEpiGroups * kOutStages * 128 * N * 2;   // output staging per epilogue group
     const int b = w + kRing * int(slot_bytes<KC>()) + stage + (2 * kRing + (kEpiGroups + 1) * kAccTiles + 1) * 8 + 16;
     return b < kOneCtaSmem ? kOneCtaSmem : b;   // the CTA's tensor memory may be all 512 columns
 }
@@ -205,8 +209,10 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int
                  : "memory");
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
-// Waits until at most one of this thread's bulk groups still reads shared memory.
-__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+// Waits until at most kOutStages − 1 of this thread's bulk groups still read shared memory.
+__device__ __forceinline__ void bulk_wait_read_stages() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(kOutStages - 1) : "memory");
+}
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // Barrier `id` of the 128 threads of one epilogue group; returns whether any passed true.
 __device__ __forceinline__ bool group_bar_or(int id, bool v) {
@@ -272,8 +278,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* ws = smem;
     uint8_t* ringp = smem + NSH * KW * 3 * N * 16;
-    uint8_t* ostage = ringp + kRing * kSlot;                     // [group][2][128 rows][N bf16]
-    uint64_t* full = reinterpret_cast<uint64_t*>(ostage + kEpiGroups * 2 * 128 * N * 2);
+    uint8_t* ostage = ringp + kRing * kSlot;                     // [group][kOutStages][128 rows][N bf16]
+    uint64_t* full = reinterpret_cast<uint64_t*>(ostage + kEpiGroups * kOutStages * 128 * N * 2);
     uint64_t* empty = full + kRing;
     uint64_t* accf = empty + kRing;                  // [group][accumulator]
     uint64_t* acce = accf + kEpiGroups * kAccTiles;
@@ -473,9 +479,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         uint32_t uses[kAccTiles];   // this group's earlier tiles per accumulator
         for (int i = 0; i < kAccTiles; ++i) uses[i] = 0;
         uint32_t n = 0;             // the CTA's tiles so far
-        uint32_t kst = 0;           // this group's tiles so far (staging buffer kst & 1)
+        uint32_t kst = 0;           // this group's tiles so far (staging buffer kst % kOutStages)
         const bool ostore = MODE != kLast && a.use_ostore;
-        const uint32_t stage0 = smem_u32(ostage) + uint32_t(g * 2 * 128 * N * 2);
+        const uint32_t stage0 = smem_u32(ostage) + uint32_t(g * kOutStages * 128 * N * 2);
         bool ok = true;
         for (int item = blockIdx.x; item < items && ok; item += gridDim.x) {
             const Item it = item_of(a, item);
@@ -535,10 +541,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                         out[c8] = make_uint4(w[0], w[1], w[2], w[3]);
                     }
                     if (ostore) {
-                        // the bulk store that last read this buffer (two tiles ago) is done
-                        if (row == 0) bulk_wait_read1();
+                        // the bulk store that last read this buffer (kOutStages tiles ago) is done
+                        if (row == 0) bulk_wait_read_stages();
                         group_bar(1 + g);
-                        const uint32_t buf = stage0 + (kst & 1u) * uint32_t(128 * N * 2) + uint32_t(row * N * 2);
+                        const uint32_t buf =
+                            stage0 + (kst % kOutStages) * uint32_t(128 * N * 2) + uint32_t(row * N * 2);
 #pragma unroll
                         for (int c8 = 0; c8 < N / 8; ++c8)
                             asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(buf + c8 * 16),
@@ -548,7 +555,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         group_bar(1 + g);
                         if (row == 0)   // rows outside the mesh are clipped by the store
                             tma_store_4d(&omap, 0, it.x0, it.y0, it.z0 + i,
-                                         stage0 + (kst & 1u) * uint32_t(128 * N * 2));
+                                         stage0 + (kst % kOutStages) * uint32_t(128 * N * 2));
                         ++kst;
                     } else {
                         uint4* dst = reinterpret_cast<uint4*>(a.Y + v * a.cout);

@@ -876,7 +876,6 @@ struct djb_solver {
     float2* phase = nullptr;    // px, py, pz tables (n + n + n/2+1)
     // brick sort of the particles (sort.cuh)
     bool sorted = true;
-    bool zp4 = false;        // z pass with 4 pencils per CTA (DJB_ZPASS_P=4)
     bool fd_scalar = false;  // stencil kernels with 4-byte copies only (DJB_FD_SCALAR=1; the 16-byte path is the default)
     djb::SortGeom sg{};
     int64_t nbins = 0;
@@ -1285,11 +1284,7 @@ int resample_deposit(djb_solver* s, int si, float* mesh) {
 void launch_zpass(djb_solver* s, float* mesh, int nh) {
     const dim3 grid(unsigned((nh + djb::kZPencils - 1) / djb::kZPencils), unsigned(s->res));
     const djb::KPhiFn kp{s->lapT, s->makT, s->s0};
-    if (DJB_ZPASS_PAIR && s->zp4) {
-        const dim3 grid4(unsigned((nh + 3) / 4), unsigned(s->res));
-        djb::k_zpencil_pair<djb::KPhiFn, 4><<<grid4, 4 * 64, 4 * djb::kZPlane * 8, s->stream>>>(
-            reinterpret_cast<float2*>(mesh), nh, s->wN, kp);
-    } else if (DJB_ZPASS_PAIR)
+    if (DJB_ZPASS_PAIR)
         djb::k_zpencil_pair<<<grid, djb::kZPairThreads, djb::kZSmem, s->stream>>>(reinterpret_cast<float2*>(mesh), nh,
                                                                                   s->wN, kp);
     else
@@ -1685,10 +1680,6 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
     }
     if (s->tiled) TRY(tiled_attrs(s->W, s->R));
     {
-        const char* zp = std::getenv("DJB_ZPASS_P");
-        s->zp4 = zp && std::strcmp(zp, "4") == 0;
-    }
-    {
         const char* fs = std::getenv("DJB_FD_SCALAR");
         s->fd_scalar = fs && std::strcmp(fs, "1") == 0;
     }
@@ -1847,8 +1838,6 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
             CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
-            CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn, 4>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * djb::kZPlane * 8));
         }
         if (s->sorted && s->gsx <= res) {
             for (int m = 0; m < s->group; ++m) {

@@ -218,7 +218,7 @@ __device__ __forceinline__ void dit_stage16(float2 (&b)[16]) {
     }
 }
 
-// The partner of the pair is `P` lanes away (P pencils per CTA, P = 4, 8 or 16).
+// The partner of the pair is `P` lanes away (P pencils per CTA, P = 8 or 16).
 template <int P>
 __device__ __forceinline__ float2 shfl_pair(float2 v) {
     return make_float2(__shfl_xor_sync(0xffffffffu, v.x, P), __shfl_xor_sync(0xffffffffu, v.y, P));
@@ -262,7 +262,7 @@ __device__ __forceinline__ void dft32_dit_pair(float2 (&b)[16], int h) {
 // pencil q, half h, and t = n2 (steps A, B') or k1 (steps B, A'); a warp reads 32/P kz
 // row pairs of P consecutive kx (8·P bytes each) per load.
 template <class KPhi, int P = 8>
-__global__ void __launch_bounds__(64 * P, P == 8 ? 2 : (P == 4 ? 4 : 1)) k_zpencil_pair(float2* __restrict__ f, int nh,
+__global__ void __launch_bounds__(64 * P, P == 8 ? 2 : 1) k_zpencil_pair(float2* __restrict__ f, int nh,
                                                                          const float2* __restrict__ wN, KPhi kphi) {
     extern __shared__ __align__(16) float2 s[];  // P transpose blocks
     const int q = threadIdx.x & (P - 1);
