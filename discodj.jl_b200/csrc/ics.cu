@@ -1,8 +1,8 @@
-// Second-order LPT initial conditions on the GPU: white noise -> phi(k) -> psi_1, psi_2 ->
-// (Psi, Pi) at growth factor D, with cuFFT transforms and fused k-space / real-space
-// kernels.
+// Second- and third-order LPT initial conditions on the GPU: white noise -> phi(k) ->
+// psi_1, psi_2 (, psi_3) -> (Psi, Pi) at growth factor D, with cuFFT transforms and fused
+// k-space / real-space kernels.
 //
-// Restates, for n_order = 2:
+// Restates, for n_order = 2 and 3 (EdS growth, as the reference's `compute_core`):
 //   src/ics/grf.jl:118-144   phi(k) = rfft(w) * (-sqrt(P(|k|) (n/L)^3) / k^2), 0 at k = 0, with
 //                            P linearly interpolated in a host table (clamped at its ends);
 //   src/lpt/nlpt_core.jl     psi_1 = -D phi (D_a = i k_a, the Nyquist entries zeroed);
@@ -11,7 +11,13 @@
 //                            spectra embedded with the Nyquist planes dropped, scaled by
 //                            (ext/n)^3; products in real space; cropped back, scaled by
 //                            (n/ext)^3); psi_2 = -1/k^2 (DC: -1) * D (-3/7 mu2);
-//   src/nbody/run_nbody.jl:180-208   Psi = D psi_1 + D^2 psi_2, Pi = dPsi/dD = psi_1 + 2 D psi_2.
+//                            third order (nlpt_core.jl:223-280, i = 3): the longitudinal source
+//                            -5/9 mu2(psi_1, psi_2) - 1/3 mu3(psi_1, psi_1, psi_1) and the
+//                            transverse source 1/3 C(psi_1, psi_2), products of the padded
+//                            derivative fields in real space with the reference's index and
+//                            sign tables; psi_3 = il (D fL - D x C) (the curl form of
+//                            nlpt_core.jl:267-280);
+//   src/nbody/run_nbody.jl:180-208   Psi = sum_m D^m psi_m, Pi = dPsi/dD = sum_m m D^(m-1) psi_m.
 //
 // Layout: real fields of n^3 floats with x fastest ([k][j][i], the library's particle
 // component blocks); cuFFT's R2C then halves x, so spectra are [kz][ky][kx], kx in
@@ -188,6 +194,129 @@ __global__ void k_lpt_combine(const float* __restrict__ p1, const float* __restr
     }
 }
 
+// Symmetric 3x3 index (a, b in 0..2) -> storage slot: diagonal 0..2, then (0,1), (0,2), (1,2).
+__device__ __forceinline__ int sym3(int a, int b) {
+    if (a == b) return a;
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    return lo == 0 ? (hi == 1 ? 3 : 4) : 5;
+}
+
+// Ext-grid spectrum of D_b psi_2,a (psi_2 = il D fL2, fL2 = fl * mu2(k) the cropped source):
+// (i k_b)(i k_a) il fl mu2_ext(k_e) on the embedded modes (0 elsewhere), scaled by 1/n^3:
+// the pad factor (ext/n)^3 and the inverse transform's 1/ext^3.
+__global__ void k_q_deriv(const float2* __restrict__ mu, int n, int ext, float dk, float fl, int a, int b,
+                          float2* __restrict__ out) {
+    const int eh = ext / 2 + 1, h = n / 2;
+    const int64_t total = int64_t(ext) * ext * eh;
+    const float scale = 1.0f / (float(n) * float(n) * float(n));
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+        const int ex = int(t % eh);
+        const int64_t r = t / eh;
+        const int ey = int(r % ext), ez = int(r / ext);
+        const int sx = ex < h ? ex : -1;
+        const int sy = ey < h ? ey : (ey > ext - h ? ey - ext + n : -1);
+        const int sz = ez < h ? ez : (ez > ext - h ? ez - ext + n : -1);
+        float2 v = make_float2(0.0f, 0.0f);
+        if (sx >= 0 && sy >= 0 && sz >= 0) {
+            const float k3[3] = {dk_half(sx, n, dk), dk_full(sy, n, dk), dk_full(sz, n, dk)};
+            const float mx = float(sx), my = float(mode_full(sy, n)), mz = float(mode_full(sz, n));
+            const float k2 = (mx * mx + my * my + mz * mz) * dk * dk;
+            const float il = (sx == 0 && sy == 0 && sz == 0) ? -1.0f : -1.0f / k2;
+            const float f = -k3[a] * k3[b] * il * fl * scale;
+            const float2 m = mu[t];
+            v = make_float2(m.x * f, m.y * f);
+        }
+        out[t] = v;
+    }
+}
+
+// The third-order sources at every ext-grid point, from P_ab = D_b psi_1,a and
+// Q_ab = D_b psi_2,a (symmetric, six slots each; P and Q point at six fields of E floats):
+//   fL3 = -5/9 mu2(psi_1, psi_2) - 1/3 mu3(psi_1, psi_1, psi_1),   C3_c = 1/3 C_c(psi_1, psi_2),
+// with mu2, C and mu3 the sums of nlpt_core.jl:223-263 (1-based index tables as there).
+// Written in place of Q's first four slots (each thread reads its point's inputs first).
+__global__ void k_lpt3_source(const float* __restrict__ P, float* __restrict__ Q, int64_t E) {
+    constexpr int MI[12] = {1, 1, 2, 3, 2, 2, 3, 1, 3, 3, 1, 2}, MJ[12] = {2, 3, 1, 1, 3, 1, 2, 2, 1, 2, 3, 3};
+    constexpr int MK[12] = {1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 3}, ML[12] = {2, 3, 2, 3, 3, 1, 3, 1, 1, 2, 1, 2};
+    constexpr float MS[12] = {1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1};
+    constexpr int CI[6] = {1, 1, 2, 2, 3, 3}, CK[6] = {2, 3, 2, 3, 2, 3}, CL[6] = {3, 2, 3, 2, 3, 2};
+    constexpr float CS[6] = {1, -1, 1, -1, 1, -1};
+    constexpr int UK[6] = {1, 1, 2, 2, 3, 3}, UL[6] = {2, 3, 3, 1, 1, 2}, UM[6] = {3, 2, 1, 3, 2, 1};
+    constexpr float US[6] = {1, -1, 1, -1, 1, -1};
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < E; t += int64_t(gridDim.x) * blockDim.x) {
+        float p[6], q[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            p[i] = P[i * E + t];
+            q[i] = Q[i * E + t];
+        }
+        auto pa = [&](int m, int ax) { return p[sym3(m - 1, ax - 1)]; };
+        auto qa = [&](int m, int ax) { return q[sym3(m - 1, ax - 1)]; };
+        float mu2 = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) mu2 += MS[i] * (pa(MI[i], MK[i]) * qa(MJ[i], ML[i]));
+        float c3[3];
+#pragma unroll
+        for (int sh = 0; sh < 3; ++sh) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                const int ci = (CI[i] - 1 + sh) % 3 + 1, ck = (CK[i] - 1 + sh) % 3 + 1, cl = (CL[i] - 1 + sh) % 3 + 1;
+                acc += CS[i] * (pa(ci, ck) * qa(ci, cl));
+            }
+            c3[sh] = acc;
+        }
+        float mu3 = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) mu3 += US[i] * (pa(1, UK[i]) * (pa(2, UL[i]) * pa(3, UM[i])));
+        Q[t] = (-5.0f / 9.0f) * mu2 - (1.0f / 3.0f) * mu3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Q[(c + 1) * E + t] = (1.0f / 3.0f) * c3[c];
+    }
+}
+
+// psi_3 component a (n grid spectrum, 1/n^3 folded in): il (i k_a FL - (i k_b C_c - i k_c C_b)),
+// (a, b, c) cyclic, FL and C_c the cropped ext spectra src[0] and src[1 + c] (each Es modes).
+__global__ void k_crop_assemble3(const float2* __restrict__ src, int64_t Es, int n, int ext, float dk, int a,
+                                 float2* __restrict__ psi3) {
+    const int nh = n / 2 + 1, eh = ext / 2 + 1, h = n / 2;
+    const int64_t total = int64_t(n) * n * nh;
+    const float inv_n3 = 1.0f / (float(n) * float(n) * float(n));
+    const float crop = float(double(n) * n * n / (double(ext) * ext * ext));
+    const int b = (a + 1) % 3, c = (a + 2) % 3;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+        const int kx = int(t % nh);
+        const int64_t r = t / nh;
+        const int ky = int(r % n), kz = int(r / n);
+        float2 q = make_float2(0.0f, 0.0f);
+        if (kx != h && ky != h && kz != h) {
+            const int ey = ky < h ? ky : ky - n + ext, ez = kz < h ? kz : kz - n + ext;
+            const int64_t e = (int64_t(ez) * ext + ey) * eh + kx;
+            const float k3[3] = {dk_half(kx, n, dk), dk_full(ky, n, dk), dk_full(kz, n, dk)};
+            const float2 fl = src[e], cb = src[(1 + b) * Es + e], cc = src[(1 + c) * Es + e];
+            const float mx = float(kx), my = float(mode_full(ky, n)), mz = float(mode_full(kz, n));
+            const float k2 = (mx * mx + my * my + mz * mz) * dk * dk;
+            const float il = (kx == 0 && ky == 0 && kz == 0) ? -1.0f : -1.0f / k2;
+            // w = k_a FL - (k_b C_c - k_c C_b); psi3 = il * i * w * crop / n^3
+            const float wx = k3[a] * fl.x - (k3[b] * cc.x - k3[c] * cb.x);
+            const float wy = k3[a] * fl.y - (k3[b] * cc.y - k3[c] * cb.y);
+            const float g = il * crop * inv_n3;
+            q = make_float2(-g * wy, g * wx);
+        }
+        psi3[t] = q;
+    }
+}
+
+// Psi += D^3 psi3, Pi += 3 D^2 psi3.
+__global__ void k_lpt_combine3(const float* __restrict__ p3, int64_t m, float D, float* __restrict__ psi,
+                               float* __restrict__ pi) {
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < m; t += int64_t(gridDim.x) * blockDim.x) {
+        const float c = p3[t];
+        psi[t] += (D * D * D) * c;
+        pi[t] += (3.0f * D * D) * c;
+    }
+}
+
 // cuFFT plans kept per (device, size, kind) for the life of the library: creating a 768^3
 // plan takes longer than the whole 512^3 computation.
 std::mutex g_plan_mu;
@@ -211,10 +340,41 @@ cufftResult cached_plan(int device, int size, cufftType kind, cufftHandle* out) 
 
 }  // namespace
 
-extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab,
-                            int32_t npk, double D, float* psi, float* pi, int32_t device, void* stream) {
+namespace {
+
+// Work area of one call, carved from one block: byte offsets of phi, the two n-grid
+// spectra, the ext spectrum of mu2, P, mu2, Q, the second ext spectrum, the two n-grid
+// real fields and the P(k) table (each 256-byte aligned).
+struct IcsLayout {
+    enum { kPhi, kSpec, kEspec, kP, kMu, kQ, kEspec2, kF, kKt, kPt, kCount };
+    int64_t off[kCount];
+    int64_t total;
+};
+
+IcsLayout ics_layout(int n, int order, int npk) {
+    const int ext = 3 * n / 2;
+    const int64_t N = int64_t(n) * n * n, Ns = int64_t(n) * n * (n / 2 + 1);
+    const int64_t E = int64_t(ext) * ext * ext, Es = int64_t(ext) * ext * (ext / 2 + 1);
+    const bool third = order == 3;
+    const int64_t bytes[IcsLayout::kCount] = {8 * Ns,        16 * Ns,       8 * Es,      4 * E * (third ? 6 : 4),
+                                              4 * E,         third ? 24 * E : 0,       third ? 8 * Es : 0,
+                                              8 * N,         8 * int64_t(npk),         8 * int64_t(npk)};
+    IcsLayout l;
+    int64_t at = 0;
+    for (int i = 0; i < IcsLayout::kCount; ++i) {
+        l.off[i] = at;
+        at += (bytes[i] + 255) / 256 * 256;
+    }
+    l.total = at;
+    return l;
+}
+
+int lpt_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab, int32_t npk,
+            int32_t order, double D, float* psi, float* pi, void* work, int64_t work_bytes, int32_t device,
+            void* stream) {
     djb::clear_error();
     if (!white || !k_tab || !p_tab || !psi || !pi) return fail(DJB_ERR_INVALID, "null argument");
+    if (order != 2 && order != 3) return fail(DJB_ERR_INVALID, "n_order must be 2 or 3");
     if (n < 4 || (n & 1) || (3 * n) % 2 != 0 || ((3 * n / 2) & 1))
         return fail(DJB_ERR_INVALID, "n must be a multiple of 4 (n and the 3/2-padded 3n/2 even)");
     if (npk < 2) return fail(DJB_ERR_INVALID, "the P(k) table needs at least 2 points");
@@ -227,21 +387,37 @@ extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const
     const int64_t N = int64_t(n) * n * n, Ns = int64_t(n) * n * nh;
     const int64_t E = int64_t(ext) * ext * ext, Es = int64_t(ext) * ext * eh;
     const double dk = 2 * M_PI / boxsize;
+    const bool third = order == 3;
+    const IcsLayout lay = ics_layout(n, order, npk);
+    const float crop = float(double(n) * n * n / (double(E)));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cufftHandle r2c_n = 0, c2r_n = 0, r2c_e = 0, c2r_e = 0;
-    float2 *phi = nullptr, *spec = nullptr, *espec = nullptr, *s1 = nullptr, *s2 = nullptr;
-    float *ediag = nullptr, *emu = nullptr, *eoff = nullptr, *f1 = nullptr, *f2 = nullptr;
+    float2 *phi = nullptr, *spec = nullptr, *espec = nullptr, *espec2 = nullptr, *s1 = nullptr, *s2 = nullptr;
+    float *P = nullptr, *Q = nullptr, *emu = nullptr, *f1 = nullptr, *f2 = nullptr;
     double *dkt = nullptr, *dpt = nullptr;
+    float2* src3 = nullptr;   // third order: the four source spectra, over P
+    uint8_t* owned = nullptr;
+    uint8_t* base = static_cast<uint8_t*>(work);
+    if (work && work_bytes < lay.total)
+        return fail(DJB_ERR_INVALID, "work area of %lld bytes, %lld needed", (long long)work_bytes,
+                    (long long)lay.total);
     ICS_CUDA(cudaSetDevice(device));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&phi), sizeof(float2) * Ns, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&spec), sizeof(float2) * Ns * 2, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&espec), sizeof(float2) * Es, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ediag), sizeof(float) * E * 3, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&emu), sizeof(float) * E, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&eoff), sizeof(float) * E, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&f1), sizeof(float) * N * 2, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&dkt), sizeof(double) * npk, st));
-    ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&dpt), sizeof(double) * npk, st));
+    if (!base) {
+        ICS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&owned), size_t(lay.total), st));
+        base = owned;
+    }
+    phi = reinterpret_cast<float2*>(base + lay.off[IcsLayout::kPhi]);
+    spec = reinterpret_cast<float2*>(base + lay.off[IcsLayout::kSpec]);
+    espec = reinterpret_cast<float2*>(base + lay.off[IcsLayout::kEspec]);
+    P = reinterpret_cast<float*>(base + lay.off[IcsLayout::kP]);
+    emu = reinterpret_cast<float*>(base + lay.off[IcsLayout::kMu]);
+    if (third) {
+        Q = reinterpret_cast<float*>(base + lay.off[IcsLayout::kQ]);
+        espec2 = reinterpret_cast<float2*>(base + lay.off[IcsLayout::kEspec2]);
+    }
+    f1 = reinterpret_cast<float*>(base + lay.off[IcsLayout::kF]);
+    dkt = reinterpret_cast<double*>(base + lay.off[IcsLayout::kKt]);
+    dpt = reinterpret_cast<double*>(base + lay.off[IcsLayout::kPt]);
     s1 = spec;
     s2 = spec + Ns;
     f2 = f1 + N;
@@ -262,32 +438,73 @@ extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const
     // mu2 on the ext grid: the three diagonal second derivatives, then the off-diagonal squares
     for (int a = 0; a < 3; ++a) {
         k_pad_deriv<<<grid_of(Es), kT, 0, st>>>(phi, n, ext, float(dk), a, a, espec);
-        ICS_FFT(cufftExecC2R(c2r_e, reinterpret_cast<cufftComplex*>(espec), ediag + a * E));
+        ICS_FFT(cufftExecC2R(c2r_e, reinterpret_cast<cufftComplex*>(espec), P + a * E));
     }
-    k_mu2_diag<<<grid_of(E), kT, 0, st>>>(ediag, ediag + E, ediag + 2 * E, E, emu);
+    k_mu2_diag<<<grid_of(E), kT, 0, st>>>(P, P + E, P + 2 * E, E, emu);
     for (int p = 0; p < 3; ++p) {
-        const int a = p == 2 ? 1 : 0, b = p == 0 ? 1 : 2;   // (0,1), (0,2), (1,2)
+        const int a = p == 2 ? 1 : 0, b = p == 0 ? 1 : 2;   // (0,1), (0,2), (1,2): slots 3, 4, 5
+        float* off = P + (third ? 3 + p : 3) * E;
         k_pad_deriv<<<grid_of(Es), kT, 0, st>>>(phi, n, ext, float(dk), a, b, espec);
-        ICS_FFT(cufftExecC2R(c2r_e, reinterpret_cast<cufftComplex*>(espec), eoff));
-        k_mu2_sub<<<grid_of(E), kT, 0, st>>>(eoff, E, emu);
+        ICS_FFT(cufftExecC2R(c2r_e, reinterpret_cast<cufftComplex*>(espec), off));
+        k_mu2_sub<<<grid_of(E), kT, 0, st>>>(off, E, emu);
     }
     ICS_CUDA(cudaGetLastError());
     ICS_FFT(cufftExecR2C(r2c_e, emu, reinterpret_cast<cufftComplex*>(espec)));
-    // psi_1, psi_2 per component, then Psi and Pi
+    src3 = reinterpret_cast<float2*>(P);
+    if (third) {
+        // Q_ab = D_b psi_2,a on the ext grid from the mu2 spectrum
+        const float fl = -3.0f / 7.0f * crop;
+        for (int slot = 0; slot < 6; ++slot) {
+            const int a = slot < 3 ? slot : (slot == 5 ? 1 : 0);
+            const int b = slot < 3 ? slot : (slot == 3 ? 1 : 2);
+            k_q_deriv<<<grid_of(Es), kT, 0, st>>>(espec, n, ext, float(dk), fl, a, b, espec2);
+            ICS_FFT(cufftExecC2R(c2r_e, reinterpret_cast<cufftComplex*>(espec2), Q + slot * E));
+        }
+        k_lpt3_source<<<grid_of(E), kT, 0, st>>>(P, Q, E);
+        ICS_CUDA(cudaGetLastError());
+        for (int f = 0; f < 4; ++f)
+            ICS_FFT(cufftExecR2C(r2c_e, Q + f * E, reinterpret_cast<cufftComplex*>(src3 + f * Es)));
+    }
+    // psi_1, psi_2 (, psi_3) per component, then Psi and Pi
     for (int a = 0; a < 3; ++a) {
         k_crop_assemble<<<grid_of(Ns), kT, 0, st>>>(espec, phi, n, ext, float(dk), a, s1, s2);
         ICS_FFT(cufftExecC2R(c2r_n, reinterpret_cast<cufftComplex*>(s1), f1));
         ICS_FFT(cufftExecC2R(c2r_n, reinterpret_cast<cufftComplex*>(s2), f2));
         k_lpt_combine<<<grid_of(N), kT, 0, st>>>(f1, f2, N, float(D), psi + a * N, pi + a * N);
+        if (third) {
+            k_crop_assemble3<<<grid_of(Ns), kT, 0, st>>>(src3, Es, n, ext, float(dk), a, s1);
+            ICS_FFT(cufftExecC2R(c2r_n, reinterpret_cast<cufftComplex*>(s1), f1));
+            k_lpt_combine3<<<grid_of(N), kT, 0, st>>>(f1, N, float(D), psi + a * N, pi + a * N);
+        }
     }
     ICS_CUDA(cudaGetLastError());
     ICS_CUDA(cudaStreamSynchronize(st));
 done:
-    for (void* q : {static_cast<void*>(phi), static_cast<void*>(spec), static_cast<void*>(espec),
-                    static_cast<void*>(ediag), static_cast<void*>(emu), static_cast<void*>(eoff),
-                    static_cast<void*>(f1), static_cast<void*>(dkt), static_cast<void*>(dpt)})
-        if (q) cudaFreeAsync(q, st);
+    if (owned) cudaFreeAsync(owned, st);
     cudaStreamSynchronize(st);
     if (prev >= 0) cudaSetDevice(prev);
     return rc;
+}
+
+}  // namespace
+
+extern "C" int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab,
+                            int32_t npk, double D, float* psi, float* pi, int32_t device, void* stream) {
+    return lpt_ics(white, n, boxsize, k_tab, p_tab, npk, 2, D, psi, pi, nullptr, 0, device, stream);
+}
+
+extern "C" int djb_lpt_ics_work_bytes(int32_t n, int32_t n_order, int32_t npk, int64_t* bytes) {
+    djb::clear_error();
+    if (!bytes) return fail(DJB_ERR_INVALID, "null argument");
+    if (n_order != 2 && n_order != 3) return fail(DJB_ERR_INVALID, "n_order must be 2 or 3");
+    if (n < 4 || (n & 3)) return fail(DJB_ERR_INVALID, "n must be a multiple of 4 (n and the 3/2-padded 3n/2 even)");
+    if (npk < 2) return fail(DJB_ERR_INVALID, "the P(k) table needs at least 2 points");
+    *bytes = ics_layout(n, n_order, npk).total;
+    return DJB_OK;
+}
+
+extern "C" int djb_lpt_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab,
+                           int32_t npk, int32_t n_order, double D, float* psi, float* pi, void* work,
+                           int64_t work_bytes, int32_t device, void* stream) {
+    return lpt_ics(white, n, boxsize, k_tab, p_tab, npk, n_order, D, psi, pi, work, work_bytes, device, stream);
 }

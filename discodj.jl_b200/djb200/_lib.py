@@ -115,6 +115,8 @@ SIGNATURES = {
     "djb_state_density_modes": [_P, _I, _IP, _DP],
     "djb_selftest_bounded_wait": [_I, _I, C.c_int64, _IP],
     "djb_lpt2_ics": [_P, _I, _D, _DP, _DP, _I, _D, _P, _P, _I, _P],
+    "djb_lpt_ics": [_P, _I, _D, _DP, _DP, _I, _I, _D, _P, _P, _P, C.c_int64, _I, _P],
+    "djb_lpt_ics_work_bytes": [_I, _I, _I, _I64P],
 }
 _RESTYPES = {"djb_version": C.c_char_p, "djb_last_error": C.c_char_p}
 

@@ -308,12 +308,13 @@ def lpt_ics(cosmo, n: int, boxsize: float, a: float, *, n_order: int = 2, seed: 
     return Psi, Pi
 
 
-def lpt2_ics_native(cosmo, n: int, boxsize: float, a: float, *, seed: int = 42, white=None, device: int = 0):
-    """2LPT (Ψ, Π = dΨ/dD) at scale factor a from the library's CUDA kernels
-    (`djb_lpt2_ics`): the same white noise → φ → ψ₁, ψ₂ chain as `lpt_ics(n_order=2)`,
-    with the fields and products in float32 on the GPU. `white`: (n,n,n) [i,j,k] tensor
-    (default: `white_noise(seed, n)` on the device). Returns native (3,n,n,n) float32
-    device tensors (the library's particle layout, `pm.native_view`)."""
+def lpt_ics_native(cosmo, n: int, boxsize: float, a: float, *, n_order: int = 2, seed: int = 42, white=None,
+                   device: int = 0):
+    """nLPT (Ψ, Π = dΨ/dD) at scale factor a from the library's CUDA kernels
+    (`djb_lpt_ics`, n_order 2 or 3): the same white noise → φ → ψ₁, ψ₂ (, ψ₃) chain as
+    `lpt_ics(n_order=...)`, with the fields and products in float32 on the GPU. `white`:
+    (n,n,n) [i,j,k] tensor (default: `white_noise(seed, n)` on the device). Returns native
+    (3,n,n,n) float32 device tensors (the library's particle layout, `pm.native_view`)."""
     import ctypes as C
 
     from . import _lib
@@ -325,8 +326,18 @@ def lpt2_ics_native(cosmo, n: int, boxsize: float, a: float, *, seed: int = 42, 
     p_tab = np.ascontiguousarray(p_tab, dtype=np.float64)
     psi = torch.empty((3, n, n, n), dtype=torch.float32, device=dev)
     pi = torch.empty_like(psi)
+    nb = np.zeros(1, dtype=np.int64)
+    _lib.check(_lib.lib.djb_lpt_ics_work_bytes(int(n), int(n_order), len(k_tab), _lib.i64ptr(nb)))
+    work = torch.empty(int(nb[0]), dtype=torch.uint8, device=dev)   # torch's cache keeps it between calls
     stream = torch.cuda.current_stream(dev).cuda_stream
-    _lib.check(_lib.lib.djb_lpt2_ics(C.c_void_p(w_native.data_ptr()), int(n), float(boxsize), _lib.dptr(k_tab),
-                                     _lib.dptr(p_tab), len(k_tab), float(cosmo.Dplus(a)), C.c_void_p(psi.data_ptr()),
-                                     C.c_void_p(pi.data_ptr()), int(device), C.c_void_p(stream)))
+    _lib.check(_lib.lib.djb_lpt_ics(C.c_void_p(w_native.data_ptr()), int(n), float(boxsize), _lib.dptr(k_tab),
+                                    _lib.dptr(p_tab), len(k_tab), int(n_order), float(cosmo.Dplus(a)),
+                                    C.c_void_p(psi.data_ptr()), C.c_void_p(pi.data_ptr()),
+                                    C.c_void_p(work.data_ptr()), int(nb[0]), int(device), C.c_void_p(stream)))
+    del work
     return psi, pi
+
+
+def lpt2_ics_native(cosmo, n: int, boxsize: float, a: float, *, seed: int = 42, white=None, device: int = 0):
+    """`lpt_ics_native` at n_order = 2 (`djb_lpt2_ics`)."""
+    return lpt_ics_native(cosmo, n, boxsize, a, n_order=2, seed=seed, white=white, device=device)

@@ -213,7 +213,7 @@ DJB_API int djb_state_power_spectrum(djb_solver* s, int32_t bins, int32_t logari
  * The particle state stays on the device. */
 DJB_API int djb_state_density_modes(djb_solver* s, int32_t nmodes, const int32_t* modes, double* out);
 
-/* ── initial conditions (2LPT) ───────────────────────────────────────────────
+/* ── initial conditions (2LPT, 3LPT) ─────────────────────────────────────────
  * Replaces the GPU path of `nbody_ics_lpt` at n_order = 2 (src/ics/grf.jl:118-144,
  * src/lpt/nlpt_core.jl:44-311, src/nbody/run_nbody.jl:180-208): white noise w (device, n^3
  * float32, x fastest) -> phi(k) = rfft(w) * (-sqrt(P(|k|) (n/L)^3) / k^2) with P linearly
@@ -226,6 +226,17 @@ DJB_API int djb_state_density_modes(djb_solver* s, int32_t nmodes, const int32_t
  * for the call. */
 DJB_API int djb_lpt2_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab,
                          int32_t npk, double D, float* psi, float* pi, int32_t device, void* stream);
+/* The same chain at n_order = 2 or 3 (`compute_core`, src/lpt/nlpt_core.jl:311, EdS
+ * growth): for 3, psi_3 from the longitudinal source -5/9 mu2(psi_1, psi_2) -
+ * 1/3 mu3(psi_1, psi_1, psi_1) and the transverse source 1/3 C(psi_1, psi_2) of
+ * nlpt_core.jl:223-280 (products of the 3/2-padded derivative fields in real space),
+ * Psi = sum_m D^m psi_m, Pi = sum_m m D^(m-1) psi_m. `work`: a device area of at least
+ * djb_lpt_ics_work_bytes bytes (about 14 (3n/2)^3 + 6 n^3 floats for n_order = 3, 5 and 6
+ * for 2), or NULL to have the call allocate and free one. */
+DJB_API int djb_lpt_ics(const float* white, int32_t n, double boxsize, const double* k_tab, const double* p_tab,
+                        int32_t npk, int32_t n_order, double D, float* psi, float* pi, void* work,
+                        int64_t work_bytes, int32_t device, void* stream);
+DJB_API int djb_lpt_ics_work_bytes(int32_t n, int32_t n_order, int32_t npk, int64_t* bytes);
 
 /* ── adjoints (vector-Jacobian products) ────────────────────────────────────
  * No counterpart in the reference, which has no adjoint; these are the transposes
