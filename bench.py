@@ -194,12 +194,16 @@ def aggregate_value(world: int, n_part: int, steps: int, ms_max: float) -> float
 
 
 def make_ics(cosmo, n, L, lpt, seed, device):
+    """nLPT (Ψ, Π) at A_INI as native (3,n,n,n) float32 tensors on `device`: the library's
+    CUDA generator (`djb_lpt_ics`) at n >= 256, the float64 torch restatement below."""
     import torch
 
+    import djb200
     from djb200 import ics
-    dt = torch.float32 if n >= 256 else torch.float64
-    psi, pi = ics.lpt_ics(cosmo, n, L, A_INI, n_order=lpt, seed=seed, device=device, dtype=dt)
-    return psi.float(), pi.float()
+    if n >= 256 and str(device).startswith("cuda"):
+        return ics.lpt_ics_native(cosmo, n, L, A_INI, n_order=lpt, seed=seed, device=torch.device(device).index or 0)
+    psi, pi = ics.lpt_ics(cosmo, n, L, A_INI, n_order=lpt, seed=seed, device=device, dtype=torch.float64)
+    return djb200.native_view(psi.float()), djb200.native_view(pi.float())
 
 
 def cpu_sample(n: int, res: int, L: float, steps: int, warmup: int, seed: int = 42):
@@ -384,15 +388,12 @@ def main():
     torch.cuda.set_device(local)
     n, res, L, lpt = SIZES[args.size]
     cosmo = djb200.Cosmology(**COSMO)
-    psi, pi = make_ics(cosmo, n, L, lpt, replica_seed(rank), dev)
-    psi_d = djb200.native_view(psi)
-    pi_d = djb200.native_view(pi)
+    psi_d, pi_d = make_ics(cosmo, n, L, lpt, replica_seed(rank), dev)
     # pinned host copies for the end-to-end leg
     psi_h = torch.empty((3, n, n, n), dtype=torch.float32, pin_memory=True)
     pi_h = torch.empty_like(psi_h, pin_memory=True)
     psi_h.copy_(psi_d)
     pi_h.copy_(pi_d)
-    del psi, pi
     torch.cuda.empty_cache()
     nsteps = args.warmup + args.steps
     co = djb200.stepper_coefficients(cosmo, "bullfrog", A_INI, A_END, nsteps)

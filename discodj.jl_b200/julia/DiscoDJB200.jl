@@ -296,4 +296,26 @@ write_snapshot_b200(S::PMSolverB200, path::AbstractString, D::Real, L::Real; p_d
     _check(ccall((:djb_state_write_snapshot, LIB), Cint, (Ptr{Cvoid}, Cstring, Float64, Float64, Float64, Float64),
                  S.handle, path, D, L, p_div, p_mul))
 
+"""
+    lpt_ics_b200(white::CuArray{Float32,3}, boxsize, k_tab, p_tab, D; n_order=2, device=0)
+        -> (Psi, Pi) as (n,n,n,3) CuArray{Float32}
+
+The GPU path of `nbody_ics_lpt` (src/ics/grf.jl:118-144, src/lpt/nlpt_core.jl:311,
+src/nbody/run_nbody.jl:180-208) at n_order 2 or 3: white noise -> phi(k) with P(k) from the
+host table (k_tab, p_tab) -> psi_1 .. psi_n_order -> Psi = sum D^m psi_m, Pi = dPsi/dD
+(djb_lpt_ics; the work block is allocated by the call).
+"""
+function lpt_ics_b200(white::AbstractArray{Float32,3}, boxsize::Real, k_tab::Vector{Float64},
+                      p_tab::Vector{Float64}, D::Real; n_order::Integer=2, device::Integer=0)
+    n = size(white, 1)
+    psi = similar(white, n, n, n, 3)
+    pi_ = similar(white, n, n, n, 3)
+    _check(ccall((:djb_lpt_ics, LIB), Cint,
+                 (Ptr{Cvoid}, Int32, Float64, Ptr{Float64}, Ptr{Float64}, Int32, Int32, Float64, Ptr{Cvoid},
+                  Ptr{Cvoid}, Ptr{Cvoid}, Int64, Int32, Ptr{Cvoid}),
+                 _ptr(white), n, boxsize, k_tab, p_tab, length(k_tab), n_order, D, _ptr(psi), _ptr(pi_),
+                 C_NULL, 0, device, C_NULL))
+    return psi, pi_
+end
+
 end # module
