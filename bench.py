@@ -253,7 +253,10 @@ def run_reference(args, world, rank):
     line = dict(metric=METRIC, value=cb["value"], unit=UNIT, n_gpus=args.gpus, steps=REF_STEPS,
                 warmup=REF_WARMUP, ms_per_step=cb["ms_per_step"], higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="f32", data="synthetic (seeded white noise -> EH P(k) -> 1LPT)",
-                config=config_block(args.size, n, res, L, lpt, world), impl="reference",
+                config=dict(config_block(args.size, n, res, L, lpt, world),
+                            ics_of_sample="1LPT at a=0.02 from the oracle (the cost of a step does not depend on "
+                                          "the IC order; the GPU arm starts from 3LPT)"),
+                impl="reference",
                 cpu_baseline={k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 e2e=dict(value=cb["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)

@@ -371,11 +371,16 @@ __device__ __forceinline__ void brick_stencil(const float* __restrict__ psi, con
 // atomics.
 constexpr unsigned kFixedMax = 4096;
 
+// `tma` != 0: m0..m2 are dense [res]^3 meshes described by tm0..tm2 (boxes of the deposit
+// box's shape); boxes that do not wrap are then converted to float in place and added to
+// the mesh with one bulk tensor reduction each.
 template <int W>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scatter_weighted_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     float sx, float sy, float sz, const float* __restrict__ abar, float scale, float* __restrict__ m0,
-    float* __restrict__ m1, float* __restrict__ m2, int* err, BrickList bl, int sorted_io) {
+    float* __restrict__ m1, float* __restrict__ m2, int* err, BrickList bl, int sorted_io,
+    const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
+    const __grid_constant__ CUtensorMap tm2, int tma) {
     extern __shared__ __align__(128) float wbox[];
     unsigned* qbox = reinterpret_cast<unsigned*>(wbox);
     __shared__ float s_max[kTileThreads / 32];
@@ -386,6 +391,7 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
     const int tid = threadIdx.x;
     const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
     const bool vec = ((pitch | res) & 3) == 0;
+    const bool bulk = tma && box_inside(box, res) && (smem_u32(wbox) & 127u) == 0u;
     const float resf = float(res);
     const int cells = box.plane * box.S[2];   // a multiple of 4
     const float sh[3] = {sx, sy, sz};
@@ -444,6 +450,24 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
                 }
         }
         __syncthreads();
+        if (bulk) {
+            // signed fixed point -> float in place (float sums stay), then one bulk reduction
+            if (fixed)
+                for (int t = 4 * tid; t < cells; t += 4 * kTileThreads) {
+                    const uint4 u = *reinterpret_cast<const uint4*>(qbox + t);
+                    *reinterpret_cast<float4*>(wbox + t) =
+                        make_float4(float(int(u.x)) * down, float(int(u.y)) * down, float(int(u.z)) * down,
+                                    float(int(u.w)) * down);
+                }
+            fence_proxy_async_smem();   // the conversions are read by the bulk copy below
+            __syncthreads();
+            if (tid == 0) {
+                tma_reduce_add_3d(comp == 0 ? &tm0 : (comp == 1 ? &tm1 : &tm2), box.o[0], box.o[1], box.o[2], wbox);
+                bulk_commit_and_wait_read();   // the box is zeroed for the next component after this
+            }
+            __syncthreads();
+            continue;
+        }
         float* mesh = comp == 0 ? m0 : (comp == 1 ? m1 : m2);
         for_box_wrapped(box, res, pitch, vec, [&](int so, int64_t go) {
             if (vec) {
@@ -469,13 +493,17 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_scat
 // particle of the brick adds its share to Ψ̄ per field (a particle belongs to one
 // brick, so no other CTA writes it). sorted_io: psi, abar and psibar are in brick order
 // (slot start + i), read and written coalesced.
+// `tma` != 0: f0 (.. f2) are dense [res]^3 meshes described by tm0 (.. tm2), boxes of the
+// deposit box's shape; boxes that do not wrap are then staged with one bulk tensor copy.
 template <int W>
 __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gather_grad_brick(
     const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res, int pitch,
     float sx, float sy, float sz, const float* __restrict__ f0, const float* __restrict__ f1,
     const float* __restrict__ f2, const float* __restrict__ abar, float scale, float* __restrict__ psibar, int* err,
-    BrickList bl, int sorted_io) {
+    BrickList bl, int sorted_io, const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
+    const __grid_constant__ CUtensorMap tm2, int tma) {
     extern __shared__ __align__(128) float fbox[];
+    __shared__ __align__(8) uint64_t s_bar;
     const int b = brick_of_block(bl, blockIdx.x);
     unsigned start, cnt;
     brick_range(bl, b, start, cnt);
@@ -488,10 +516,29 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_SCATTER_BLOCKS) k_gath
     LatticeDiv ld;
     ld.init(n);
     const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, bl.ssx);
+    const bool bulk = tma && box_inside(box, res) && (smem_u32(fbox) & 127u) == 0u;
+    const unsigned box_bytes = unsigned(box.plane) * unsigned(box.S[2]) * 4u;
+    if (bulk && tid == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    unsigned parity = 0;
 #pragma unroll 1
     for (int f = 0; f < nf; ++f) {
-        stage_box_wrapped(fbox, f == 0 ? f0 : (f == 1 ? f1 : f2), box, res, pitch, vec);
-        __syncthreads();
+        if (bulk) {
+            if (tid == 0) {
+                fence_proxy_async_smem();   // the previous field's reads precede the refill
+                mbar_arrive_expect_tx(&s_bar, box_bytes);
+                tma_load_3d(fbox, f == 0 ? &tm0 : (f == 1 ? &tm1 : &tm2), box.o[0], box.o[1], box.o[2], &s_bar);
+            }
+            const bool ok = mbar_wait(&s_bar, parity);
+            parity ^= 1u;
+            if (__syncthreads_or(!ok)) {   // the copy never completed: report, do not spin
+                if (tid == 0) atomicOr(err, 8);
+                return;
+            }
+        } else {
+            stage_box_wrapped(fbox, f == 0 ? f0 : (f == 1 ? f1 : f2), box, res, pitch, vec);
+            __syncthreads();
+        }
         for (unsigned slot = tid; slot < cnt; slot += kTileThreads) {
             const int64_t p = bl.perm[start + slot];
             const int64_t io = sorted_io ? int64_t(start + slot) : p;

@@ -850,6 +850,9 @@ struct djb_solver {
     float* phi[kMaxGroup] = {nullptr, nullptr};
     CUtensorMap tmap[kMaxGroup];
     CUtensorMap tmap_s[kMaxGroup];
+    CUtensorMap tmap_adj[3];     // the VJP work meshes, deposit-box boxes (dense meshes only)
+    CUtensorMap tmap_rho;        // the first dense mesh, deposit-box boxes (the VJP's rho-bar gather)
+    bool have_tmap_adj = false;
     bool tma = false;
     // res == 1024: the dense transforms are batched 2-D transforms of the z planes and
     // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
@@ -1501,18 +1504,19 @@ void launch_vjp_kernels(djb_solver* s, int stage, const float* psi, const float*
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const size_t smem = scatter_smem(s);
         const djb::BrickList bl = brick_list(s);
+        const int tma = s->have_tmap_adj ? 1 : 0;
         if (stage == 0)
             djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, s->adj[0], s->adj[1], s->adj[2],
-                abar, scale, psibar, s->err, bl, 1);
+                abar, scale, psibar, s->err, bl, 1, s->tmap_adj[0], s->tmap_adj[1], s->tmap_adj[2], tma);
         else if (stage == 1)
             djb::k_scatter_weighted_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, abar, scale, s->adj[0], s->adj[1],
-                s->adj[2], s->err, bl, 1);
+                s->adj[2], s->err, bl, 1, s->tmap_adj[0], s->tmap_adj[1], s->tmap_adj[2], tma);
         else
             djb::k_gather_grad_brick<W><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
                 psi, s->q1, s->n, s->np, s->Lf, s->res, pitch, sh.x, sh.y, sh.z, rho, nullptr, nullptr, nullptr,
-                scale, psibar, s->err, bl, 1);
+                scale, psibar, s->err, bl, 1, s->tmap_rho, s->tmap_rho, s->tmap_rho, tma);
         return;
     }
     if (stage == 0)
@@ -1543,6 +1547,11 @@ int force_vjp(djb_solver* s, float* psi, const float* abar, float* psibar) {
     const size_t rho_floats = s->phi[0] ? size_t(s->res) * s->res * s->res : size_t(s->mesh_floats);
     for (int c = 0; c < 3; ++c)
         if (!s->adj[c]) TRY(dmalloc(s, (void**)&s->adj[c], rho_floats * sizeof(float)));
+    if (s->tma && s->phi[0] && !s->have_tmap_adj) {   // dense meshes: bulk reductions of the cotangent deposit
+        for (int c = 0; c < 3; ++c) TRY(make_tmap(&s->tmap_adj[c], s->adj[c], s->res, s->ssx, s->sS));
+        TRY(make_tmap(&s->tmap_rho, rho_mesh(s, 0), s->res, s->ssx, s->sS));
+        s->have_tmap_adj = true;
+    }
     float* rho = rho_mesh(s, 0);
     const int pitch = rho_pitch(s);
     const float inv_ns = 1.0f / float(s->nshift);
@@ -1839,7 +1848,8 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
             CUDA_TRY(cudaFuncSetAttribute(djb::k_zpencil_pair<djb::KPhiFn>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, djb::kZSmem));
         }
-        if (s->sorted && s->gsx <= res) {
+        const char* tm = std::getenv("DJB_TMA");   // DJB_TMA=0: boxes by asynchronous copies only
+        if (s->sorted && s->gsx <= res && !(tm && std::strcmp(tm, "0") == 0)) {
             for (int m = 0; m < s->group; ++m) {
                 TRY(make_tmap(&s->tmap[m], s->phi[m], res, s->gsx, s->gS));
                 TRY(make_tmap(&s->tmap_s[m], s->phi[m], res, s->ssx, s->sS));

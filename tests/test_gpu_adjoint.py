@@ -80,6 +80,27 @@ def test_stencils_16_byte_staging_at_1024_mesh(djb, monkeypatch):
     assert rel(g16, g4) < 1e-5
 
 
+def test_vjp_bulk_tensor_boxes_at_1024_mesh(djb, monkeypatch):
+    """On the dense 1024³ meshes the adjoint's brick kernels stage and flush their boxes
+    with bulk tensor copies; with those off (DJB_TMA=0: asynchronous copies and vector
+    reductions, the form the oracle comparisons at small sizes take) the step VJP must
+    agree."""
+    n, res, L = 32, 1024, 1000.0
+    psi = _clustered(n, L, 6, amp=8.0)
+    mom = np.random.default_rng(5).standard_normal((n, n, n, 3)).astype(np.float32)
+    pb = np.random.default_rng(6).standard_normal((n, n, n, 3)).astype(np.float32)
+    mb = np.random.default_rng(7).standard_normal((n, n, n, 3)).astype(np.float32)
+    cfg = djb.PMConfig(res_pm=res, n_part=n, boxsize=L, worder=4, grad_order=6, antialias=1)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("DJB_TMA", flag)
+        with djb.PMSolver(cfg) as S:
+            out[flag] = S.step_vjp(0.01, 0.9, 0.05, 0.01, psi, mom, pb, mb)
+    for a, b in zip(out["1"], out["0"]):
+        assert np.isfinite(a).all()
+        assert rel(a, b) < 1e-5   # float atomics and reductions reorder only
+
+
 def test_step_vjp_vs_oracle(djb):
     from oracle import adjoint as oad
     from oracle import pm as opm
