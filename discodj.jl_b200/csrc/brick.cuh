@@ -486,4 +486,95 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
     }
 }
 
+// Interpolation of three node fields (the force correction on the mesh) to the brick's
+// particles with the mass-assignment weights at their unshifted positions: out_c(p) =
+// scale * sum_n W(X_p - n) f_c(n). One CTA per brick; the brick's deposit boxes of the
+// three fields (rows of sx nodes) are staged together, one bulk tensor copy each where
+// the box does not wrap (`tma` != 0: f is three dense [res]^3 meshes described by
+// tm0..tm2), so each particle's 3 W^3 loads come from shared memory.
+template <int W>
+__global__ void __launch_bounds__(kTileThreads, 2) k_interp3_brick(
+    const float* __restrict__ psi, const float* __restrict__ q1, int n, int64_t np, float L, int res,
+    const float* __restrict__ f, float scale, float* __restrict__ out, int* err, BrickList bl, int sx,
+    const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
+    const __grid_constant__ CUtensorMap tm2, int tma) {
+    extern __shared__ __align__(128) float fbox[];
+    __shared__ __align__(8) uint64_t s_bar;
+    const int b = brick_of_block(bl, blockIdx.x);
+    unsigned start, cnt;
+    brick_range(bl, b, start, cnt);
+    if (cnt == 0) return;
+    const int tid = threadIdx.x;
+    const int64_t cells = int64_t(res) * res * res;
+    const TileBox box = aligned_box(bl, b, bl.sos, bl.sSs, sx);
+    const int bcells = box.plane * box.S[2];
+    const int stride = box_stride(bcells);   // boxes on 128-byte boundaries
+    const bool bulk = tma && box_inside(box, res) && (smem_u32(fbox) & 127u) == 0u;
+    if (bulk) {
+        if (tid == 0) mbar_init(&s_bar, 1);
+        __syncthreads();
+        if (tid == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&s_bar, 3u * unsigned(bcells) * 4u);
+            tma_load_3d(fbox, &tm0, box.o[0], box.o[1], box.o[2], &s_bar);
+            tma_load_3d(fbox + stride, &tm1, box.o[0], box.o[1], box.o[2], &s_bar);
+            tma_load_3d(fbox + 2 * stride, &tm2, box.o[0], box.o[1], box.o[2], &s_bar);
+        }
+        const bool ok = mbar_wait(&s_bar, 0);
+        if (__syncthreads_or(!ok)) {   // the copies never completed: report, do not spin
+            if (tid == 0) atomicOr(err, 8);
+            return;
+        }
+    } else {
+        const bool vec = (res & 3) == 0;
+        for (int c = 0; c < 3; ++c) stage_box_wrapped(fbox + c * stride, f + c * cells, box, res, res, vec);
+        __syncthreads();
+    }
+    const float resf = float(res);
+    LatticeDiv ld;
+    ld.init(n);
+#pragma unroll 1
+    for (unsigned slot = tid; slot < cnt; slot += kTileThreads) {
+        const int64_t p = bl.perm[start + slot];
+        int ijk[3];
+        ld.ijk(p, ijk[0], ijk[1], ijk[2]);
+        float w[3][W];
+        int d[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float gc = grid_coord(psi[p + a * np] + q1[ijk[a]], L, resf, err);
+            const int bb = wbase<W>(gc);
+#pragma unroll
+            for (int o = 0; o < W; ++o) w[a][o] = wk<W>(fabsf(gc - float(bb + WLo<W>::v + o)));
+            d[a] = box_rel(bb + WLo<W>::v, box.o[a], res);
+            if (d[a] < 0 || d[a] > box.S[a] - W) {   // not binned consistently: report, stay in bounds
+                atomicOr(err, 2);
+                d[a] = d[a] < 0 ? 0 : box.S[a] - W;
+            }
+        }
+        float v[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int z = 0; z < W; ++z) {
+            float sy[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int y = 0; y < W; ++y) {
+                const float* row = fbox + ((d[2] + z) * box.S[1] + d[1] + y) * box.P + d[0];
+                float sxv[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+                for (int x = 0; x < W; ++x) {
+                    sxv[0] += w[0][x] * row[x];
+                    sxv[1] += w[0][x] * row[stride + x];
+                    sxv[2] += w[0][x] * row[2 * stride + x];
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) sy[c] += w[1][y] * sxv[c];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] += w[2][z] * sy[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[p + c * np] = scale * v[c];
+    }
+}
+
 }  // namespace djb

@@ -1202,6 +1202,8 @@ int scatter_attrs_w() {
                                   kBrickSmemMax));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_gather_grad_brick<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kBrickSmemMax));
+    CUDA_TRY(cudaFuncSetAttribute(djb::k_interp3_brick<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kBrickSmemMax));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   int(cudaSharedmemCarveoutMaxShared)));
     CUDA_TRY(cudaFuncSetAttribute(djb::k_scatter_brick<W, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1480,6 +1482,33 @@ int fd_vec(const djb_solver* s, int res, int pitch, std::initializer_list<const 
 int nn_correction(djb_solver* s) {
     TRY(djb_nn_set_stream(s->nn, s->stream));
     TRY(djb_nn_apply(s->nn, s->nnf, s->res, s->nnd, DJB_MEM_DEVICE));
+    // brick-owned form when the particles are in brick order and the three fields' deposit
+    // boxes fit two CTAs per SM
+    const int sxI = (s->sS + ((s->sg.brick % 4 == 0) ? (s->sfirst & 3) : 3) + 3) & ~3;
+    const size_t smem = 3 * size_t(djb::box_stride(sxI * s->sS * s->sS)) * 4;
+    if (s->cur_perm && s->tiled && smem <= size_t(kBrickSmemMax)) {
+        const int64_t cells = int64_t(s->res) * s->res * s->res;
+        CUtensorMap tm[3];
+        int tma = 0;
+        if (s->tma && s->phi[0] && sxI <= s->res) {
+            for (int c = 0; c < 3; ++c) TRY(make_tmap(&tm[c], s->nnd + c * cells, s->res, sxI, s->sS));
+            tma = 1;
+        } else {
+            for (int c = 0; c < 3; ++c) tm[c] = s->tmap_s[0];
+        }
+        const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
+#define DJB_INTERPB(W_)                                                                                        \
+    if (s->W == W_)                                                                                            \
+        djb::k_interp3_brick<W_><<<nbricks, djb::kTileThreads, smem, s->stream>>>(                             \
+            s->psi, s->q1, s->n, s->np, s->Lf, s->res, s->nnd, s->nn_out, s->nnacc, s->err, brick_list(s), sxI,  \
+            tm[0], tm[1], tm[2], tma);
+        DJB_INTERPB(2)
+        DJB_INTERPB(3)
+        DJB_INTERPB(4)
+#undef DJB_INTERPB
+        CUDA_TRY(cudaGetLastError());
+        return DJB_OK;
+    }
 #define DJB_INTERP(W_)                                                                                          \
     if (s->W == W_)                                                                                             \
         djb::k_interp3<W_><<<blocks(s->np), kThreads, 0, s->stream>>>(s->psi, s->q1, s->n, s->np, s->Lf, s->res, \
