@@ -57,7 +57,10 @@ constexpr int kRing = DJB_CONV_RING;                   // staged planes
 constexpr int kAccTiles = 16;                          // tile accumulators in tensor memory
 constexpr int kMaxSegment = kAccTiles;                 // z segment length (tiles) at most
 constexpr int kOneCtaSmem = 116 * 1024;                // more than half an SM: one CTA per SM
-constexpr int kEpiGroups = 2;                          // epilogue groups of four warps, alternate tiles
+#ifndef DJB_CONV_EPI
+#define DJB_CONV_EPI 2
+#endif
+constexpr int kEpiGroups = DJB_CONV_EPI;               // epilogue groups of four warps, alternate tiles
 #ifndef DJB_CONV_OSTAGES
 #define DJB_CONV_OSTAGES 4
 #endif
