@@ -855,7 +855,7 @@ struct djb_solver {
     bool have_tmap_adj = false;
     bool tma = false;
     // res == 1024: the dense transforms are batched 2-D transforms of the z planes and
-    // the z stages run fused with Kφ in k_zpencil_kphi (zpencil.cuh); wN = exp(-2πi j/res)
+    // the z stages run fused with Kφ in k_zpencil_pair (zpencil.cuh); wN = exp(-2πi j/res)
     bool zpass = false;
     float2* wN = nullptr;
     float* adj[3] = {nullptr, nullptr, nullptr};  // VJP work meshes (allocated on first use)
