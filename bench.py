@@ -518,6 +518,19 @@ def main():
     roof = dict(bound="hbm", kernel=top, achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                 traffic=traffic, peak_source=f"{peak_kind} hbm_gbs",
                 algorithmic_bytes_per_launch=per_launch_bytes, ms_per_launch=per_launch_ms)
+    # the pipe that does bound the brick interpolation: shared-memory wavefronts (one per SM
+    # clock at most), from the committed ncu count per particle-shift and this run's time
+    pipe = None
+    if top == "gather" and tr and tr.get("smem_wavefronts_per_particle_shift"):
+        wf = tr["smem_wavefronts_per_particle_shift"] * n ** 3 * 2
+        sm_hz = float((clk or {}).get("sm_mhz") or 0) * 1e6
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        if sm_hz > 0:
+            ach = wf / (per_launch_ms / 1e3)
+            pipe = dict(kernel="gather", unit="shared-memory wavefronts/s", wavefronts_per_launch=wf, achieved=ach,
+                        peak=sms * sm_hz, frac=ach / (sms * sm_hz),
+                        source="wavefronts per particle-shift from profiles/traffic.json; peak = SMs x median SM "
+                               "clock of this run (one 128-byte wavefront per clock per SM)")
     phases = {k: dict(ms_per_step=v[0] / args.steps, launches=v[1]) for k, v in prof.items() if v[2]}
     step_roof = dict(algorithmic_bytes=step_bytes, achieved=step_bytes / (step_ms / 1e3) / 1e9, peak=peak,
                      frac=step_bytes / (step_ms / 1e3) / 1e9 / peak, unit="GB/s")
@@ -531,7 +544,7 @@ def main():
         line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                     ms_per_step=step_ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
                     data="synthetic (seeded white noise -> EH P(k) -> 3LPT)",
-                    config=config_block(args.size, n, res, L, lpt, world), roofline=roof,
+                    config=config_block(args.size, n, res, L, lpt, world), roofline=roof, pipe_roofline=pipe,
                     step_roofline=step_roof, phases=phases, cpu_baseline=cpu, e2e=e2e, adjoint=adjoint, nn=nn,
                     nn_corrected=nnc, clocks=clk,
                     gpu_launches=int(sum(v[1] for v in prof.values())),
