@@ -899,6 +899,10 @@ struct djb_solver {
     float* nnf = nullptr;    // 4 res³ meshes (network input)
     float* nnd = nullptr;    // 3 res³ meshes (network output)
     float* nnacc = nullptr;  // 3·np particle corrections
+    int nn_every = 1;        // network schedule (djb_solver_nn_schedule): from step nn_start on,
+    int nn_start = 0;        //   on every nn_every-th step
+    int64_t nn_steps = 0;    // steps taken since the state or the network was set
+    bool nn_valid = false;   // nnacc holds a correction of the current particles
     int64_t bytes = 0;
     std::vector<void*> allocs;
 };
@@ -1320,6 +1324,14 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
     const int64_t nspec = int64_t(s->res) * s->res * nh;
     const bool ik = (s->cfg.grad_order == 0);
     const bool resample = (s->cfg.n_resample > 1);
+    // the network runs from step nn_start on, on every nn_every-th step (and on every
+    // force outside a step); between its evaluations each particle keeps the correction it
+    // was last given; before nn_start the force is uncorrected
+    const bool nn_active = s->nn && (!step || s->nn_steps >= s->nn_start);
+    const bool nn_eval =
+        nn_active && (!step || !s->nn_valid || (s->nn_steps - s->nn_start) % s->nn_every == 0);
+    if (s->nn && step) ++s->nn_steps;
+    if (nn_eval) s->nn_valid = true;
     s->cur_perm = nullptr;
     // the first drift is applied by the binning pass (or the first deposit without the
     // sort), before the network correction reads the positions
@@ -1353,7 +1365,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
             else CUFFT_TRY(cufftExecR2C(s->r2c, mesh, spec));
             s->prof.end(s->stream, PH_R2C, 0);
             // network input, δ: the unshifted density is still in phi[0] after the R2C
-            const bool nn_here = s->nn && first == 0 && m == 0;
+            const bool nn_here = nn_eval && first == 0 && m == 0;
             if (nn_here) {
                 const float f = float(double(s->res) * s->res * s->res / double(s->np));
                 djb::k_mesh_affine<<<grid_for(int64_t(s->res) * s->res * s->res), 256, 0, s->stream>>>(
@@ -1432,7 +1444,7 @@ int force(djb_solver* s, bool step, double dd1, double alpha, double beta, doubl
         a.dd2 = float(dd2);
         a.err = s->err;
         a.perm = s->cur_perm;
-        a.extra = s->nn ? s->nnacc : nullptr;
+        a.extra = nn_active ? s->nnacc : nullptr;
         s->prof.begin(s->stream, PH_GATHER);
         launch_gather(s, a, ns);
         s->prof.end(s->stream, PH_GATHER, 1);
@@ -2134,6 +2146,21 @@ int djb_solver_attach_nn(djb_solver* s, djb_nn* net, double delta_scale, double 
     s->nn_in = float(delta_scale);
     s->nn_fin = float(force_scale);
     s->nn_out = float(out_scale);
+    s->nn_steps = 0;
+    s->nn_valid = false;
+    return DJB_OK;
+}
+
+int djb_solver_nn_schedule(djb_solver* s, int32_t every, int32_t start) {
+    djb::clear_error();
+    if (!s) return fail(DJB_ERR_INVALID, "null solver");
+    if (every < 1 || start < 0) return fail(DJB_ERR_INVALID, "every must be at least 1 and start at least 0");
+    CUDA_TRY(cudaSetDevice(s->cfg.device));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->nn_every = every;
+    s->nn_start = start;
+    s->nn_steps = 0;
+    s->nn_valid = false;
     return DJB_OK;
 }
 
@@ -2228,6 +2255,8 @@ int djb_set_state(djb_solver* s, const float* psi, const float* mom, double mom_
     djb::clear_error();
     if (!s || !psi || !mom) return fail(DJB_ERR_INVALID, "null argument");
     CUDA_TRY(cudaSetDevice(s->cfg.device));
+    s->nn_steps = 0;      // a new state: the next step evaluates the network
+    s->nn_valid = false;
     const size_t count = size_t(3 * s->np);
     TRY(copy_in(s, s->psi, psi, count, mem));
     if (mom_scale == 1.0) {

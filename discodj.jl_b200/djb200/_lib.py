@@ -110,6 +110,7 @@ SIGNATURES = {
     "djb_nn_backward_output_grad": [_P, _P, _P, _I, _I],
     "djb_nn_info": [_P, _IP, _IP, _IP, _IP, _IP],
     "djb_solver_attach_nn": [_P, _P, _D, _D, _D],
+    "djb_solver_nn_schedule": [_P, _I, _I],
     "djb_mesh_interp3": [_P, _P, _P, _P, _I],
     "djb_mesh_deposit3": [_P, _P, _P, _P, _I],
     "djb_state_density_modes": [_P, _I, _IP, _DP],

@@ -53,9 +53,12 @@ def initial_state(cosmo, n: int, boxsize: float, seed: int, device: int = 0):
 
 
 def run(cosmo, psi, pi, *, res: int, boxsize: float, n_steps: int, opts=OPTS, device: int = 0, net=None,
-        scales=None, keep_states: bool = False, timing: bool = False):
-    """BullFrog run from (psi, pi) on a res³ mesh, optionally with an attached network.
-    Returns (final Ψ, final Π, [Ψ after each step] or None, device ms per step or None)."""
+        scales=None, keep_states: bool = False, timing: bool = False, every: int = 1, start: int = 0):
+    """BullFrog run from (psi, pi) on a res³ mesh, optionally with an attached network
+    (from step `start` on, on every `every`-th step: `PMSolver.nn_schedule`). Returns
+    (final Ψ, final Π, [Ψ after each step] or None, device ms per step or None); the timing
+    covers every step but the first two (one-time work-area allocations), which a run with
+    a schedule repeats untimed first, so that the time is the mean over the whole run."""
     import torch
     n = int(psi.shape[1])
     co = stepper_coefficients(cosmo, "bullfrog", A_INI, 1.0, n_steps)
@@ -66,10 +69,19 @@ def run(cosmo, psi, pi, *, res: int, boxsize: float, n_steps: int, opts=OPTS, de
         if net is not None:
             net.set_stream(stream.cuda_stream)
             S.attach_nn(net, *scales)
+            S.nn_schedule(every, start)
+        scheduled = net is not None and (every > 1 or start > 0)
+        if timing and scheduled:
+            # an untimed pass of the whole schedule takes the one-time allocations; the
+            # timed pass below then averages over every step of the run
+            S.set_state(psi, pi)
+            for k in range(n_steps):
+                S.step(co["ddrift1"][k], co["alpha"][k], co["beta"][k], co["ddrift2"][k])
         S.set_state(psi, pi)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        warm = 2 if timing else 0    # the first steps carry one-time work-area allocations
+        # the first steps carry one-time work-area allocations
+        warm = (0 if scheduled else 2) if timing else 0
         for k in range(n_steps):
             if k == warm:
                 torch.cuda.synchronize(device)
@@ -199,7 +211,7 @@ def train(cosmo, *, n=128, boxsize=250.0, seeds=range(64), snapshots=20, epochs=
 
 
 def evaluate(cosmo, net, scales, *, n, boxsize, seeds, n_steps=20, opts_lo=OPTS_LO, opts_hi=OPTS, device=0,
-             bins=32, timing=False):
+             bins=32, timing=False, every=1, start=0):
     """Plain 1×, corrected 1× and plain 2× runs from each held-out seed. Returns per-bin
     P(k) ratios to the 2× run (mean over seeds) for k < k_Nyq/2 of the 1× mesh, their
     largest deviations, and (timing) device ms per step of the corrected 1× and plain 2×."""
@@ -213,7 +225,7 @@ def evaluate(cosmo, net, scales, *, n, boxsize, seeds, n_steps=20, opts_lo=OPTS_
         p1, _, _, t1 = run(cosmo, p0, m0, res=n, boxsize=boxsize, n_steps=n_steps, opts=opts_lo, device=device,
                            timing=timing)
         pc, _, _, tc = run(cosmo, p0, m0, res=n, boxsize=boxsize, n_steps=n_steps, opts=opts_lo, device=device,
-                           net=net, scales=scales, timing=timing)
+                           net=net, scales=scales, timing=timing, every=every, start=start)
         k, P2, nm = state_pk(p2, res=n, boxsize=boxsize, bins=bins, device=device)
         _, P1, _ = state_pk(p1, res=n, boxsize=boxsize, bins=bins, device=device)
         _, Pc, _ = state_pk(pc, res=n, boxsize=boxsize, bins=bins, device=device)

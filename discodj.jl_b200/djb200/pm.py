@@ -222,6 +222,12 @@ class PMSolver:
                                        float(force_scale), float(out_scale)))
         self._net = net   # the network must outlive its attachment
 
+    def nn_schedule(self, every: int = 1, start: int = 0):
+        """The attached network corrects the force from step `start` on, running on every
+        `every`-th of those steps; in between, each particle keeps the correction it was
+        last given (`djb_solver_nn_schedule`)."""
+        check(lib.djb_solver_nn_schedule(self._h, int(every), int(start)))
+
     def mesh_interp3(self, psi, mesh3):
         """(3,n,n,n) device tensor of the W-order interpolation of three res³ meshes
         ((3,res,res,res) device tensor [c][z][y][x]) at X = q + psi (device, native layout)."""

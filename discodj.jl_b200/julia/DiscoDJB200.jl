@@ -281,6 +281,9 @@ particles (djb_solver_attach_nn); `attach_nn!(S, nothing)` detaches.
 attach_nn!(S::PMSolverB200, net::ForceNetB200, scales) =
     _check(ccall((:djb_solver_attach_nn, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Float64, Float64, Float64),
                  S.handle, net.handle, scales[1], scales[2], scales[3]))
+"""    nn_schedule!(S; every=1, start=0)   (djb_solver_nn_schedule)"""
+nn_schedule!(S::PMSolverB200; every::Integer=1, start::Integer=0) =
+    _check(ccall((:djb_solver_nn_schedule, LIB), Cint, (Ptr{Cvoid}, Int32, Int32), S.handle, every, start))
 attach_nn!(S::PMSolverB200, ::Nothing) =
     _check(ccall((:djb_solver_attach_nn, LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Float64, Float64, Float64),
                  S.handle, C_NULL, 1.0, 1.0, 1.0))

@@ -335,6 +335,12 @@ DJB_API int djb_nn_info(const djb_nn* h, int32_t* layers, int32_t* cin, int32_t*
  * network runs on the solver's stream (its stream is set to the solver's at every force). */
 DJB_API int djb_solver_attach_nn(djb_solver* s, djb_nn* net, double delta_scale, double force_scale,
                                  double out_scale);
+/* Network schedule: steps of djb_step/djb_run are counted from djb_set_state,
+ * djb_solver_attach_nn or this call (0-based); the attached network corrects the force
+ * from step `start` on (earlier steps are uncorrected) and runs on every `every`-th of
+ * those steps (the first always), each particle keeping the correction it was last given
+ * in between; djb_pm_acceleration always runs it. Default: every = 1, start = 0. */
+DJB_API int djb_solver_nn_schedule(djb_solver* s, int32_t every, int32_t start);
 /* out (n,n,n,3) = the solver's W-order interpolation (pm.jl:344-364, no shift) of the three
  * res^3 meshes mesh3 ([channel][z][y][x]) at X = q + psi. */
 DJB_API int djb_mesh_interp3(djb_solver* s, const float* psi, const float* mesh3, float* out, int32_t mem);

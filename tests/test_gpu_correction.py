@@ -112,6 +112,42 @@ def test_attached_network_adds_its_interpolated_correction(djb, cosmo):
     assert rel(again.cpu().numpy(), plain.cpu().numpy()) < 1e-6      # detached: plain force again
 
 
+def test_network_schedule(djb, cosmo):
+    """djb_solver_nn_schedule: before `start` the steps are uncorrected (equal to the plain
+    run), from it on every step is corrected; with every = 2 the steps in between reuse
+    the particles' last correction (and differ from both)."""
+    import torch
+
+    from djb200 import correction, stepper_coefficients
+    from djb200.nn import ForceNet
+    n, L, steps = 32, 62.5, 4
+    p0, m0 = correction.initial_state(cosmo, n, L, seed=5)
+    co = stepper_coefficients(cosmo, "bullfrog", correction.A_INI, 1.0, steps)
+    cfg = djb.PMConfig(res_pm=n, n_part=n, boxsize=L, **correction.OPTS_LO)
+
+    def run(net, every=1, start=0):
+        with djb.PMSolver(cfg) as S:
+            if net is not None:
+                S.attach_nn(net, 0.3, 2.0, 0.05)
+                S.nn_schedule(every, start)
+            S.set_state(p0, m0)
+            for k in range(steps):
+                S.step(co["ddrift1"][k], co["alpha"][k], co["beta"][k], co["ddrift2"][k])
+            p, _ = S.get_state(device=True)
+        return p.cpu().numpy()
+
+    with ForceNet(seed=11) as net:
+        plain = run(None)
+        late = run(net, 1, steps)         # never active within the run
+        full = run(net, 1, 0)
+        half = run(net, 2, 0)
+        tail = run(net, 1, 2)
+    assert np.array_equal(late, plain)
+    assert rel(full, plain) > 1e-4
+    for x in (half, tail):
+        assert rel(x, plain) > 1e-6 and rel(x, full) > 1e-6
+
+
 @pytest.mark.slow
 def test_training_gains_over_plain_pm(djb, cosmo, capsys):
     """64³ particles, L = 125 (the resolution of the 128³ / L = 250 training set):
