@@ -113,9 +113,10 @@ def test_attached_network_adds_its_interpolated_correction(djb, cosmo):
 
 
 def test_network_schedule(djb, cosmo):
-    """djb_solver_nn_schedule: before `start` the steps are uncorrected (equal to the plain
-    run), from it on every step is corrected; with every = 2 the steps in between reuse
-    the particles' last correction (and differ from both)."""
+    """djb_solver_nn_schedule: before `start` the steps are uncorrected (the plain run, up
+    to the reordering of float reductions), from it on every step is corrected; with
+    every = 2 the steps in between reuse the particles' last correction (and differ from
+    both)."""
     import torch
 
     from djb200 import correction, stepper_coefficients
@@ -142,10 +143,12 @@ def test_network_schedule(djb, cosmo):
         full = run(net, 1, 0)
         half = run(net, 2, 0)
         tail = run(net, 1, 2)
-    assert np.array_equal(late, plain)
-    assert rel(full, plain) > 1e-4
+    # two runs of the same force agree to float-reduction reordering only
+    noise = max(rel(late, plain), 1e-7)
+    assert noise < 1e-5
+    assert rel(full, plain) > 100 * noise
     for x in (half, tail):
-        assert rel(x, plain) > 1e-6 and rel(x, full) > 1e-6
+        assert rel(x, plain) > 10 * noise and rel(x, full) > 10 * noise
 
 
 @pytest.mark.slow
