@@ -34,6 +34,15 @@ def test_library_exports_every_declared_symbol():
     assert sorted(_lib.SIGNATURES) == syms
 
 
+def test_julia_binding_calls_only_declared_symbols():
+    """Every `ccall` of the Julia host binding names an entry point of the header (the
+    binding is not executed here: Julia is not installed)."""
+    jl = open(os.path.join(ROOT, "discodj.jl_b200", "julia", "DiscoDJB200.jl")).read()
+    called = set(re.findall(r"ccall\(\(:(djb_\w+)", jl))
+    assert len(called) >= 15
+    assert called <= set(declared_symbols()), sorted(called - set(declared_symbols()))
+
+
 def test_version_and_error_text():
     assert b"sm_100a" in djb200.lib.djb_version()
     assert djb200.lib.djb_last_error() is not None
