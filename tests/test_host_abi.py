@@ -43,6 +43,29 @@ def test_julia_binding_calls_only_declared_symbols():
     assert called <= set(declared_symbols()), sorted(called - set(declared_symbols()))
 
 
+def test_lpt_work_area_sizes_and_rejections():
+    """djb_lpt_ics_work_bytes (no device needed): the third order needs more than the
+    second, the area grows with n, and invalid sizes and orders are rejected."""
+    import ctypes as C
+
+    from djb200 import _lib
+    out = C.c_int64(0)
+
+    def wb(n, order, npk=64):
+        rc = _lib.lib.djb_lpt_ics_work_bytes(n, order, npk, C.byref(out))
+        return rc, out.value
+
+    rc2, b2 = wb(32, 2)
+    rc3, b3 = wb(32, 3)
+    assert rc2 == rc3 == 0 and 0 < b2 < b3
+    ext = 48
+    assert b3 >= 4 * ext ** 3 * 14       # P, Q, mu2 and two ext spectra
+    assert wb(64, 3)[1] > 7 * b3
+    for n, order in ((30, 2), (32, 4), (32, 1)):
+        assert wb(n, order)[0] == _lib.DJB_ERR_INVALID
+    assert wb(32, 2, npk=1)[0] == _lib.DJB_ERR_INVALID
+
+
 def test_version_and_error_text():
     assert b"sm_100a" in djb200.lib.djb_version()
     assert djb200.lib.djb_last_error() is not None
