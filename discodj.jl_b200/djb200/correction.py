@@ -16,7 +16,7 @@ Training uses only pairs that this PM code generates:
   relative to the residual's mean square. Its gradient with respect to the network's
   output mesh is the transpose of the interpolation (`djb_mesh_deposit3`), which the
   network back-propagates (`djb_nn_backward_output_grad`); Adam on float32 weights.
-The plain PM step stays the fallback (detach) and the judge: evaluation runs plain 1×,
+The plain PM step stays the fallback (detach) and the yardstick: evaluation runs plain 1×,
 corrected 1× and plain 2× from the same held-out ICs and compares their P(k) at a = 1
 (CIC deposit on the 1× mesh, float64 shells) for k < k_Nyq/2 of the 1× mesh.
 
