@@ -12,7 +12,12 @@ library. Restates:
   (src/ics/grf.jl:118-144),
 * the first-order LPT shape ψ₁ = −∇φ with the Nyquist derivative zeroed
   (src/lpt/nlpt_core.jl:56-67), Ψ = D(a)·ψ₁ and Π = dΨ/dD = ψ₁
-  (src/nbody/run_nbody.jl:180-208 at n_order = 1).
+  (src/nbody/run_nbody.jl:180-208 at n_order = 1),
+* the second- and third-order shapes of `compute_core` (src/lpt/nlpt_core.jl:95-311,
+  EdS growth) with its 3/2-padded products, written here through the invariants of the
+  displacement-gradient matrices A = ∂ψ₁ and B = ∂ψ₂ (μ₂(A,B) = tr A tr B − Σ A_ab B_ab,
+  μ₃ = det A, the transverse vector from the antisymmetric part of A·B) rather than the
+  reference's index tables, as an independent check of the restatements that use them.
 White noise comes from numpy's PCG64 generator (the reference's N-GenIC/GSL noise
 is not restated). Particle fields are (n,n,n,3) indexed [i,j,k,c].
 """
@@ -106,7 +111,7 @@ def zeldovich_shape(fphi: np.ndarray, boxsize: float) -> np.ndarray:
     ks = (kf[:, None, None], kf[None, :, None], kh[None, None, :])
     out = np.empty((n, n, n, 3))
     for c in range(3):
-        out[..., c] = np.fft.irfftn(-(1j * ks[c]) * fphi, s=(n, n, n))
+        out[..., c] = np.fft.irfftn(-(1j * ks[c]) * fphi, s=(n, n, n), axes=(0, 1, 2))
     return out
 
 
@@ -116,3 +121,68 @@ def zeldovich_ics(n: int, boxsize: float, D: float, *, Omega_c, Omega_b, h, n_s,
     pk = linear_power_spectrum(Omega_c, Omega_b, h, n_s, sigma8)
     psi1 = zeldovich_shape(fphi_from_white(white, boxsize, pk), boxsize)
     return D * psi1, psi1
+
+
+# ── second and third order (compute_core, nlpt_core.jl:95-311) ─────────────────────
+def _axes_k(n: int, boxsize: float):
+    """ik derivative factors (Nyquist zeroed) of the full, full and half axes, and k²."""
+    dk = 2 * math.pi / boxsize
+    kf = np.fft.fftfreq(n, d=1.0 / n) * dk
+    kh = np.arange(n // 2 + 1, dtype=np.float64) * dk
+    k2 = kf[:, None, None] ** 2 + kf[None, :, None] ** 2 + kh[None, None, :] ** 2
+    kfz, khz = kf.copy(), kh.copy()
+    kfz[n // 2] = 0.0
+    khz[-1] = 0.0
+    return (kfz[:, None, None], kfz[None, :, None], khz[None, None, :]), k2
+
+
+def _embed(f: np.ndarray, n: int, e: int) -> np.ndarray:
+    """Half spectrum of the n grid into the e grid (Nyquist planes dropped), × (e/n)³."""
+    h = n // 2
+    out = np.zeros((e, e, e // 2 + 1), dtype=complex)
+    src = np.r_[0:h, h + 1:n]
+    dst = np.r_[0:h, e - h + 1:e]
+    out[np.ix_(dst, dst, np.arange(h))] = f[np.ix_(src, src, np.arange(h))]
+    return out * (e / n) ** 3
+
+
+def _crop(f: np.ndarray, n: int, e: int) -> np.ndarray:
+    """The inverse of _embed on the kept modes (× (n/e)³), zero on the Nyquist planes."""
+    h = n // 2
+    out = np.zeros((n, n, n // 2 + 1), dtype=complex)
+    src = np.r_[0:h, e - h + 1:e]
+    dst = np.r_[0:h, h + 1:n]
+    out[np.ix_(dst, dst, np.arange(h))] = f[np.ix_(src, src, np.arange(h))]
+    return out * (n / e) ** 3
+
+
+def lpt_shapes(fphi: np.ndarray, boxsize: float, order: int = 3):
+    """[ψ₁, ψ₂(, ψ₃)] as (n,n,n,3) float64 fields for φ(k) on the half spectrum."""
+    n = fphi.shape[0]
+    e = 3 * n // 2
+    d, k2 = _axes_k(n, boxsize)
+    with np.errstate(divide="ignore"):
+        il = np.where(k2 > 0, -1.0 / np.where(k2 > 0, k2, 1.0), -1.0)
+    real = lambda f: np.fft.irfftn(f, s=(e, e, e), axes=(0, 1, 2))
+    spec = lambda x: _crop(np.fft.rfftn(x), n, e)
+    psi1 = [-(1j * d[a]) * fphi for a in range(3)]
+    # A[a][b] = ∂_b ψ₁_a on the padded grid
+    A = [[real(_embed((1j * d[b]) * psi1[a], n, e)) for b in range(3)] for a in range(3)]
+    trA = A[0][0] + A[1][1] + A[2][2]
+    mu2 = 0.5 * (trA * trA - sum(A[a][b] * A[b][a] for a in range(3) for b in range(3)))
+    fl2 = (-3.0 / 7.0) * spec(mu2)
+    psi2 = [il * (1j * d[a]) * fl2 for a in range(3)]
+    shapes = [psi1, psi2]
+    if order >= 3:
+        B = [[real(_embed((1j * d[b]) * psi2[a], n, e)) for b in range(3)] for a in range(3)]
+        trB = B[0][0] + B[1][1] + B[2][2]
+        mu2ab = trA * trB - sum(A[b][a] * B[a][b] for a in range(3) for b in range(3))
+        det = (A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0])
+               + A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]))
+        AB = [[sum(A[i][r] * B[i][c] for i in range(3)) for c in range(3)] for r in range(3)]
+        fl3 = spec((-5.0 / 9.0) * mu2ab - (1.0 / 3.0) * det)
+        ct = [spec((1.0 / 3.0) * (AB[(c + 1) % 3][(c + 2) % 3] - AB[(c + 2) % 3][(c + 1) % 3])) for c in range(3)]
+        psi3 = [il * ((1j * d[a]) * fl3 - ((1j * d[(a + 1) % 3]) * ct[(a + 2) % 3] - (1j * d[(a + 2) % 3]) * ct[(a + 1) % 3]))
+                for a in range(3)]
+        shapes.append(psi3)
+    return [np.stack([np.fft.irfftn(c, s=(n, n, n), axes=(0, 1, 2)) for c in comps], axis=-1) for comps in shapes]

@@ -117,3 +117,35 @@ def test_oracle_zeldovich_shape_matches_fixture(golden):
     from oracle import ics as oi
     fphi = golden["ics/fphi_re"] + 1j * golden["ics/fphi_im"]
     assert rel(oi.zeldovich_shape(fphi, 100.0), golden["ics/psi1"]) < 1e-12
+
+
+def test_oracle_2lpt_matches_fixture(golden, cosmo):
+    """The oracle's invariant-form nLPT (oracle/ics.py `lpt_shapes`) at second order gives
+    the fixture's 2LPT Ψ, Π at a = 0.05 from its fphi (tolerance 1e-12)."""
+    from oracle import ics as oi
+    fphi = golden["ics/fphi_re"] + 1j * golden["ics/fphi_im"]
+    psi1, psi2 = oi.lpt_shapes(fphi, 100.0, order=2)
+    tabs = cz.compute_timetables(cosmo)
+    D = cz.Dplus(tabs, 0.05)
+    assert rel(D * psi1 + D * D * psi2, golden["ics/psi_ini"]) < 1e-12
+    assert rel(psi1 + 2 * D * psi2, golden["ics/pi_ini"]) < 1e-12
+
+
+@pytest.mark.parametrize("n", [16, 32])
+def test_oracle_3lpt_pins_the_index_table_restatement(golden, n):
+    """The third order has no golden vector; the oracle's invariant form (μ₂(A,B) =
+    tr A tr B − Σ A_ba B_ab, μ₃ = det A, the transverse part from A·B − (A·B)ᵀ) and the
+    package's restatement with the reference's index tables (`djb200.ics.compute_core`,
+    whose third-order shape the GPU generator is tested against) agree at round-off."""
+    import torch
+
+    from djb200 import ics
+    from oracle import ics as oi
+    rng = np.random.default_rng(n)
+    white = rng.standard_normal((n, n, n))
+    pk = oi.linear_power_spectrum(0.261, 0.049, 0.677, 0.965, 0.81)
+    fphi = oi.fphi_from_white(white, 0.5 * n * 2.0, pk)
+    ref = oi.lpt_shapes(fphi, 0.5 * n * 2.0, order=3)
+    got = ics.compute_core(torch.from_numpy(fphi), 0.5 * n * 2.0, n_order=3)
+    for m in (1, 2, 3):
+        assert rel(got[f"psi_{m}"].numpy(), ref[m - 1]) < 1e-12
