@@ -369,12 +369,12 @@ DJB_API int djb_selftest_bounded_wait(int32_t device, int32_t arrive, int64_t li
  * exit); more bins are rejected with DJB_ERR_INVALID. The call allocates no
  * device memory and calls no allocating library routine. The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) and caches
- * it, so make that first call before any stream capture begins. All calls share
+ * it. All calls share
  * the one array, which keeps the last call's contents (each call clears the sums
  * it uses): calls that overlap on the GPU, on different streams or threads, race.
  * Runs on `stream` (a cudaStream_t, NULL = legacy default) of `device`. Every call
  * copies the sums into host stack arrays and synchronises `stream` before it
- * returns. The calling thread's current device is the same after the call as
+ * returns, so no call can be recorded into a CUDA graph. The calling thread's current device is the same after the call as
  * before it. Same results as djb_power_spectrum for the same field. */
 DJB_API int djb_power_spectrum_shells_noalloc(const void* spectrum, int32_t res, double boxsize,
                                               int32_t bins, int32_t logarithmic, double scale2,
