@@ -328,7 +328,11 @@ __device__ __forceinline__ void stage_box_wrapped(float* sbox, const float* __re
 // the kick and drift. The shifts are the outer loop: the brick's box is staged once per
 // shift for all of its particles, and the sums over the shifts go through the
 // acceleration array (the last shift applies the mean, the correction and the
-// kick-drift). `tma` != 0: the potentials are dense [res]^3 meshes (pitch == res)
+// kick-drift). With `A.part` (6 blocks of np floats) they go through it instead, in
+// sorted order, together with a copy of Ψ made in the call's first shift: a thread
+// visits the same sorted positions in every shift of a force call (the same `perm`,
+// the same slots), so it reads back only what it wrote, and its accesses are coalesced
+// where the particle-order ones are scattered. `tma` != 0: the potentials are dense [res]^3 meshes (pitch == res)
 // described by tm0/tm1 (box sx x S x S); boxes that do not wrap are then fetched with one
 // bulk tensor copy.
 template <int W, int R, int NS>
@@ -380,10 +384,15 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
         const bool finish = A.last && g == NS - 1;  // mean, correction, kick-drift
 #pragma unroll 1
         for (unsigned slot = tid; slot < cnt; slot += kTileThreads) {
-            const int64_t p = bl.perm[start + slot];
+            const int64_t at = int64_t(start) + slot;  // sorted position: this thread's in every shift
+            const int64_t p = bl.perm[at];
             int i, j, k;
             ld.ijk(p, i, j, k);
-            const float ps[3] = {A.psi[p], A.psi[p + np], A.psi[p + 2 * np]};
+            // after the call's first shift, Ψ comes from the sorted copy (coalesced)
+            const bool from_part = A.part && !first_sum;
+            const float ps[3] = {from_part ? A.part[at + 3 * np] : A.psi[p],
+                                 from_part ? A.part[at + 4 * np] : A.psi[p + np],
+                                 from_part ? A.part[at + 5 * np] : A.psi[p + 2 * np]};
             const float X[3] = {ps[0] + A.q1[i], ps[1] + A.q1[j], ps[2] + A.q1[k]};
             float w[3][W], u[3][E];
             int d[3];
@@ -453,9 +462,15 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
             }
             float a3[3] = {sX, sY, sZ};
             if (!first_sum) {
-                a3[0] += A.acc[p];
-                a3[1] += A.acc[p + np];
-                a3[2] += A.acc[p + 2 * np];
+                if (A.part) {
+                    a3[0] += A.part[at];
+                    a3[1] += A.part[at + np];
+                    a3[2] += A.part[at + 2 * np];
+                } else {
+                    a3[0] += A.acc[p];
+                    a3[1] += A.acc[p + np];
+                    a3[2] += A.acc[p + 2 * np];
+                }
             }
             if (finish) {
                 if (A.divide) {
@@ -476,10 +491,16 @@ __global__ void __launch_bounds__(kTileThreads, DJB_BRICK_GATHER_BLOCKS) k_gathe
                     A.mom[p + c * np] = m;
                     A.psi[p + c * np] = ps[c] + A.dd2 * m;
                 }
-            } else {
+            } else if (finish || !A.part) {
                 A.acc[p] = a3[0];
                 A.acc[p + np] = a3[1];
                 A.acc[p + 2 * np] = a3[2];
+            } else {  // partial sums (and, after the first shift, Ψ) in sorted order
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    A.part[at + c * np] = a3[c];
+                    if (first_sum) A.part[at + (3 + c) * np] = ps[c];
+                }
             }
         }
         __syncthreads();  // the box is read before the next shift's copy

@@ -399,6 +399,7 @@ struct GatherArgs {
     int* err;
     const int* perm;    // brick-sorted particle order for the tiled kernels (null: Lagrangian tiles)
     const float* extra; // (3 blocks of np) added to the final acceleration, or null (network correction)
+    float* part;        // brick interpolation: partial sums and Ψ in sorted order (6 blocks of np), or null
 };
 
 template <int W, int R, int NS>
@@ -888,6 +889,7 @@ struct djb_solver {
     unsigned* bsum = nullptr;
     uint2* keyrank = nullptr;
     int* perm = nullptr;
+    float* part = nullptr;  // brick interpolation's partial sums and Ψ in sorted order (6 np floats), or null
     const int* cur_perm = nullptr;  // order used by the tiled kernels of the current force call
     int* err = nullptr;
     bool have_state = false;
@@ -1153,12 +1155,14 @@ void launch_gather_wr(djb_solver* s, const djb::GatherArgs& a, int ns) {
         const size_t smem = gather_smem(s);
         const unsigned nbricks = unsigned(s->sg.nb) * s->sg.nb * s->sg.nb;
         const int tma = (s->tma && a.mesh[0] == s->phi[0]) ? 1 : 0;
+        djb::GatherArgs ag = a;
+        ag.part = (a.perm == s->perm) ? s->part : nullptr;
         if (ns == 1)
             djb::k_gather_brick<W, RR, 1><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
-                a, brick_list(s), s->tmap[0], s->tmap[0], tma);
+                ag, brick_list(s), s->tmap[0], s->tmap[0], tma);
         else
             djb::k_gather_brick<W, RR, 2><<<nbricks, djb::kTileThreads, smem, s->stream>>>(
-                a, brick_list(s), s->tmap[0], s->tmap[1], tma);
+                ag, brick_list(s), s->tmap[0], s->tmap[1], tma);
         return;
     }
     if (R > 0 && s->tiled) {
@@ -1837,6 +1841,11 @@ int create(const djb_pm_config* cfg, djb_solver** out) {
         TRY(dmalloc(s, (void**)&s->bsum, sizeof(unsigned) * size_t(s->nscan)));
         TRY(dmalloc(s, (void**)&s->keyrank, sizeof(uint2) * size_t(s->np)));
         TRY(dmalloc(s, (void**)&s->perm, sizeof(int) * size_t(s->np)));
+        // sorted-order partial sums of the brick interpolation (several shifts);
+        // DJB_GATHER_PART=0: through the acceleration array in particle order
+        const char* gp = std::getenv("DJB_GATHER_PART");
+        if (s->R > 0 && s->nshift > 1 && !(gp && std::strcmp(gp, "0") == 0))
+            TRY(dmalloc(s, (void**)&s->part, 6 * sizeof(float) * size_t(s->np)));
     }
     CUDA_TRY(cudaMemset(s->err, 0, sizeof(int)));
     size_t work = 0;
