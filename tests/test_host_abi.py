@@ -167,3 +167,59 @@ def test_3lpt_shapes_are_transverse_free_at_second_order_and_scale_cubically(gol
     assert rel(b["psi_2"].numpy(), 4.0 * a["psi_2"].numpy()) < 1e-12
     assert rel(b["psi_3"].numpy(), 8.0 * a["psi_3"].numpy()) < 1e-12
     assert float(a["psi_3"].abs().max()) > 0
+
+
+def _eds_growth_known_answers(D1, Dda, D2, D3):
+    """The reference's growth known answers (test/runtests.jl:40-54): EdS-like growth at
+    high redshift, D(0.04)/D(0.02) = 2 within 0.05 and f(0.02) = 1 within 0.05; the
+    higher-order growth factors at their EdS limits at a = 0.01 within 2%
+    (D2 = -3/7 D1², D3a = 1/3 D1³, D3b = -10/21 D1³, D3c = 1/7 D1³); D2(1) < 0."""
+    assert abs(D1(0.04) / D1(0.02) - 2.0) < 0.05
+    assert abs(0.02 * Dda(0.02) / D1(0.02) - 1.0) < 0.05
+    a = 0.01
+    d1 = D1(a)
+    assert abs(D2(a) / (-3 / 7 * d1 ** 2) - 1) < 2e-2
+    for name, coef in (("D3a", 1 / 3), ("D3b", -10 / 21), ("D3c", 1 / 7)):
+        assert abs(D3(name, a) / (coef * d1 ** 3) - 1) < 2e-2, name
+    assert D2(1.0) < 0
+
+
+def test_growth_known_answers_library_and_oracle():
+    from oracle import cosmology as cz
+    c = djb200.Cosmology("Planck18EEBAOSN")
+    at = c.table("a")
+    _eds_growth_known_answers(c.Dplus, c.growth_Dplusda, c.D2plus,
+                              lambda name, x: float(np.interp(x, at, c.table(name))))
+    o = cz.compute_timetables(cz.Cosmology.named("Planck18EEBAOSN"))
+    _eds_growth_known_answers(lambda x: cz.Dplus(o, x), lambda x: cz.growth_Dplusda(o, x),
+                              lambda x: cz.D2plus(o, x),
+                              lambda name, x: float(np.interp(x, o.a_table, getattr(o, name + "_table"))))
+
+
+def test_transfer_and_sigma8_known_answers():
+    """The reference's transfer and linear-P(k) known answers (test/runtests.jl:56-86):
+    the Eisenstein-Hu T(k) lies in (0, 1] and tends to 1 at k = 1e-3 h/Mpc (within 0.05);
+    σ8 integrated back from the P(k) table with the 8 Mpc/h top hat (trapezoid in k)
+    is the cosmology's σ8 within 1%. For the package's generator and the oracle's."""
+    import math
+
+    from djb200 import ics
+    from oracle import ics as oi
+    p = djb200.Cosmology("Planck18EEBAOSN").params
+    p = p() if callable(p) else p
+    k = 10.0 ** np.linspace(-3, 1, 100)
+    tables = []
+    for T, (kk, pk) in ((ics.eisenstein_hu(p, k), ics.linear_power_spectrum(p)),
+                        (oi.eisenstein_hu(p["Omega_c"], p["Omega_b"], p["h"], k),
+                         oi.linear_power_spectrum(p["Omega_c"], p["Omega_b"], p["h"], p["n_s"], p["sigma8"]))):
+        assert np.all((T > 0) & (T <= 1.0))
+        assert abs(T[0] - 1.0) < 0.05
+        assert np.all(pk > 0)
+        x = kk * 8.0
+        W = 3 * (np.sin(x) - x * np.cos(x)) / x ** 3
+        W[x < 1e-3] = 1.0
+        integ = kk ** 2 * pk * W ** 2 / (2 * math.pi ** 2)
+        s8 = math.sqrt(np.sum(0.5 * (integ[:-1] + integ[1:]) * np.diff(kk)))
+        assert abs(s8 - p["sigma8"]) / p["sigma8"] < 0.01
+        tables.append(pk)
+    assert rel(tables[0], tables[1]) < 1e-12
