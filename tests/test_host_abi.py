@@ -223,3 +223,54 @@ def test_transfer_and_sigma8_known_answers():
         assert abs(s8 - p["sigma8"]) / p["sigma8"] < 0.01
         tables.append(pk)
     assert rel(tables[0], tables[1]) < 1e-12
+
+
+@pytest.mark.parametrize("generator", ["package", "oracle"])
+def test_lpt_known_answers(generator):
+    """The reference's IC known answers (test/runtests.jl:121-171) at 16³, L = 100, for
+    the package's CPU generator (white noise -> φ -> compute_core) and the oracle's
+    invariant-form shapes: 1LPT has no bulk motion (|mean Ψ_x| < 0.1); rms Ψ grows as
+    D ∝ a in matter domination (rms(a=0.04)/rms(a=0.02) = 2 within 0.05); 2LPT differs
+    from 1LPT at a = 0.02, by less than 5% of the rms; positions mod(q + Ψ, L) at a = 0.1
+    lie in [0, L)."""
+    import torch
+
+    from djb200 import ics
+    from oracle import ics as oi
+    n, L = 16, 100.0
+    c = djb200.Cosmology("Planck18EEBAOSN")
+    p = c.params() if callable(c.params) else c.params
+    fphi = ics.white_noise_to_fphi(ics.white_noise(42, n), L, ics.linear_power_spectrum(p))
+    if generator == "package":
+        shp = {k: v.numpy() for k, v in ics.compute_core(fphi, L, n_order=2).items()}
+        s1, s2 = shp["psi_1"], shp["psi_2"]
+    else:
+        s1, s2 = oi.lpt_shapes(fphi.numpy(), L, order=2)
+
+    def psi(a, order):
+        D = c.Dplus(a)
+        return D * s1 + (D * D * s2 if order == 2 else 0.0)
+
+    rms = lambda x: float(np.sqrt(np.mean(x ** 2)))
+    assert abs(float(np.mean(psi(0.02, 1)[..., 0]))) < 0.1
+    assert abs(rms(psi(0.04, 1)) / rms(psi(0.02, 1)) - 2.0) < 0.05
+    frac = rms(psi(0.02, 1) - psi(0.02, 2)) / rms(psi(0.02, 1))
+    assert 0 < frac < 0.05
+    q = (np.stack(np.meshgrid(*(np.arange(n),) * 3, indexing="ij"), axis=-1)) * (L / n)
+    pos = np.mod(q + psi(0.1, 1), L)
+    assert np.all((pos >= 0) & (pos < L))
+
+
+def test_power_spectrum_white_noise_known_answer():
+    """The reference's P(k) known answer (test/runtests.jl:175-187) for the oracle's
+    `evaluate_power_spectrum` (the checker of the library's P(k)): white noise on 32³,
+    L = 100, 10 bins: 10 values, P ≥ 0, bin centres increasing, and the mean of the
+    non-empty bins within a factor 2 of the shot noise V/N (not V²/N)."""
+    from oracle import power as opw
+    rng = np.random.default_rng(0)
+    res, L = 32, 100.0
+    k, pk, nm = opw.evaluate_power_spectrum(rng.standard_normal((res, res, res)), L, bins=10)
+    assert len(k) == 10 and np.all(pk >= 0) and np.all(np.diff(k) > 0)
+    Vn = L ** 3 / res ** 3
+    nz = pk[pk > 0]
+    assert 0.5 * Vn < nz.mean() < 2.0 * Vn
