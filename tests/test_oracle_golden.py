@@ -149,3 +149,26 @@ def test_oracle_3lpt_pins_the_index_table_restatement(golden, n):
     got = ics.compute_core(torch.from_numpy(fphi), 0.5 * n * 2.0, n_order=3)
     for m in (1, 2, 3):
         assert rel(got[f"psi_{m}"].numpy(), ref[m - 1]) < 1e-12
+
+
+def test_oracle_plane_wave_linear_growth(cosmo):
+    """nbody_parity_tests.jl:68-90 on the float64 oracle, at the reference's own bars: a
+    1e-3 fundamental plane wave stays one-dimensional (transverse < 1e-12) and grows as
+    D(a) to within 1e-2 at 32³ for BullFrog (1 and 16 steps), FastPM (16) and the
+    symplectic stepper (64), the error falling more than 3x from 16³ to 32³."""
+    from oracle import nbody as onb
+    c = cz.compute_timetables(cosmo)
+    L, a0 = 100.0, 0.05
+    D0, D1 = cz.Dplus(c, a0), cz.Dplus(c, 1.0)
+    for st, ns in (("bullfrog", 1), ("bullfrog", 16), ("fastpm", 16), ("symplectic", 64)):
+        err = {}
+        for n in (16, 32):
+            q = np.arange(n) * (L / n)
+            psi1 = np.zeros((n, n, n, 3))
+            psi1[..., 0] = (1e-3 * np.sin(2 * np.pi * q / L))[:, None, None]
+            Psi, _, _ = onb.run_nbody(c, D0 * psi1, psi1.copy(), boxsize=L, a_ini=a0, a_end=1.0, n_steps=ns,
+                                      res_pm=2 * n, stepper=st, return_displacement=True)
+            assert np.max(np.abs(Psi[..., 1:])) < 1e-12
+            err[n] = abs(np.sum(Psi[..., 0] * psi1[..., 0]) / np.sum(psi1[..., 0] ** 2) / D1 - 1)
+        assert err[32] < 1e-2, (st, ns)
+        assert err[16] / err[32] > 3, (st, ns)
